@@ -1,0 +1,180 @@
+"""Krylov solvers and preconditioners (oracle restatement).
+
+The reference calls ``jax.scipy.sparse.linalg.{cg, bicgstab, gmres}``
+(src/solvers/jax_linear_solver.py:349-397) with ``tol=1e-10, atol=0,
+maxiter=100, restart=30`` (config/settings.py:104-106) and x0 = the current
+Picard iterate.  jax/jaxlib are third-party and unpinned
+(requirements.txt:1-2) and absent here, so these are restatements of the
+published algorithms with JAX's documented stopping semantics:
+
+* CG: preconditioned Hestenes-Stiefel; stop when ``r.r <= max(tol^2 b.b, atol^2)``
+  (recursive residual) or after ``maxiter`` iterations.
+* BiCGSTAB: van der Vorst (1992), right preconditioned, shadow residual
+  r_hat = r0, rho0 = alpha0 = omega0 = 1, early exit on ``s.s < atol2``,
+  breakdown exit when rho, alpha or omega is exactly zero.
+* GMRES(m): Saad-Schultz, left preconditioned; ``maxiter`` counts restart
+  cycles; each cycle runs all m Arnoldi steps (classical Gram-Schmidt with one
+  re-orthogonalisation pass) unless the new basis vector vanishes, solves the
+  (m+1) x m least-squares problem, and tests the preconditioned residual
+  ``||M(b - A x)||`` against ``||M b|| * min(1, max(tol*||b||, atol)/||b||)``.
+
+Jacobi: ``Preconditioner.create_jacobi`` (jax_linear_solver.py:11-36):
+``M x = x / d`` with d = diag(A), zeros replaced by 1.
+"""
+import numpy as np
+
+
+def jacobi_inverse_diagonal(A):
+    d = A.diagonal().astype(np.float64)
+    return 1.0 / np.where(d != 0, d, 1.0)
+
+
+def _precond(dinv):
+    if dinv is None:
+        return lambda v: v
+    return lambda v: dinv * v
+
+
+def cg(A, b, x0, tol=1e-10, atol=0.0, maxiter=100, dinv=None):
+    """Returns (x, iterations)."""
+    M = _precond(dinv)
+    matvec = A.__matmul__ if not callable(A) else A
+    bs = float(b @ b)
+    atol2 = max(tol * tol * bs, atol * atol)
+    x = np.array(x0, dtype=np.float64, copy=True)
+    r = b - matvec(x)
+    z = M(r)
+    p = z.copy()
+    gamma = float(r @ z)
+    k = 0
+    while True:
+        rs = gamma if dinv is None else float(r @ r)
+        if not (rs > atol2 and k < maxiter):
+            break
+        Ap = matvec(p)
+        alpha = gamma / float(p @ Ap)
+        x = x + alpha * p
+        r = r - alpha * Ap
+        z = M(r)
+        gamma_new = float(r @ z)
+        beta = gamma_new / gamma
+        gamma = gamma_new
+        p = z + beta * p
+        k += 1
+    return x, k
+
+
+def bicgstab(A, b, x0, tol=1e-10, atol=0.0, maxiter=100, dinv=None):
+    """Returns (x, iterations); iterations < 0 flags a breakdown exit."""
+    M = _precond(dinv)
+    matvec = A.__matmul__ if not callable(A) else A
+    bs = float(b @ b)
+    atol2 = max(tol * tol * bs, atol * atol)
+    x = np.array(x0, dtype=np.float64, copy=True)
+    r = b - matvec(x)
+    rhat = r.copy()
+    rho = alpha = omega = 1.0
+    p = r.copy()
+    q = r.copy()
+    k = 0
+    while float(r @ r) > atol2 and k < maxiter and k >= 0:
+        rho_new = float(rhat @ r)
+        beta = rho_new / rho * alpha / omega
+        p = r + beta * (p - omega * q)
+        phat = M(p)
+        q = matvec(phat)
+        alpha_new = rho_new / float(rhat @ q)
+        s = r - alpha_new * q
+        exit_early = float(s @ s) < atol2
+        shat = M(s)
+        t = matvec(shat)
+        with np.errstate(all="ignore"):
+            omega_new = float(t @ s) / float(t @ t)
+        if exit_early:
+            x = x + alpha_new * phat
+            r = s
+        else:
+            x = x + (alpha_new * phat + omega_new * shat)
+            r = s - omega_new * t
+        if omega_new == 0 or alpha_new == 0:
+            k = -11
+        else:
+            k = k + 1
+        if rho_new == 0:
+            k = -10
+        rho, alpha, omega = rho_new, alpha_new, omega_new
+    return x, k
+
+
+def _safe_normalize(v, thresh=None):
+    n = float(np.sqrt(v @ v))
+    if thresh is None:
+        thresh = np.finfo(np.float64).eps
+    if n > thresh:
+        return v / n, n
+    return np.zeros_like(v), 0.0
+
+
+def gmres(A, b, x0, tol=1e-10, atol=0.0, restart=30, maxiter=100, dinv=None):
+    """Returns (x, restart_cycles)."""
+    M = _precond(dinv)
+    matvec = A.__matmul__ if not callable(A) else A
+    n = b.shape[0]
+    m = min(restart, n)
+    b_norm = float(np.sqrt(b @ b))
+    atol_eff = max(tol * b_norm, atol)
+    Mb_norm = float(np.sqrt(M(b) @ M(b)))
+    ptol = Mb_norm * min(1.0, atol_eff / b_norm) if b_norm > 0 else 0.0
+    x = np.array(x0, dtype=np.float64, copy=True)
+    unit, rnorm = _safe_normalize(M(b - matvec(x)))
+    eps = np.finfo(np.float64).eps
+    k = 0
+    while k < maxiter and rnorm > ptol:
+        V = np.zeros((m + 1, n))
+        H = np.zeros((m + 1, m))
+        V[0] = unit
+        steps = 0
+        for j in range(m):
+            w = M(matvec(V[j]))
+            w_norm0 = float(np.sqrt(w @ w))
+            h = np.zeros(m + 1)
+            for _ in range(2):                       # CGS2: project twice
+                c = V[: j + 1] @ w
+                w = w - c @ V[: j + 1]
+                h[: j + 1] += c
+            unit_w, w_norm = _safe_normalize(w, thresh=eps * w_norm0)
+            h[j + 1] = w_norm
+            H[:, j] = h
+            V[j + 1] = unit_w
+            steps = j + 1
+            if w_norm == 0.0:
+                break
+        beta_vec = np.zeros(m + 1)
+        beta_vec[0] = rnorm
+        y = np.linalg.lstsq(H[: steps + 1, :steps], beta_vec[: steps + 1], rcond=None)[0]
+        x = x + y @ V[:steps]
+        unit, rnorm = _safe_normalize(M(b - matvec(x)))
+        k += 1
+    return x, k
+
+
+def solve_system(A, b, x0, solver_type="gmres", precond_type="none", tol=1e-10,
+                 maxiter=100, restart=30):
+    """Dispatch of src/solvers/solver_types.py:7-67 (Jacobi or no preconditioner).
+
+    Returns (x, iterations).  ``direct`` solves exactly (the reference densifies
+    and calls jnp.linalg.solve; a sparse LU gives the same solution).
+    """
+    if precond_type not in ("none", None, "jacobi"):
+        raise NotImplementedError(f"oracle preconditioner {precond_type!r}")
+    dinv = jacobi_inverse_diagonal(A) if precond_type == "jacobi" else None
+    if solver_type == "cg":
+        return cg(A, b, x0, tol=tol, maxiter=maxiter, dinv=dinv)
+    if solver_type == "bicgstab":
+        return bicgstab(A, b, x0, tol=tol, maxiter=maxiter, dinv=dinv)
+    if solver_type == "gmres":
+        return gmres(A, b, x0, tol=tol, restart=restart, maxiter=maxiter, dinv=dinv)
+    if solver_type == "direct":
+        import scipy.sparse.linalg as spla
+        return spla.spsolve(A.tocsc(), b), 0
+    raise ValueError(f"Unsupported solver type: {solver_type}")

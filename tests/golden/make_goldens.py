@@ -1,0 +1,85 @@
+"""Regenerate the committed golden fixtures from the reference tree.
+
+Run in a container that has the reference checked out (read-only) at
+/root/reference:
+
+    python tests/golden/make_goldens.py [/root/reference]
+
+It writes, next to this script:
+  * ``re2d_metrics.json``  -- every row of resultsRE2D/benchmark_results_*_WA.csv
+    (test case, mesh, solver, preconditioner, Picard iteration total and the six
+    analytical-error metrics to 5 significant digits);
+  * ``test3d_<solver>.npz`` -- results3D/numerical_results_Test3D_*_mesh25.npz:
+    per-step iterations, dt, times, Picard errors and the pressure-head field of
+    steps 0, 4 and 9 (the full 10 x 9261 field is not needed);
+  * ``mesh_digests.json`` -- shape and SHA-256 of the reference meshes
+    (data/mesh/richards/p*.csv, t*.csv, p_3D.csv, t_3D.csv; nitrogen p_*.csv,
+    t_*.csv) as loaded by src/mesh/loader.py:69-71 (float64 points, 0-based
+    int64 connectivity), so the structured generators can be checked without
+    the reference tree.
+Nothing at test time reads the reference tree.
+"""
+import csv
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def digest(a):
+    a = np.ascontiguousarray(a)
+    return {"shape": list(a.shape), "dtype": str(a.dtype), "sha256": hashlib.sha256(a.tobytes()).hexdigest()}
+
+
+def load_csv(path, dtype):
+    return np.loadtxt(path, delimiter=",", dtype=dtype, ndmin=2)
+
+
+def main(ref):
+    rows = []
+    d = os.path.join(ref, "resultsRE2D")
+    for name in sorted(os.listdir(d)):
+        if not name.endswith(".csv"):
+            continue
+        hw = "gpu" if "_gpu_" in name else "cpu"
+        with open(os.path.join(d, name)) as f:
+            for r in csv.DictReader(f):
+                rows.append({"file": name, "hw": hw, "test_case": r["test_case"], "mesh": int(r["mesh_size"]),
+                             "solver": r["solver"], "precond": r["preconditioner"],
+                             "iterations": int(r["iterations"]),
+                             "metrics": [float(r[k]) for k in ("l2_pressure", "linf_pressure", "l2_saturation",
+                                                               "linf_saturation", "l2_relative_pressure",
+                                                               "l2_relative_saturation")],
+                             "simulation_time": float(r["simulation_time"])})
+    with open(os.path.join(HERE, "re2d_metrics.json"), "w") as f:
+        json.dump(rows, f, indent=0)
+
+    for solver in ("bicgstab", "gmres"):
+        z = np.load(os.path.join(ref, "results3D", f"numerical_results_Test3D_{solver}_{solver}_none_mesh25.npz"),
+                    allow_pickle=True)
+        np.savez_compressed(os.path.join(HERE, f"test3d_{solver}.npz"),
+                            iterations=z["iterations"], dt_values=z["dt_values"], times=z["times"],
+                            errors=z["errors"], steps=np.array([0, 4, 9]),
+                            pressure_head=z["pressure_head"][[0, 4, 9]], theta=z["theta"][[0, 4, 9]])
+
+    meshes = {}
+    mdir = os.path.join(ref, "data", "mesh")
+    for n in (25, 50, 100, 200):
+        meshes[f"richards/p{n}"] = digest(load_csv(os.path.join(mdir, "richards", f"p{n}.csv"), np.float64))
+        meshes[f"richards/t{n}"] = digest(load_csv(os.path.join(mdir, "richards", f"t{n}.csv"), np.int64) - 1)
+    meshes["richards/p_3D"] = digest(load_csv(os.path.join(mdir, "richards", "p_3D.csv"), np.float64))
+    meshes["richards/t_3D"] = digest(load_csv(os.path.join(mdir, "richards", "t_3D.csv"), np.int64) - 1)
+    for n in (25, 50, 100):
+        meshes[f"nitrogen/p_{n}"] = digest(load_csv(os.path.join(mdir, "nitrogen", f"p_{n}.csv"), np.float64))
+        meshes[f"nitrogen/t_{n}"] = digest(load_csv(os.path.join(mdir, "nitrogen", f"t_{n}.csv"), np.int64) - 1)
+    with open(os.path.join(HERE, "mesh_digests.json"), "w") as f:
+        json.dump(meshes, f, indent=1)
+    print(f"wrote {len(rows)} CSV rows, 2 Test3D fixtures, {len(meshes)} mesh digests")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
