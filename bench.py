@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: DOF x Picard-iterations / s of the implicit 2D Richards step on B200.
+
+Workload (the 1024^2 configuration): unit square, 1024 x 1024 cells split into
+2 P1 triangles (2,097,152 elements, 1,050,625 nodes), van Genuchten-Mualem soil
+(theta_r .102, theta_s .368, alpha 3.35, n 2, m .5) with per-element
+log-normal Ks (ln Ks ~ N(ln .0922, 1), seed-generated), h0 = -1, Dirichlet
+h = -0.1 on the top edge, no-flux elsewhere; 20 implicit steps at dt = 1e-4;
+Picard tolerance 1e-6 (relative); every linear solve to a 1e-8 relative
+residual.  Two paths on the same GPU: plain FP64 Jacobi-CG and FP32 Jacobi-CG
+inside FP64 iterative refinement on the true residual (the headline `value`).
+
+A "step" is one implicit time step (a full device-resident Picard loop).  The
+timed region runs K steps from the initial state after W untimed warm-up
+steps; L2 is flushed (a 256 MiB write) between timed steps, outside the
+events.  `--impl reference` times the CPU oracle (the NumPy/SciPy
+restatement of the reference's algorithm; JAX is not installed) on a bounded
+sample: one Picard iteration of the same workload per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "jax-wspm_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "DOF*Picard-iters/s at 1e-8 residual (1024^2 2D Richards, mixed FP32/FP64 refinement; FP64 alongside)"
+UNIT = "DOF*Picard-iter/s"
+VG_PHI_UNIT_KS = (3.35, 0.368, 0.102, 2.0, 0.5, 1.0)
+KS_MEAN = 0.0922
+
+
+def workload(n, seed):
+    from wspm_b200 import mesh
+    pts, tri = mesh.structured_triangles(n, 1.0)
+    rng = np.random.default_rng(seed)
+    Ks = np.exp(np.log(KS_MEAN) + 1.0 * rng.standard_normal(len(tri)))
+    top = np.where(pts[:, 1] == 1.0)[0]
+    return pts, tri, Ks, top
+
+
+def algorithmic_bytes_cg(N, nnz, w):
+    """One Jacobi-CG iteration: B_spmv + 11 N w, B_spmv = nnz (w+4) + (N+1) 4 + 2 N w."""
+    return nnz * (w + 4) + (N + 1) * 4 + 2 * N * w + 11 * N * w
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for s in self.samples for j in range(4) if s[5 + j].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def allreduce_max(v, world):
+    import torch
+    if world == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_path(eng, h0, dt, steps, warmup, world, flush):
+    """Warm up, then time `steps` steps from h0 with per-step CUDA events; returns totals."""
+    import torch
+    eng.set_state(h0)
+    eng.dt_dev.fill_(dt)
+    for _ in range(warmup):
+        eng.launch_step(dt)
+    torch.cuda.synchronize()
+    eng.set_state(h0)
+    res_buf = torch.zeros((steps, 8), dtype=torch.int32, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier(world)
+    for k in range(steps):
+        flush()
+        ev[k][0].record()
+        eng.launch_step(dt)
+        ev[k][1].record()
+        res_buf[k].copy_(eng.result)
+    barrier(world)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    r = res_buf.cpu().numpy()
+    its, kits, refs, bodies = int(r[:, 1].sum()), int(r[:, 2].sum()), int(r[:, 3].sum()), r[:, 6]
+    launches = sum(eng.kernel_launches(int(r[k, 1]), int(r[k, 3]), int(bodies[k])) for k in range(steps))
+    return {"ms": ms, "picard_its": its, "krylov_its": kits, "refinements": refs, "status": r[:, 0].tolist(),
+            "launches": launches}
+
+
+def time_e2e(eng, h0, dt, steps, world, flush):
+    """Same metric through the public step API with host (pinned) buffers: H2D + step + D2H per step."""
+    import torch
+    N = eng.dm.n_nodes
+    h_host = torch.from_numpy(np.asarray(h0, dtype=np.float64)).pin_memory()
+    out_host = torch.empty(N, dtype=torch.float64).pin_memory()
+    res_host = torch.empty((steps, 8), dtype=torch.int32).pin_memory()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    eng.set_state(h0)
+    barrier(world)
+    for k in range(steps):
+        flush()
+        ev[k][0].record()
+        src = h_host if k == 0 else out_host
+        eng.h_n.copy_(src, non_blocking=True)
+        eng.launch_step(dt)
+        out_host.copy_(eng.h_n, non_blocking=True)
+        res_host[k].copy_(eng.result, non_blocking=True)
+        ev[k][1].record()
+    barrier(world)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    its = int(res_host[:, 1].sum())
+    return {"ms": ms, "picard_its": its, "h2d": N * 8, "d2h": N * 8 + 32}
+
+
+def roofline_probe(dm, eng, fp32, reps=200):
+    """Average duration of one Jacobi-CG iteration (fused K1 + K2) on the assembled system."""
+    import ctypes
+    import torch
+    from wspm_b200 import _lib
+    from wspm_b200._lib import check, lib
+    N = dm.n_nodes
+    if fp32:
+        vals, dinv = eng.vals32, eng.dinv.float()
+        b, x = eng.rhs.float(), eng.h_m.float()
+    else:
+        vals, dinv, b, x = eng.vals, eng.dinv, eng.rhs, eng.h_m.clone()
+    work = torch.empty(int(lib.wspm_krylov_workspace_doubles(N, 0, 0)), dtype=torch.float64, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def run(iters):
+        check("cg_iterations", lib.wspm_cg_iterations(ctypes.byref(dm.c_pat), int(fp32), _lib.dptr(vals),
+                                                       _lib.dptr(b), _lib.dptr(x), _lib.dptr(dinv), iters,
+                                                       _lib.dptr(work), work.numel(), st))
+    run(20)
+    torch.cuda.synchronize()
+    times = {}
+    for iters in (0, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run(iters)
+        e1.record()
+        torch.cuda.synchronize()
+        times[iters] = e0.elapsed_time(e1)
+    return (times[reps] - times[0]) / reps * 1e-3     # seconds per CG iteration
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(key):
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get(key)
+    return None
+
+
+def cpu_baseline(n, seed, picard_its=1):
+    """Oracle (NumPy/SciPy, single thread) on one Picard iteration of the same workload."""
+    from oracle import picard as opic
+    pts, tri, Ks, top = workload(n, seed)
+    prob, h0 = opic.vg_dirichlet_case(pts, tri, top, Ks_elem=Ks, tol=1e-8, maxiter=100000)
+    _, _, theta_n = prob.model(h0)
+    t0 = time.perf_counter()
+    h = h0.copy()
+    for _ in range(picard_its):
+        A, b = prob.linear_system(h, theta_n, 1e-4)
+        from oracle.krylov import solve_system
+        h, _ = solve_system(A, b, h, "cg", "jacobi", tol=1e-8, maxiter=100000)
+    dt = time.perf_counter() - t0
+    return {"value": len(pts) * picard_its / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{picard_its} Picard iteration(s) of the {n}^2 workload (assembly + Jacobi-CG to 1e-8), "
+                      f"NumPy/SciPy oracle, 1 thread, {dt:.1f} s"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import picard as opic
+    from oracle.krylov import solve_system
+    pts, tri, Ks, top = workload(args.n, args.seed)
+    prob, h0 = opic.vg_dirichlet_case(pts, tri, top, Ks_elem=Ks, tol=1e-8, maxiter=100000)
+    _, _, theta_n = prob.model(h0)
+
+    def one():
+        A, b = prob.linear_system(h0, theta_n, 1e-4)
+        solve_system(A, b, h0, "cg", "jacobi", tol=1e-8, maxiter=100000)
+
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    dt = time.perf_counter() - t0
+    v = len(pts) * args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"2D Richards {args.n}^2 VG, per-element log-normal Ks, dt 1e-4, "
+                                   "1 Picard iteration per step (bounded CPU sample)",
+                       "nodes": len(pts), "elements": len(tri), "seed": args.seed},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": "one Picard iteration (assembly + Jacobi-CG to 1e-8) of the same workload "
+                                       "per step; NumPy/SciPy oracle (JAX, the reference's runtime, is not "
+                                       "installed), single thread"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=1024)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--inner-tol", type=float, default=1e-5,
+                    help="floor of the relative tolerance of each FP32 solve in the refinement loop")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="drive the Picard/Krylov loops from the host (same kernels; for ncu, which cannot "
+                         "profile kernels inside conditional graphs)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from wspm_b200.device import DeviceMesh, merge_dirichlet
+    from wspm_b200.engine import PicardEngine
+    world, rank, local = dist_setup(args)
+    pts, tri, Ks, top = workload(args.n, args.seed)
+    N, E = len(pts), len(tri)
+    dm = DeviceMesh(pts, tri, device=f"cuda:{local}")
+    bc = merge_dirichlet(N, [(top, -0.1)])
+    h0 = -np.ones(N)
+    dt = 1e-4
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = lambda: flush_buf.fill_(1.0)  # noqa: E731
+    common = dict(Ks_elem=Ks, bc_val=bc, solver="cg", precond="jacobi", krylov_tol=1e-8, krylov_maxiter=20000,
+                  picard_tol=1e-6, picard_maxiter=100, picard_relative=True)
+    eng64 = PicardEngine(dm, "vg", VG_PHI_UNIT_KS, mixed=False, **common)
+    engmx = PicardEngine(dm, "vg", VG_PHI_UNIT_KS, mixed=True, inner_tol=args.inner_tol, inner_maxiter=20000,
+                         refine_maxiter=30, **common)
+    eng64.host_loop = engmx.host_loop = args.host_loop
+    with ClockSampler(local) as clk:
+        r64 = time_path(eng64, h0, dt, args.steps, args.warmup, world, flush)
+        h64 = eng64.h_n.clone()
+        rmx = time_path(engmx, h0, dt, args.steps, args.warmup, world, flush)
+        hmx = engmx.h_n.clone()
+    e2e = time_e2e(engmx, h0, dt, args.steps, world, flush)
+    # accuracy of the mixed path against FP64 and of both against the true residual
+    from wspm_b200.device import spmv
+    res_true = {}
+    for name, eng in (("fp64", eng64), ("mixed", engmx)):
+        r = eng.rhs - spmv(dm, eng.vals, eng.x)
+        res_true[name] = float(torch.linalg.norm(r) / torch.linalg.norm(eng.rhs))
+    rel_diff = float(torch.linalg.norm(hmx - h64) / torch.linalg.norm(h64))
+    # roofline of the dominant kernels (one Jacobi-CG iteration = fused K1 + K2)
+    t_it32 = roofline_probe(dm, engmx, fp32=True)
+    t_it64 = roofline_probe(dm, eng64, fp32=False)
+    nnz = dm.pattern.nnz
+    peak, peak_kind = load_peaks()
+    b32 = algorithmic_bytes_cg(N, nnz, 4)
+    b64 = algorithmic_bytes_cg(N, nnz, 8)
+    ms64 = allreduce_max(r64["ms"], world)
+    msmx = allreduce_max(rmx["ms"], world)
+    mse2e = allreduce_max(e2e["ms"], world)
+    if rank != 0:
+        barrier(world)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    v64 = world * N * r64["picard_its"] / (ms64 * 1e-3)
+    vmx = world * N * rmx["picard_its"] / (msmx * 1e-3)
+    ve2e = world * N * e2e["picard_its"] / (mse2e * 1e-3)
+    ach32 = b32 / t_it32 / 1e9
+    ach64 = b64 / t_it64 / 1e9
+    line = {
+        "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": msmx / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 Krylov + f64 refinement/assembly", "data": "synthetic (seeded log-normal Ks)",
+        "config": {"workload": f"2D Richards {args.n}^2 P1 triangles, VG soil, per-element log-normal Ks "
+                               f"(sigma_lnK 1, seed {args.seed}), h0 -1, top Dirichlet -0.1, dt 1e-4 fixed, "
+                               f"{args.steps} steps from the initial state",
+                   "nodes": N, "elements": E, "nnz": nnz, "picard_tol": 1e-6, "krylov_residual": 1e-8,
+                   "l2_policy": "L2 flushed (256 MiB write) between timed steps",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "loop_control": "host" if args.host_loop else "device (CUDA graph conditional nodes)"},
+        "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "picard_its": r64["picard_its"],
+                 "krylov_its": r64["krylov_its"], "true_rel_residual": res_true["fp64"]},
+        "mixed": {"value": vmx, "picard_its": rmx["picard_its"], "inner_krylov_its": rmx["krylov_its"],
+                  "refinements": rmx["refinements"], "true_rel_residual": res_true["mixed"],
+                  "rel_diff_vs_fp64": rel_diff, "speedup_vs_fp64": vmx / v64},
+        "status": {"fp64": r64["status"], "mixed": rmx["status"]},
+        "e2e": {"value": ve2e, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+        "gpu_launches": rmx["launches"] + r64["launches"],
+        "roofline": {"bound": "hbm", "kernel": "one FP32 Jacobi-CG iteration (fused SpMV kernel + update kernel)",
+                     "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak, "peak_kind": peak_kind,
+                     "traffic": load_traffic("cg_iteration_f32"), "algorithmic_bytes": b32,
+                     "seconds_per_iteration": t_it32,
+                     "fp64": {"achieved": ach64, "frac": ach64 / peak, "algorithmic_bytes": b64,
+                              "seconds_per_iteration": t_it64, "traffic": load_traffic("cg_iteration_f64")}},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args.n, args.seed)
+    print(json.dumps(line))
+    barrier(world)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

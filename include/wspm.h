@@ -1,0 +1,214 @@
+/*
+ * wspm.h -- C ABI of libwspm.so, the B200 (sm_100a) implementation of the
+ * JAX-WSPM implicit P1-FEM Picard step.
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer (caller-allocated; the library
+ *    never allocates device memory).  Sizes are explicit.  `stream` is a
+ *    cudaStream_t passed as void*; NULL means the legacy default stream.
+ *  - Every entry point returns an int status (WSPM_OK = 0).  Launch and
+ *    argument errors are reported synchronously; numerical outcomes
+ *    (iteration caps, NaN, breakdown) are written to device status words
+ *    so that no call has to synchronise with the host.
+ *  - Sparse matrices use the SELL-32 layout described by wspm_pattern: rows
+ *    are grouped in slices of 32; entry k of row i lives at
+ *    slice_ptr[i/32] + 32*k + i%32.  Padding entries have column = own row
+ *    and value 0.
+ *  - Meshes: conn is element-major int32 [E*nv] (0-based), coords is
+ *    node-major float64 [N*dim].
+ *
+ * The reference (JAX-WSPM) is pure Python + JAX; each entry point below names
+ * the reference function whose behaviour it implements (file:line within the
+ * reference project).  Python shims with the reference's own signatures live
+ * in jax-wspm_b200/src/ (see INTEGRATION.md).
+ */
+#ifndef WSPM_H
+#define WSPM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define WSPM_OK            0
+#define WSPM_MAXITER       1   /* Krylov or Picard iteration cap reached      */
+#define WSPM_NAN           2   /* non-finite residual / iterate               */
+#define WSPM_BREAKDOWN     3   /* Krylov breakdown (rho, alpha or omega = 0)  */
+#define WSPM_BAD_ARG      10   /* invalid argument (null pointer, size, ...)  */
+#define WSPM_CUDA_ERROR   11   /* a CUDA runtime call failed                  */
+#define WSPM_UNSUPPORTED  12   /* feature/combination not implemented         */
+
+/* ---- solver / model ids ------------------------------------------------ */
+#define WSPM_SOLVER_CG        0
+#define WSPM_SOLVER_BICGSTAB  1
+#define WSPM_SOLVER_GMRES     2
+#define WSPM_PRECOND_NONE     0
+#define WSPM_PRECOND_JACOBI   1
+#define WSPM_SOIL_VAN_GENUCHTEN 0
+#define WSPM_SOIL_EXPONENTIAL   1
+
+/* ---- data descriptors -------------------------------------------------- */
+typedef struct wspm_mesh {
+    int32_t n_nodes;
+    int32_t n_elems;
+    int32_t dim;              /* 2 (triangles) or 3 (tetrahedra)             */
+    int32_t nv;               /* vertices per element: dim + 1               */
+    const int32_t *conn;      /* [n_elems * nv]                              */
+    const double  *coords;    /* [n_nodes * dim]                             */
+} wspm_mesh;
+
+typedef struct wspm_pattern {
+    int32_t n_rows;
+    int32_t n_slices;         /* ceil(n_rows / 32)                           */
+    int32_t max_width;        /* max over slices of slice_width              */
+    int32_t max_inc;          /* max over slices of inc_width                */
+    int64_t nnz_padded;       /* slice_ptr[n_slices]                         */
+    const int64_t *slice_ptr; /* [n_slices + 1]                              */
+    const int32_t *slice_width;/* [n_slices]                                 */
+    const int32_t *cols;      /* [nnz_padded]                                */
+    const int32_t *diag_pos;  /* [n_rows] position k of the diagonal entry   */
+    /* node -> element incidence, same sliced layout (element ids ascending) */
+    const int64_t *inc_ptr;   /* [n_slices + 1]                              */
+    const int32_t *inc_width; /* [n_slices]                                  */
+    const int32_t *inc_elem;  /* element id, -1 = padding                    */
+    const uint32_t *inc_slots;/* bits 0-1: local vertex of the row's node;
+                                 bits 2+6j..7+6j: row position of vertex j   */
+} wspm_pattern;
+
+/* ---- soil models -------------------------------------------------------- */
+/* van_genuchten_model, src/models/van_genuchten.py:9-47 (vmapped over nodes).
+ * phi = {alpha, theta_s, theta_r, n, m, Ks} (host array, 6 doubles).
+ * Any of C, K, theta may be NULL.                                          */
+int wspm_soil_van_genuchten(const double *h, int64_t n, const double *phi,
+                            double *C, double *K, double *theta, void *stream);
+
+/* exponential_model, src/models/exponential.py:10-41.
+ * phi = {alpha0, theta_s, theta_r, Ks} (host array, 4 doubles).            */
+int wspm_soil_exponential(const double *h, int64_t n, const double *phi,
+                          double *C, double *K, double *theta, void *stream);
+
+/* ---- assembly ----------------------------------------------------------- */
+/* assemble_global_matrices_sparse_re, src/numerics/assembly_re_v2.py:62-166
+ * (mesh->dim == 2) and assemble_global_matrices_sparse_3D,
+ * src/numerics/assembly_re_3D.py:72-169 (mesh->dim == 3), fused with
+ * apply_dirichlet_bcs (src/models/boundary.py:38-53) and the diagonal of
+ * Preconditioner.create_jacobi (src/solvers/jax_linear_solver.py:11-36).
+ *   quad_points [nq*dim], weights [nq]: host arrays (the reference's rule).
+ *   Ks_elem: optional per-element factor multiplying K (NULL = 1).
+ *   bc_val:  optional per-node Dirichlet value, NaN = free node (NULL = none).
+ *   vals32, dinv: optional outputs (NULL = skip).                          */
+int wspm_assemble_richards(const wspm_mesh *mesh, const wspm_pattern *pat,
+                           const double *theta_m, const double *theta_n,
+                           const double *h_m, const double *K, const double *C,
+                           const double *Ks_elem,
+                           const double *quad_points, const double *weights, int32_t nq,
+                           double dt, const double *bc_val,
+                           double *vals, float *vals32, double *rhs, double *dinv,
+                           void *stream);
+
+/* ---- sparse kernels ----------------------------------------------------- */
+/* y = A x (BCOO matvec inside jax.scipy.sparse.linalg, SELL-32 here).       */
+int wspm_spmv_f64(const wspm_pattern *pat, const double *vals, const double *x,
+                  double *y, void *stream);
+int wspm_spmv_f32(const wspm_pattern *pat, const float *vals, const float *x,
+                  float *y, void *stream);
+
+/* apply_dirichlet_bcs, src/models/boundary.py:38-53: rows nodes[i] become
+ * e_i and rhs[nodes[i]] = values[i].  nodes must be unique; callers that
+ * apply several sets in sequence (top, then bottom) merge them first, later
+ * sets overriding earlier ones.                                            */
+int wspm_apply_dirichlet(const wspm_pattern *pat, const int32_t *nodes,
+                         const double *values, int32_t n_bc, double *vals,
+                         double *rhs, void *stream);
+
+/* Preconditioner.create_jacobi, src/solvers/jax_linear_solver.py:11-36:
+ * dinv = 1 / diag(A) with zero diagonals replaced by 1.                    */
+int wspm_jacobi_dinv(const wspm_pattern *pat, const double *vals, double *dinv,
+                     void *stream);
+
+/* ---- Krylov solves -------------------------------------------------------- */
+/* solve_system, src/solvers/solver_types.py:7-67 with JAXSparseSolver
+ * (src/solvers/jax_linear_solver.py:255-329): x holds x0 on entry and the
+ * solution on exit.  dinv == NULL means no preconditioner.  `work` is a
+ * device buffer of wspm_krylov_workspace_doubles() doubles.  `result` is a
+ * device int32[4]: {status, iterations, 0, 0}; iterations count Krylov
+ * iterations (CG, BiCGSTAB) or restart cycles (GMRES) like JAX's maxiter.  */
+int64_t wspm_krylov_workspace_doubles(int32_t n_rows, int32_t solver, int32_t restart);
+int wspm_krylov_solve(const wspm_pattern *pat, const double *vals,
+                      const double *b, double *x, const double *dinv,
+                      int32_t solver, double tol, double atol, int32_t maxiter,
+                      int32_t restart, double *work, int64_t work_doubles,
+                      int32_t *result, void *stream);
+
+/* Measurement hook (no reference counterpart): runs exactly `iters` Jacobi-CG
+ * iterations (fused kernels K1+K2, no convergence test) from x on the given
+ * system as plain launches on `stream`, so the per-iteration time of the
+ * dominant kernels can be taken with CUDA events.  fp32 != 0 selects the FP32
+ * kernels (vals, b, x, dinv are then float arrays).  `work` as for CG.       */
+int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const void *vals, const void *b, void *x,
+                       const void *dinv, int32_t iters, double *work, int64_t work_doubles, void *stream);
+
+/* ---- Picard time step (device-resident loop in a CUDA graph) ------------- */
+/* RichardsSolver.solve_timestep, src/solvers/richards_solver_v2.py:107-168
+ * (relative Picard error) and RichardsSolver3D.solve_timestep,
+ * src/solvers/richards_solver_3D_v2.py:177-222 (absolute error).  One call
+ * runs one implicit time step; the Picard loop, the Krylov loop and both
+ * convergence tests run on the device inside one CUDA graph.              */
+typedef struct wspm_picard_desc {
+    const wspm_mesh *mesh;
+    const wspm_pattern *pat;
+    int32_t soil_model;        /* WSPM_SOIL_*                                */
+    double  phi[6];            /* soil parameters (see wspm_soil_*)          */
+    const double *Ks_elem;     /* optional per-element conductivity factor   */
+    const double *bc_val;      /* optional Dirichlet values (NaN = free)     */
+    double quad_points[16 * 3];/* reference quadrature rule (nq <= 16)       */
+    double weights[16];
+    int32_t nq;
+    int32_t solver;            /* WSPM_SOLVER_*                              */
+    int32_t precond;           /* WSPM_PRECOND_*                             */
+    double  krylov_tol;        /* relative tolerance                         */
+    int32_t krylov_maxiter;    /* iterations (CG, BiCGSTAB) or cycles (GMRES) */
+    int32_t restart;           /* GMRES restart length m (1..32)             */
+    int32_t mixed;             /* 1: FP32 Krylov inside FP64 refinement      */
+    double  inner_tol;         /* mixed: relative tolerance of each FP32 solve */
+    int32_t inner_maxiter;
+    int32_t refine_maxiter;
+    double  picard_tol;
+    int32_t picard_maxiter;
+    int32_t picard_relative;   /* 1: ||h-h_m||/||h||, 0: ||h-h_m||           */
+    /* state (device, caller-owned, n_nodes doubles unless noted) */
+    double *h_n;               /* in: previous step; out: this step's head   */
+    double *theta_n;           /* scratch: theta(h_n)                        */
+    double *h_m, *x;           /* Picard iterate, Krylov iterate             */
+    double *K, *C, *theta_m;   /* soil fields                                */
+    double *vals;              /* [pat->nnz_padded]                          */
+    float  *vals32;            /* [pat->nnz_padded], mixed only              */
+    double *rhs, *dinv;
+    double *work;              /* wspm_picard_workspace_doubles()            */
+    int64_t work_doubles;
+    double *dt_dev;            /* device double: the step's dt               */
+    int32_t *result;           /* device int32[8]: status, picard its,
+                                  total Krylov its, refinement its, ...     */
+    double *result_f64;        /* device double[4]: picard error, ...       */
+} wspm_picard_desc;
+
+int64_t wspm_picard_workspace_doubles(int32_t n_rows, int32_t mixed);
+int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out);
+int wspm_picard_step(void *plan, void *stream);
+/* The same step with the loops driven from the host (identical kernels; the
+ * host reads the device's convergence words between bounded chunks of
+ * Krylov iterations).  Synchronises with the host; for profiling tools that
+ * cannot follow conditional graph nodes, and as a fallback.               */
+int wspm_picard_step_host(void *plan, void *stream);
+int wspm_picard_destroy(void *plan);
+
+/* ---- misc ------------------------------------------------------------------ */
+const char *wspm_version(void);
+const char *wspm_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WSPM_H */

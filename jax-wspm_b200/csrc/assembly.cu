@@ -1,0 +1,266 @@
+// Soil-model and Richards assembly kernels.
+//
+// Assembly is row-gather: thread i owns row i of the global matrix.  It walks
+// the elements incident to node i (ascending element id, the order in which
+// the reference's COO entries meet in BCOO.sum_duplicates and in which its
+// fori_loop scatters the right-hand side, assembly_re_v2.py:145-164), computes
+// row "local vertex of i" of each element matrix in registers, and
+// accumulates into the row's SELL slots held in shared memory.  Each row is
+// written exactly once, coalesced across the warp, with no atomics.
+//
+// Element math (P1, constant gradient): G = J^-1 dN/dref, detJ signed as
+// jnp.linalg.det.  With the reference's quadrature rule (points Q, weights W)
+//   Kbar   = sum_q w_q (N_q . K)            = sum_j s_j K_j,  s_j = sum_q w_q N_qj
+//   Ml_i   = rowsum_j sum_q w_q N_qi N_qj * detJ = mcoef_i * detJ
+//   A_e    = Kbar (G^T G) detJ + diag(Ml * C) / dt
+//   b_e,i  = -Kbar G[dim-1, i] detJ - Ml_i (theta_m,i - theta_n,i - C_i h_i) / dt
+// which is compute_local_matrices_mixed_form (assembly_re_v2.py:13-60) and its
+// 3D twin (assembly_re_3D.py:12-70).
+#include "common.cuh"
+#include "soil.cuh"
+
+namespace wspm {
+
+__global__ void soil_kernel(SoilParams sp, const double *__restrict__ h, int64_t n,
+                            double *C, double *K, double *theta) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double c, k, t;
+        soil_eval(sp, h[i], c, k, t);
+        if (C) C[i] = c;
+        if (K) K[i] = k;
+        if (theta) theta[i] = t;
+    }
+}
+
+struct RichardsAsmArgs {
+    int n_rows;
+    const int64_t *slice_ptr;
+    const int32_t *slice_width;
+    const int32_t *diag_pos;
+    const int64_t *inc_ptr;
+    const int32_t *inc_width;
+    const int32_t *inc_elem;
+    const uint32_t *inc_slots;
+    const int32_t *conn;
+    const double *coords;
+    const double *theta_m, *theta_n, *h_m, *K, *C, *Ks_elem, *bc_val;
+    double s[4];       // K-average weights per vertex
+    double mcoef[4];   // lumped-mass coefficients per vertex
+    double inv_dt;
+    const double *dt_dev;   // when set, dt is read from device memory (graph replay)
+    double *vals;
+    float *vals32;
+    double *rhs, *dinv;
+};
+
+template <int DIM>
+__device__ __forceinline__ void p1_geometry(const double *__restrict__ coords, const int (&nd)[DIM + 1],
+                                            double (&G)[DIM][DIM + 1], double &detJ) {
+    if constexpr (DIM == 2) {
+        const double x0 = coords[2 * nd[0]], y0 = coords[2 * nd[0] + 1];
+        const double J00 = coords[2 * nd[1]] - x0, J01 = coords[2 * nd[1] + 1] - y0;
+        const double J10 = coords[2 * nd[2]] - x0, J11 = coords[2 * nd[2] + 1] - y0;
+        detJ = J00 * J11 - J01 * J10;
+        const double id = 1.0 / detJ;
+        // J^-1 = [[J11, -J01], [-J10, J00]] / det ; G[:,1] = J^-1[:,0], G[:,2] = J^-1[:,1]
+        G[0][1] = J11 * id;  G[1][1] = -J10 * id;
+        G[0][2] = -J01 * id; G[1][2] = J00 * id;
+        G[0][0] = -(G[0][1] + G[0][2]);
+        G[1][0] = -(G[1][1] + G[1][2]);
+    } else {
+        double J[3][3];
+        const double *p0 = coords + 3 * nd[0];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const double *pr = coords + 3 * nd[r + 1];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) J[r][c] = pr[c] - p0[c];
+        }
+        const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+        const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+        const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+        detJ = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+        const double id = 1.0 / detJ;
+        // inverse = adj / det, adj[r][c] = cofactor[c][r]
+        double inv[3][3];
+        inv[0][0] = c00 * id;
+        inv[1][0] = c01 * id;
+        inv[2][0] = c02 * id;
+        inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+        inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+        inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+        inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+        inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+        inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            G[d][1] = inv[d][0];
+            G[d][2] = inv[d][1];
+            G[d][3] = inv[d][2];
+            G[d][0] = -((inv[d][0] + inv[d][1]) + inv[d][2]);
+        }
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
+    constexpr int NV = DIM + 1;
+    extern __shared__ double acc_sm[];   // [max_width][blockDim.x]
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = i >> 5, lane = i & 31;
+    if (s >= ((a.n_rows + kSlice - 1) >> 5)) return;
+    const int width = a.slice_width[s];
+    if (i >= a.n_rows) {
+        // padding rows of the last slice: keep their slots defined (zero)
+        const int64_t pb = a.slice_ptr[s] + lane;
+        for (int k = 0; k < width; ++k) {
+            a.vals[pb + (int64_t)kSlice * k] = 0.0;
+            if (a.vals32) a.vals32[pb + (int64_t)kSlice * k] = 0.0f;
+        }
+        return;
+    }
+    double *acc = acc_sm + threadIdx.x;
+    const int stride = blockDim.x;
+    for (int k = 0; k < width; ++k) acc[k * stride] = 0.0;
+    const int dpos = a.diag_pos[i];
+
+    const double inv_dt = a.dt_dev ? 1.0 / *a.dt_dev : a.inv_dt;
+    const double bcv = a.bc_val ? a.bc_val[i] : __longlong_as_double(0x7ff8000000000000ULL);
+    double rhs_i, diag;
+    if (!isnan(bcv)) {
+        acc[dpos * stride] = 1.0;
+        rhs_i = bcv;
+        diag = 1.0;
+    } else {
+        const double Ci = a.C[i];
+        const double tm = a.theta_m[i], tn = a.theta_n[i], hi = a.h_m[i];
+        const double storage = tm - tn - Ci * hi;
+        double bsum = 0.0;
+        const int deg = a.inc_width[s];
+        const int64_t ib = a.inc_ptr[s] + lane;
+        for (int k = 0; k < deg; ++k) {
+            const int e = a.inc_elem[ib + (int64_t)kSlice * k];
+            if (e < 0) break;
+            const uint32_t packed = a.inc_slots[ib + (int64_t)kSlice * k];
+            const int li = packed & 3;
+            int nd[NV];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) nd[j] = a.conn[(int64_t)e * NV + j];
+            double G[DIM][NV], detJ;
+            p1_geometry<DIM>(a.coords, nd, G, detJ);
+            double Kbar = 0.0;
+#pragma unroll
+            for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], a.K[nd[j]], Kbar);
+            if (a.Ks_elem) Kbar *= a.Ks_elem[e];
+            const double kd = Kbar * detJ;
+            const double Ml = a.mcoef[li] * detJ;
+            double gli[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) gli[d] = G[d][li];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                double gg = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) gg = fma(gli[d], G[d][j], gg);
+                double v = kd * gg;
+                if (j == li) v += inv_dt * (Ml * Ci);
+                const int kpos = (packed >> (2 + 6 * j)) & 63;
+                acc[kpos * stride] += v;
+            }
+            bsum += -kd * gli[DIM - 1] - inv_dt * (Ml * storage);
+        }
+        rhs_i = bsum;
+        diag = acc[dpos * stride];
+    }
+    a.rhs[i] = rhs_i;
+    if (a.dinv) a.dinv[i] = 1.0 / (diag != 0.0 ? diag : 1.0);
+    const int64_t vb = a.slice_ptr[s] + lane;
+    for (int k = 0; k < width; ++k) {
+        const double v = acc[k * stride];
+        a.vals[vb + (int64_t)kSlice * k] = v;
+        if (a.vals32) a.vals32[vb + (int64_t)kSlice * k] = (float)v;
+    }
+}
+
+// Host-side quadrature constants from the reference rule.
+void quadrature_constants(int dim, const double *Q, const double *W, int nq, double s[4], double m[4]) {
+    const int nv = dim + 1;
+    for (int j = 0; j < 4; ++j) s[j] = m[j] = 0.0;
+    double mass[4][4] = {};
+    for (int q = 0; q < nq; ++q) {
+        double N[4];
+        const double *p = Q + q * dim;
+        if (dim == 2) { N[0] = 1 - p[0] - p[1]; N[1] = p[0]; N[2] = p[1]; }
+        else { N[0] = 1.0 - p[0] - p[1] - p[2]; N[1] = p[0]; N[2] = p[1]; N[3] = p[2]; }
+        for (int i = 0; i < nv; ++i) {
+            s[i] += W[q] * N[i];
+            for (int j = 0; j < nv; ++j) mass[i][j] += W[q] * (N[i] * N[j]);
+        }
+    }
+    for (int i = 0; i < nv; ++i) {
+        double r = 0.0;
+        for (int j = 0; j < nv; ++j) r += mass[i][j];
+        m[i] = r;
+    }
+}
+
+static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_pattern *pat,
+                                         const double *theta_m, const double *theta_n, const double *h_m,
+                                         const double *K, const double *C, const double *Ks_elem,
+                                         const double s[4], const double mc[4], double dt, const double *dt_dev,
+                                         const double *bc_val, double *vals, float *vals32, double *rhs,
+                                         double *dinv, cudaStream_t st) {
+    RichardsAsmArgs a;
+    a.n_rows = pat->n_rows;
+    a.slice_ptr = pat->slice_ptr; a.slice_width = pat->slice_width; a.diag_pos = pat->diag_pos;
+    a.inc_ptr = pat->inc_ptr; a.inc_width = pat->inc_width; a.inc_elem = pat->inc_elem; a.inc_slots = pat->inc_slots;
+    a.conn = mesh->conn; a.coords = mesh->coords;
+    a.theta_m = theta_m; a.theta_n = theta_n; a.h_m = h_m; a.K = K; a.C = C; a.Ks_elem = Ks_elem; a.bc_val = bc_val;
+    for (int j = 0; j < 4; ++j) { a.s[j] = s[j]; a.mcoef[j] = mc[j]; }
+    a.inv_dt = 1.0 / dt;
+    a.dt_dev = dt_dev;
+    a.vals = vals; a.vals32 = vals32; a.rhs = rhs; a.dinv = dinv;
+    const int threads = 128;
+    const int blocks = (pat->n_slices * kSlice + threads - 1) / threads;
+    const size_t smem = (size_t)pat->max_width * threads * sizeof(double);
+    if (mesh->dim == 2) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(richards_rows_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        richards_rows_kernel<2><<<blocks, threads, smem, st>>>(a);
+    } else {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(richards_rows_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        richards_rows_kernel<3><<<blocks, threads, smem, st>>>(a);
+    }
+    return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+}
+
+int launch_richards_assembly(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
+                             const double *theta_n, const double *h_m, const double *K, const double *C,
+                             const double *Ks_elem, const double s[4], const double mc[4], double dt,
+                             const double *bc_val, double *vals, float *vals32, double *rhs, double *dinv,
+                             cudaStream_t st) {
+    return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, s, mc, dt, nullptr,
+                                         bc_val, vals, vals32, rhs, dinv, st);
+}
+
+int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
+                                    const double *theta_n, const double *h_m, const double *K, const double *C,
+                                    const double *Ks_elem, const double s[4], const double mc[4],
+                                    const double *dt_dev, const double *bc_val, double *vals, float *vals32,
+                                    double *rhs, double *dinv, cudaStream_t st) {
+    return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, s, mc, 1.0, dt_dev,
+                                         bc_val, vals, vals32, rhs, dinv, st);
+}
+
+int launch_soil(const SoilParams &sp, const double *h, int64_t n, double *C, double *K, double *theta,
+                cudaStream_t st) {
+    if (n <= 0) return WSPM_OK;
+    int64_t b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    soil_kernel<<<(int)b, 256, 0, st>>>(sp, h, n, C, K, theta);
+    return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+}
+
+}  // namespace wspm

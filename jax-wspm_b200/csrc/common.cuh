@@ -1,0 +1,143 @@
+// Shared device helpers for libwspm (sm_100a).
+//
+// Reductions are deterministic: every block writes its partial sums to a
+// fixed slot, the last block to arrive (atomic ticket, no spinning) sums the
+// slots in slot order and publishes the scalar.  The grid size of every
+// reducing kernel is a fixed function of the problem size, so results are
+// bitwise repeatable run to run.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "wspm.h"
+
+namespace wspm {
+
+constexpr int kSlice = 32;          // SELL slice height == warp size
+constexpr int kBlock = 256;         // threads per block for vector kernels
+constexpr int kMaxPartials = 16384; // partial-sum slots: one block per 256 rows up to 4M rows
+
+// One thread per row (or element) up to kMaxPartials blocks, grid-stride beyond.
+inline int reduction_blocks(int64_t n) {
+    int64_t b = (n + kBlock - 1) / kBlock;
+    if (b < 1) b = 1;
+    if (b > kMaxPartials) b = kMaxPartials;
+    return (int)b;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of NV values per thread; result valid in thread 0.
+template <typename T, int NV>
+__device__ __forceinline__ void block_sum(T (&v)[NV]) {
+    __shared__ T sh[NV][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) sh[j][wid] = v[j];
+    }
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    if (wid == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            T t = lane < nw ? sh[j][lane] : T(0);
+            v[j] = warp_sum(t);
+        }
+    }
+    __syncthreads();
+}
+
+// Publish per-block partials; returns true in exactly one block (the last to
+// finish), whose threads can then read all partials.  `partials` is laid out
+// [NV][gridDim.x].  The ticket is reset by the last block.
+template <typename T, int NV>
+__device__ __forceinline__ bool publish_partials(T (&v)[NV], T *partials, unsigned int *ticket) {
+    __shared__ bool is_last;
+    block_sum<T, NV>(v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) partials[j * gridDim.x + blockIdx.x] = v[j];
+        __threadfence();
+        unsigned int t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// In the last block: fixed-order sum of the partials; result in thread 0.
+// Loads go through L2 (ld.global.cg: the other blocks' stores are visible
+// there after their __threadfence) and are unrolled so many are in flight.
+template <typename T, int NV>
+__device__ __forceinline__ void final_sum(const T *partials, T (&out)[NV], unsigned int *ticket) {
+    const int nb = (int)gridDim.x;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const T *pj = partials + (int64_t)j * nb;
+        T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+        int b = threadIdx.x;
+        const int step = blockDim.x;
+        for (; b + 3 * step < nb; b += 4 * step) {
+            const T x0 = __ldcg(pj + b), x1 = __ldcg(pj + b + step);
+            const T x2 = __ldcg(pj + b + 2 * step), x3 = __ldcg(pj + b + 3 * step);
+            a0 += x0; a1 += x1; a2 += x2; a3 += x3;
+        }
+        for (; b < nb; b += step) a0 += __ldcg(pj + b);
+        out[j] = (a0 + a1) + (a2 + a3);
+    }
+    block_sum<T, NV>(out);
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+__device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
+
+// Row i of a SELL-32 matrix times x, with x supplied by the functor xf(col).
+// MW > 0: all column indices and values of the row are loaded before the
+// gathers and FMAs (memory-level parallelism); requires row width <= MW.
+template <typename T, int MW, typename XF>
+__device__ __forceinline__ T sell_row_dot(const int64_t *__restrict__ slice_ptr, const int32_t *__restrict__ slice_width,
+                                          const int32_t *__restrict__ cols, const T *__restrict__ vals, int i, XF xf) {
+    const int s = i >> 5, lane = i & 31;
+    const int w = __ldg(slice_width + s);
+    const int64_t base = __ldg(slice_ptr + s) + lane;
+    T acc = T(0);
+    if constexpr (MW > 0) {
+        int c[MW];
+        T v[MW];
+#pragma unroll
+        for (int k = 0; k < MW; ++k) {
+            if (k < w) {
+                c[k] = __ldg(cols + base + (int64_t)kSlice * k);
+                v[k] = __ldg(vals + base + (int64_t)kSlice * k);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < MW; ++k)
+            if (k < w) acc = fma(v[k], xf(c[k]), acc);
+    } else {
+        for (int k = 0; k < w; ++k) {
+            const int64_t o = base + (int64_t)kSlice * k;
+            acc = fma(__ldg(vals + o), xf(__ldg(cols + o)), acc);
+        }
+    }
+    return acc;
+}
+
+}  // namespace wspm
+
+#define WSPM_CUDA_TRY(expr)                                   \
+    do {                                                      \
+        cudaError_t _e = (expr);                              \
+        if (_e != cudaSuccess) return WSPM_CUDA_ERROR;        \
+    } while (0)

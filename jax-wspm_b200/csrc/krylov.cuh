@@ -1,0 +1,113 @@
+// Krylov solvers on SELL-32 matrices: declarations shared by krylov.cu,
+// picard.cu and capi.cu.
+#pragma once
+#include "common.cuh"
+
+namespace wspm {
+
+struct Sell {
+    int n_rows;
+    int n_slices;
+    int max_width;
+    const int64_t *slice_ptr;
+    const int32_t *slice_width;
+    const int32_t *cols;
+};
+
+inline Sell make_sell(const wspm_pattern *p) {
+    Sell s;
+    s.n_rows = p->n_rows; s.n_slices = p->n_slices; s.max_width = p->max_width;
+    s.slice_ptr = p->slice_ptr; s.slice_width = p->slice_width; s.cols = p->cols;
+    return s;
+}
+
+// Device-resident solver scalars (one cache line per group).
+struct KrylovState {
+    double gamma, alpha, beta, atol2, bs, rr, pq, rz;      // CG
+    double rho, omega, sigma, ss, ts, tt, rho_next;        // BiCGSTAB
+    double rnorm, ptol, wn0, wn, inv_wn, b_norm, mb_norm;  // GMRES
+    double inner_tol;                                      // refinement: tolerance of the next inner solve
+    int k, done, status, exit_early, broken, steps, pad0, pad1;
+    unsigned int ticket[4];
+};
+
+// Precision-generic CG over one matrix.  Buffers are carved from a workspace.
+template <typename T>
+struct CgBuffers {
+    T *r, *z, *p0, *p1, *q;
+    T *partials;      // [4 * kMaxPartials]
+    KrylovState *st;
+};
+
+// Launch helpers.  `cond`/`use_cond`: CUDA-graph conditional handle set by the
+// last block of the convergence-testing kernel (while-loop continue flag).
+// Rows are processed with their column/value loads issued up front, unrolled
+// to a compile-time width MW (8 for triangle meshes, 16 for tetrahedra, 0 =
+// generic loop); the launch helpers pick MW from the pattern's max width.
+#define WSPM_WIDTH_DISPATCH(maxw, ...)             \
+    do {                                            \
+        if ((maxw) <= 8) {                          \
+            constexpr int MW = 8;                   \
+            __VA_ARGS__;                            \
+        } else if ((maxw) <= 16) {                  \
+            constexpr int MW = 16;                  \
+            __VA_ARGS__;                            \
+        } else {                                    \
+            constexpr int MW = 0;                   \
+            __VA_ARGS__;                            \
+        }                                           \
+    } while (0)
+
+template <typename T>
+void cg_enqueue_init(const Sell &A, const T *vals, const T *b, const double *b64_source,
+                     const T *x0, T *x, const T *dinv, const CgBuffers<T> &w, double tol, double atol,
+                     int maxiter, bool zero_x0, cudaGraphConditionalHandle cond, int use_cond,
+                     cudaStream_t st, const double *tol_dev = nullptr);
+template <typename T>
+void cg_enqueue_body(const Sell &A, const T *vals, T *x, const T *dinv, const CgBuffers<T> &w,
+                     int maxiter, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
+
+struct BicgBuffers {
+    double *r, *rhat, *p, *phat, *q, *t;
+    double *partials;
+    KrylovState *st;
+};
+void bicgstab_enqueue_init(const Sell &A, const double *vals, const double *b, const double *x0, double *x,
+                           const BicgBuffers &w, double tol, double atol, int maxiter,
+                           cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
+void bicgstab_enqueue_body(const Sell &A, const double *vals, const double *b, double *x, const double *dinv,
+                           const BicgBuffers &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
+                           cudaStream_t st);
+
+struct GmresBuffers {
+    double *V;        // [(m+1) * n]
+    double *w;        // [n]
+    double *H;        // [(m+1) * m], column-major by Arnoldi step: H[j*(m+1) + i]
+    double *y;        // [m]
+    double *hbuf;     // [2 * (m+1)]
+    double *partials; // [(m+2) * kMaxPartials]
+    KrylovState *st;
+    int m;
+    int64_t ld;       // leading dimension of V (padded n)
+};
+void gmres_enqueue_init(const Sell &A, const double *vals, const double *b, const double *x0, double *x,
+                        const double *dinv, const GmresBuffers &w, double tol, double atol, int maxiter,
+                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
+void gmres_enqueue_body(const Sell &A, const double *vals, const double *b, double *x, const double *dinv,
+                        const GmresBuffers &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
+                        cudaStream_t st);
+
+// Workspace sizing / carving (in doubles).
+int64_t cg_workspace_doubles(int n, int bytes_per_elem);
+int64_t bicgstab_workspace_doubles(int n);
+int64_t gmres_workspace_doubles(int n, int m);
+template <typename T>
+CgBuffers<T> carve_cg(double *work, int n, int64_t *used);
+BicgBuffers carve_bicgstab(double *work, int n, int64_t *used);
+GmresBuffers carve_gmres(double *work, int n, int m, int64_t *used);
+
+void copy_kernel_d(const double *src, double *dst, int n, cudaStream_t st);
+void spmv_f64(const Sell &A, const double *vals, const double *x, double *y, cudaStream_t st);
+void spmv_f32(const Sell &A, const float *vals, const float *x, float *y, cudaStream_t st);
+
+}  // namespace wspm

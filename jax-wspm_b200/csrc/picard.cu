@@ -1,0 +1,497 @@
+// One implicit Richards time step as a single CUDA graph.
+//
+//   step_init:  theta_n = theta(h_n); h_m = h_n; Picard counters reset
+//   WHILE picard (err >= tol && it < maxit):                richards_solver_v2.py:160-165
+//     soil:       C, K, theta_m at h_m                       :114-115
+//     assembly:   A, b, Dirichlet rows, Jacobi 1/diag        :118-146
+//     Krylov:     FP64 CG | BiCGSTAB | GMRES(m), x0 = h_m    :148-153
+//                 or FP32 CG inside FP64 iterative refinement on the true residual
+//     update:     err = ||x - h_m|| (/ ||x||); h_m = x; it++ :155
+//   step_finish: h_n = h_m, counters to the caller's result words
+//
+// Every loop is a conditional WHILE node whose handle is cleared by the
+// kernel that tests convergence, and every loop has an iteration cap, so
+// the graph always terminates.  The host launches the graph once per time
+// step and never synchronises inside it.
+#include <new>
+#include "krylov.cuh"
+#include "graph.cuh"
+#include "soil.cuh"
+
+namespace wspm {
+
+int launch_soil(const SoilParams &sp, const double *h, int64_t n, double *C, double *K, double *theta,
+                cudaStream_t st);
+void quadrature_constants(int dim, const double *Q, const double *W, int nq, double s[4], double m[4]);
+int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
+                                    const double *theta_n, const double *h_m, const double *K, const double *C,
+                                    const double *Ks_elem, const double s[4], const double mc[4],
+                                    const double *dt_dev, const double *bc_val, double *vals, float *vals32,
+                                    double *rhs, double *dinv, cudaStream_t st);
+
+struct PicardState {
+    double err, tol;
+    int it, maxit, relative, status;
+    int krylov_total, refine_total, krylov_maxiter_hits, last_krylov_status;
+    int bodies;        // Krylov loop bodies executed (launch accounting)
+    int solver;        // WSPM_SOLVER_*
+    int cont;          // 1 while the Picard loop continues (read by the host-driven mode)
+    unsigned int ticket[4];
+};
+
+__global__ void state_reset_kernel(unsigned int *words, int n_words) {
+    for (int i = threadIdx.x; i < n_words; i += blockDim.x) words[i] = 0u;
+}
+
+__global__ void step_init_kernel(SoilParams sp, int n, const double *__restrict__ h_n, double *theta_n, double *h_m,
+                                 PicardState *ps, double tol, int maxit, int relative, int solver,
+                                 cudaGraphConditionalHandle cond, int use_cond) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double c, k, t;
+        const double h = h_n[i];
+        soil_eval(sp, h, c, k, t);
+        theta_n[i] = t;
+        h_m[i] = h;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ps->err = __longlong_as_double(0x7ff0000000000000ULL);  // +inf, like the reference's carry
+        ps->tol = tol; ps->it = 0; ps->maxit = maxit; ps->relative = relative; ps->status = WSPM_OK;
+        ps->krylov_total = 0; ps->refine_total = 0; ps->krylov_maxiter_hits = 0; ps->last_krylov_status = 0;
+        ps->bodies = 0;
+        ps->solver = solver;
+        ps->cont = maxit > 0 ? 1 : 0;
+        for (int j = 0; j < 4; ++j) ps->ticket[j] = 0u;
+        if (use_cond) cudaGraphSetConditional(cond, maxit > 0 ? 1u : 0u);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) picard_update_kernel(int n, const double *__restrict__ x, double *h_m,
+                                                               double *partials, PicardState *ps,
+                                                               const KrylovState *ks, const KrylovState *irs,
+                                                               cudaGraphConditionalHandle cond, int use_cond) {
+    double v[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double xi = x[i];
+        const double d = xi - h_m[i];
+        v[0] += d * d;
+        v[1] += xi * xi;
+        h_m[i] = xi;
+    }
+    if (publish_partials<double, 2>(v, partials, &ps->ticket[0])) {
+        double tot[2];
+        final_sum<double, 2>(partials, tot, &ps->ticket[0]);
+        if (threadIdx.x == 0) {
+            const double dn = sqrt(tot[0]);
+            const double err = ps->relative ? dn / sqrt(tot[1]) : dn;
+            ps->err = err;
+            ps->it += 1;
+            if (irs) {
+                ps->refine_total += irs->k;
+                ps->krylov_total += irs->steps;   // inner iterations accumulated by the refinement loop
+                ps->bodies += irs->pad0;          // inner CG bodies accumulated by the refinement loop
+                ps->last_krylov_status = irs->status;
+            } else {
+                const int kk = ks->k > 0 ? ks->k : 0;
+                ps->krylov_total += kk;
+                // CG bodies hold two iterations; BiCGSTAB one; GMRES bodies are restart cycles
+                ps->bodies += ps->solver == WSPM_SOLVER_CG ? (kk + 1) / 2 : (ps->solver == WSPM_SOLVER_BICGSTAB ? (ks->k < 0 ? 1 : kk) : kk);
+                ps->last_krylov_status = ks->status;
+            }
+            if (ps->last_krylov_status == WSPM_MAXITER) ps->krylov_maxiter_hits += 1;
+            int cont = (err >= ps->tol) && (ps->it < ps->maxit);
+            if (!isfinite(err)) { cont = 0; ps->status = WSPM_NAN; }
+            else if (!cont && err >= ps->tol) ps->status = WSPM_MAXITER;
+            ps->cont = cont;
+            if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+        }
+    }
+}
+
+__global__ void step_finish_kernel(int n, const double *__restrict__ h_m, double *h_n, const PicardState *ps,
+                                   int32_t *result, double *result_f64) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) h_n[i] = h_m[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        result[0] = ps->status;
+        result[1] = ps->it;
+        result[2] = ps->krylov_total;
+        result[3] = ps->refine_total;
+        result[4] = ps->krylov_maxiter_hits;
+        result[5] = ps->last_krylov_status;
+        result[6] = ps->bodies;
+        result_f64[0] = ps->err;
+    }
+}
+
+// ---- mixed precision: FP32 CG corrections inside FP64 refinement ----------
+// ir state (KrylovState): bs, atol2, rr, k (refinement iterations), steps (inner
+// iterations summed), status.
+template <int MW>
+__global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const double *__restrict__ vals,
+                                                             const double *__restrict__ b, const double *x,
+                                                             double *r, const double *__restrict__ dinv,
+                                                             float *dinv32, double *partials, KrylovState *irs,
+                                                             const KrylovState *inner, int is_init, double tol,
+                                                             double inner_floor, int maxit,
+                                                             cudaGraphConditionalHandle cond, int use_cond) {
+    double v[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
+        const double acc = sell_row_dot<double, MW>(A.slice_ptr, A.slice_width, A.cols, vals, i,
+                                                    [&](int c) { return x[c]; });
+        const double ri = b[i] - acc;
+        r[i] = ri;
+        if (is_init && dinv32) dinv32[i] = (float)dinv[i];
+        v[0] += ri * ri;
+        v[1] += b[i] * b[i];
+    }
+    if (publish_partials<double, 2>(v, partials, &irs->ticket[0])) {
+        double tot[2];
+        final_sum<double, 2>(partials, tot, &irs->ticket[0]);
+        if (threadIdx.x == 0) {
+            if (is_init) {
+                irs->bs = tot[1];
+                irs->atol2 = tol * tol * tot[1];
+                irs->k = 0;
+                irs->steps = 0;
+                irs->pad0 = 0;
+                irs->status = WSPM_OK;
+            } else {
+                irs->k += 1;
+                irs->steps += inner->k;
+                irs->pad0 += (inner->k + 1) / 2;
+            }
+            irs->rr = tot[0];
+            // the next FP32 solve aims at the reduction the FP64 residual still needs
+            // (half of it, for margin), never tighter than the floor FP32 can reach
+            const double need = 0.5 * sqrt(irs->atol2 / fmax(tot[0], 1e-300));
+            irs->inner_tol = fmin(0.5, fmax(inner_floor, need));
+            int cont = tot[0] > irs->atol2 && irs->k < maxit;
+            if (!cont && tot[0] > irs->atol2) irs->status = WSPM_MAXITER;
+            if (!isfinite(tot[0])) { cont = 0; irs->status = WSPM_NAN; }
+            irs->done = !cont;
+            if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+        }
+    }
+}
+
+__global__ void ir_correct_kernel(int n, double *x, const float *__restrict__ d) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += (double)d[i];
+}
+
+struct PicardPlan {
+    wspm_mesh mesh;
+    wspm_pattern pat;
+    wspm_picard_desc d;
+    SoilParams sp_field;   // soil for the assembly (Ks = 1 when Ks_elem is given)
+    SoilParams sp_theta;   // soil for theta_n
+    double s[4], mc[4];
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    PicardState *ps = nullptr;
+    double *partials = nullptr;
+    CgBuffers<double> cg64;
+    CgBuffers<float> cg32;
+    BicgBuffers bicg;
+    GmresBuffers gm;
+    KrylovState *irs = nullptr;
+    double *r64 = nullptr;
+    float *x32 = nullptr, *dinv32 = nullptr;
+};
+
+int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
+    const int64_t vec = (n + 31) & ~int64_t(31);
+    int64_t t = 64 + ((sizeof(PicardState) + 7) / 8) + 2 * kMaxPartials + 64;
+    if (mixed) {
+        t += cg_workspace_doubles(n, 4) + 64 + vec /* r64 */ + vec /* x32 + dinv32 as floats */ + 64;
+        t += 64 + ((sizeof(KrylovState) + 7) / 8);
+    } else if (solver == WSPM_SOLVER_BICGSTAB) {
+        t += bicgstab_workspace_doubles(n);
+    } else if (solver == WSPM_SOLVER_GMRES) {
+        t += gmres_workspace_doubles(n, restart);
+    } else {
+        t += cg_workspace_doubles(n, 8);
+    }
+    return t;
+}
+
+static int build_picard_graph(PicardPlan *P) {
+    const wspm_picard_desc &d = P->d;
+    const int n = P->mesh.n_nodes;
+    const Sell A = make_sell(&P->pat);
+    const int nb = reduction_blocks(n);
+    const double *dinv = d.precond == WSPM_PRECOND_JACOBI ? d.dinv : nullptr;
+    cudaStream_t cs;
+    WSPM_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    WSPM_CUDA_TRY(cudaGraphCreate(&g, 0));
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); cudaStreamDestroy(cs); return WSPM_CUDA_ERROR; }
+
+    cudaGraphConditionalHandle hp;
+    e = make_cond_handle(cs, &hp);
+    state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)P->ps->ticket, 4);
+    {
+        KrylovState *sts[4] = {P->cg64.st, P->cg32.st, P->bicg.st, P->gm.st};
+        for (KrylovState *k : sts)
+            if (k) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
+        if (P->irs) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)P->irs, (int)(sizeof(KrylovState) / 4));
+    }
+    step_init_kernel<<<nb, kBlock, 0, cs>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
+                                            d.picard_maxiter, d.picard_relative, d.solver, hp, 1);
+    if (e == cudaSuccess) e = capture_while(cs, hp, [&](cudaStream_t bs) {
+        launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, bs);
+        launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
+                                        P->s, P->mc, d.dt_dev, d.bc_val, d.vals, d.mixed ? d.vals32 : nullptr,
+                                        d.rhs, d.dinv, bs);
+        const KrylovState *ks = nullptr;
+        const KrylovState *irs = nullptr;
+        if (d.mixed) {
+            cudaGraphConditionalHandle hir;
+            make_cond_handle(bs, &hir);
+            copy_kernel_d(d.h_m, d.x, n, bs);
+            WSPM_WIDTH_DISPATCH(A.max_width,
+                                ir_residual_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, d.rhs, d.x, P->r64, d.dinv,
+                                                                              P->dinv32, P->partials, P->irs, P->cg32.st,
+                                                                              1, d.krylov_tol, d.inner_tol,
+                                                                              d.refine_maxiter, hir, 1));
+            capture_while(bs, hir, [&](cudaStream_t ibs) {
+                cudaGraphConditionalHandle hcg;
+                make_cond_handle(ibs, &hcg);
+                const float *dv32 = dinv ? P->dinv32 : nullptr;
+                cg_enqueue_init<float>(A, d.vals32, nullptr, P->r64, P->x32, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
+                                       d.inner_maxiter, true, hcg, 1, ibs, &P->irs->inner_tol);
+                capture_while(ibs, hcg, [&](cudaStream_t cbs) {
+                    cg_enqueue_body<float>(A, d.vals32, P->x32, dv32, P->cg32, d.inner_maxiter, hcg, 1, cbs);
+                });
+                ir_correct_kernel<<<nb, kBlock, 0, ibs>>>(n, d.x, P->x32);
+                WSPM_WIDTH_DISPATCH(A.max_width,
+                                    ir_residual_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, d.rhs, d.x, P->r64,
+                                                                                   d.dinv, nullptr, P->partials,
+                                                                                   P->irs, P->cg32.st, 0,
+                                                                                   d.krylov_tol, d.inner_tol,
+                                                                                   d.refine_maxiter, hir, 1));
+            });
+            irs = P->irs;
+        } else if (d.solver == WSPM_SOLVER_BICGSTAB) {
+            cudaGraphConditionalHandle hk;
+            make_cond_handle(bs, &hk);
+            bicgstab_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, P->bicg, d.krylov_tol, 0.0, d.krylov_maxiter, hk, 1,
+                                  bs);
+            capture_while(bs, hk, [&](cudaStream_t kbs) {
+                bicgstab_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->bicg, d.krylov_maxiter, hk, 1, kbs);
+            });
+            ks = P->bicg.st;
+        } else if (d.solver == WSPM_SOLVER_GMRES) {
+            cudaGraphConditionalHandle hk;
+            make_cond_handle(bs, &hk);
+            gmres_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, dinv, P->gm, d.krylov_tol, 0.0, d.krylov_maxiter, hk, 1,
+                               bs);
+            capture_while(bs, hk, [&](cudaStream_t kbs) {
+                gmres_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->gm, d.krylov_maxiter, hk, 1, kbs);
+            });
+            ks = P->gm.st;
+        } else {
+            cudaGraphConditionalHandle hk;
+            make_cond_handle(bs, &hk);
+            cg_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, dinv, P->cg64, d.krylov_tol, 0.0,
+                                    d.krylov_maxiter, false, hk, 1, bs);
+            capture_while(bs, hk, [&](cudaStream_t kbs) {
+                cg_enqueue_body<double>(A, d.vals, d.x, dinv, P->cg64, d.krylov_maxiter, hk, 1, kbs);
+            });
+            ks = P->cg64.st;
+        }
+        picard_update_kernel<<<nb, kBlock, 0, bs>>>(n, d.x, d.h_m, P->partials, P->ps, ks, irs, hp, 1);
+    });
+    step_finish_kernel<<<nb, kBlock, 0, cs>>>(n, d.h_m, d.h_n, P->ps, d.result, d.result_f64);
+    cudaGraph_t out = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(cs, &out);
+    cudaStreamDestroy(cs);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return WSPM_CUDA_ERROR; }
+    e = cudaGraphInstantiate(&P->exec, g, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return WSPM_CUDA_ERROR; }
+    P->graph = g;
+    return WSPM_OK;
+}
+
+// Host-driven variant of the same step: identical kernels, loop control from
+// the host (bounded loops that read the device's done/cont words).  Used when
+// a tool cannot follow conditional graph nodes (ncu profiles no kernel node
+// of such graphs) and as a fallback.
+static int read_flag(const int *dev_word, cudaStream_t st, int *out, int *pinned) {
+    WSPM_CUDA_TRY(cudaMemcpyAsync(pinned, dev_word, sizeof(int), cudaMemcpyDeviceToHost, st));
+    WSPM_CUDA_TRY(cudaStreamSynchronize(st));
+    *out = *pinned;
+    return WSPM_OK;
+}
+
+static int picard_step_host(PicardPlan *P, cudaStream_t st) {
+    const wspm_picard_desc &d = P->d;
+    const int n = P->mesh.n_nodes;
+    const Sell A = make_sell(&P->pat);
+    const int nb = reduction_blocks(n);
+    const double *dinv = d.precond == WSPM_PRECOND_JACOBI ? d.dinv : nullptr;
+    const cudaGraphConditionalHandle none = cudaGraphConditionalHandle();
+    int *pinned = nullptr;
+    WSPM_CUDA_TRY(cudaMallocHost(&pinned, sizeof(int)));
+    int rc = WSPM_OK, flag = 0;
+    constexpr int kChunk = 8;
+    state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)P->ps->ticket, 4);
+    KrylovState *sts[5] = {P->cg64.st, P->cg32.st, P->bicg.st, P->gm.st, P->irs};
+    for (KrylovState *k : sts)
+        if (k) state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
+    step_init_kernel<<<nb, kBlock, 0, st>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
+                                            d.picard_maxiter, d.picard_relative, d.solver, none, 0);
+    for (int it = 0; it < d.picard_maxiter && rc == WSPM_OK; ++it) {
+        launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, st);
+        launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem, P->s,
+                                        P->mc, d.dt_dev, d.bc_val, d.vals, d.mixed ? d.vals32 : nullptr, d.rhs,
+                                        d.dinv, st);
+        const KrylovState *ks = nullptr, *irs = nullptr;
+        if (d.mixed) {
+            copy_kernel_d(d.h_m, d.x, n, st);
+            WSPM_WIDTH_DISPATCH(A.max_width,
+                                ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.x, P->r64, d.dinv,
+                                                                              P->dinv32, P->partials, P->irs,
+                                                                              P->cg32.st, 1, d.krylov_tol, d.inner_tol,
+                                                                              d.refine_maxiter, none, 0));
+            const float *dv32 = dinv ? P->dinv32 : nullptr;
+            for (int r = 0; r <= d.refine_maxiter && rc == WSPM_OK; ++r) {
+                if ((rc = read_flag(&P->irs->done, st, &flag, pinned)) != WSPM_OK || flag) break;
+                cg_enqueue_init<float>(A, d.vals32, nullptr, P->r64, P->x32, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
+                                       d.inner_maxiter, true, none, 0, st, &P->irs->inner_tol);
+                for (int b = 0; b < (d.inner_maxiter + 1) / 2 + 1; b += kChunk) {
+                    if ((rc = read_flag(&P->cg32.st->done, st, &flag, pinned)) != WSPM_OK || flag) break;
+                    for (int c = 0; c < kChunk; ++c)
+                        cg_enqueue_body<float>(A, d.vals32, P->x32, dv32, P->cg32, d.inner_maxiter, none, 0, st);
+                }
+                ir_correct_kernel<<<nb, kBlock, 0, st>>>(n, d.x, P->x32);
+                WSPM_WIDTH_DISPATCH(A.max_width,
+                                    ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.x, P->r64,
+                                                                                  d.dinv, nullptr, P->partials, P->irs,
+                                                                                  P->cg32.st, 0, d.krylov_tol,
+                                                                                  d.inner_tol, d.refine_maxiter, none,
+                                                                                  0));
+            }
+            irs = P->irs;
+        } else {
+            KrylovState *kst = nullptr;
+            int max_bodies = d.krylov_maxiter;
+            if (d.solver == WSPM_SOLVER_BICGSTAB) {
+                bicgstab_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, P->bicg, d.krylov_tol, 0.0, d.krylov_maxiter, none,
+                                      0, st);
+                kst = P->bicg.st;
+            } else if (d.solver == WSPM_SOLVER_GMRES) {
+                gmres_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, dinv, P->gm, d.krylov_tol, 0.0, d.krylov_maxiter,
+                                   none, 0, st);
+                kst = P->gm.st;
+            } else {
+                cg_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, dinv, P->cg64, d.krylov_tol, 0.0,
+                                        d.krylov_maxiter, false, none, 0, st);
+                kst = P->cg64.st;
+                max_bodies = (d.krylov_maxiter + 1) / 2;
+            }
+            for (int b = 0; b < max_bodies + 1 && rc == WSPM_OK; b += kChunk) {
+                if ((rc = read_flag(&kst->done, st, &flag, pinned)) != WSPM_OK || flag) break;
+                for (int c = 0; c < kChunk; ++c) {
+                    if (d.solver == WSPM_SOLVER_BICGSTAB)
+                        bicgstab_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->bicg, d.krylov_maxiter, none, 0, st);
+                    else if (d.solver == WSPM_SOLVER_GMRES)
+                        gmres_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->gm, d.krylov_maxiter, none, 0, st);
+                    else
+                        cg_enqueue_body<double>(A, d.vals, d.x, dinv, P->cg64, d.krylov_maxiter, none, 0, st);
+                }
+            }
+            ks = kst;
+        }
+        picard_update_kernel<<<nb, kBlock, 0, st>>>(n, d.x, d.h_m, P->partials, P->ps, ks, irs, none, 0);
+        if (rc == WSPM_OK && (rc = read_flag(&P->ps->cont, st, &flag, pinned)) == WSPM_OK && !flag) break;
+    }
+    step_finish_kernel<<<nb, kBlock, 0, st>>>(n, d.h_m, d.h_n, P->ps, d.result, d.result_f64);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFreeHost(pinned);
+    if (rc == WSPM_OK && (e != cudaSuccess || cudaGetLastError() != cudaSuccess)) rc = WSPM_CUDA_ERROR;
+    return rc;
+}
+
+}  // namespace wspm
+
+using namespace wspm;
+
+extern "C" int wspm_picard_step_host(void *plan, void *stream) {
+    if (!plan) return WSPM_BAD_ARG;
+    return picard_step_host((PicardPlan *)plan, (cudaStream_t)stream);
+}
+
+extern "C" int64_t wspm_picard_workspace_doubles(int32_t n_rows, int32_t mixed) {
+    // sized for the largest solver choice so that one buffer fits any plan
+    int64_t a = picard_workspace_doubles(n_rows, mixed, WSPM_SOLVER_GMRES, 32);
+    int64_t b = picard_workspace_doubles(n_rows, mixed, WSPM_SOLVER_BICGSTAB, 0);
+    int64_t c = picard_workspace_doubles(n_rows, mixed, WSPM_SOLVER_CG, 0);
+    return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
+
+extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out) {
+    if (!desc || !plan_out || !desc->mesh || !desc->pat) return WSPM_BAD_ARG;
+    const wspm_picard_desc &d = *desc;
+    const int n = d.mesh->n_nodes;
+    if (n <= 0 || d.pat->n_rows != n || d.nq <= 0 || d.nq > 16) return WSPM_BAD_ARG;
+    if (d.mesh->dim != 2 && d.mesh->dim != 3) return WSPM_BAD_ARG;
+    if (!d.h_n || !d.theta_n || !d.h_m || !d.x || !d.K || !d.C || !d.theta_m || !d.vals || !d.rhs || !d.dinv ||
+        !d.work || !d.dt_dev || !d.result || !d.result_f64)
+        return WSPM_BAD_ARG;
+    if (d.mixed && !d.vals32) return WSPM_BAD_ARG;
+    if (d.mixed && d.solver != WSPM_SOLVER_CG) return WSPM_UNSUPPORTED;
+    if (d.solver == WSPM_SOLVER_GMRES && (d.restart < 1 || d.restart > 32)) return WSPM_UNSUPPORTED;
+    if (d.solver < WSPM_SOLVER_CG || d.solver > WSPM_SOLVER_GMRES) return WSPM_BAD_ARG;
+    if (d.work_doubles < wspm_picard_workspace_doubles(n, d.mixed)) return WSPM_BAD_ARG;
+    PicardPlan *P = new (std::nothrow) PicardPlan();
+    if (!P) return WSPM_BAD_ARG;
+    P->mesh = *d.mesh;
+    P->pat = *d.pat;
+    P->d = d;
+    P->d.mesh = &P->mesh;
+    P->d.pat = &P->pat;
+    P->sp_field.model = d.soil_model;
+    P->sp_theta.model = d.soil_model;
+    for (int j = 0; j < 6; ++j) P->sp_field.p[j] = P->sp_theta.p[j] = d.phi[j];
+    quadrature_constants(d.mesh->dim, d.quad_points, d.weights, d.nq, P->s, P->mc);
+    // carve the workspace
+    double *p = d.work;
+    P->ps = (PicardState *)p; p += 64;
+    P->partials = p; p += 2 * kMaxPartials + 64;
+    int64_t used = 0;
+    if (d.mixed) {
+        P->cg32 = carve_cg<float>(p, n, &used); p += used + 64;
+        const int64_t vec = (n + 31) & ~int64_t(31);
+        P->r64 = p; p += vec;
+        P->x32 = (float *)p; P->dinv32 = (float *)p + vec; p += vec + 64;
+        P->irs = (KrylovState *)p; p += 64 + ((sizeof(KrylovState) + 7) / 8);
+    } else if (d.solver == WSPM_SOLVER_BICGSTAB) {
+        P->bicg = carve_bicgstab(p, n, &used); p += used;
+    } else if (d.solver == WSPM_SOLVER_GMRES) {
+        const int m = d.restart < n ? d.restart : n;
+        P->gm = carve_gmres(p, n, m, &used); p += used;
+    } else {
+        P->cg64 = carve_cg<double>(p, n, &used); p += used;
+    }
+    int rc = build_picard_graph(P);
+    if (rc != WSPM_OK) { delete P; return rc; }
+    *plan_out = P;
+    return WSPM_OK;
+}
+
+extern "C" int wspm_picard_step(void *plan, void *stream) {
+    if (!plan) return WSPM_BAD_ARG;
+    PicardPlan *P = (PicardPlan *)plan;
+    WSPM_CUDA_TRY(cudaGraphLaunch(P->exec, (cudaStream_t)stream));
+    return WSPM_OK;
+}
+
+extern "C" int wspm_picard_destroy(void *plan) {
+    if (!plan) return WSPM_OK;
+    PicardPlan *P = (PicardPlan *)plan;
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    delete P;
+    return WSPM_OK;
+}

@@ -1,0 +1,114 @@
+"""ctypes binding of libwspm.so (declarations mirror include/wspm.h).
+
+Importing this module loads the CUDA library built in-tree next to it.  There
+is no fallback: if the library is missing or fails to load, the import raises
+``RuntimeError`` so a GPU run can never silently compute on the host.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwspm.so")
+
+WSPM_OK, WSPM_MAXITER, WSPM_NAN, WSPM_BREAKDOWN = 0, 1, 2, 3
+WSPM_BAD_ARG, WSPM_CUDA_ERROR, WSPM_UNSUPPORTED = 10, 11, 12
+SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2}
+PRECONDS = {"none": 0, None: 0, "jacobi": 1}
+SOIL_VG, SOIL_EXP = 0, 1
+
+c_int32, c_int64, c_double, c_void_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class WspmMesh(ctypes.Structure):
+    _fields_ = [("n_nodes", c_int32), ("n_elems", c_int32), ("dim", c_int32), ("nv", c_int32),
+                ("conn", c_void_p), ("coords", c_void_p)]
+
+
+class WspmPattern(ctypes.Structure):
+    _fields_ = [("n_rows", c_int32), ("n_slices", c_int32), ("max_width", c_int32), ("max_inc", c_int32),
+                ("nnz_padded", c_int64),
+                ("slice_ptr", c_void_p), ("slice_width", c_void_p), ("cols", c_void_p), ("diag_pos", c_void_p),
+                ("inc_ptr", c_void_p), ("inc_width", c_void_p), ("inc_elem", c_void_p), ("inc_slots", c_void_p)]
+
+
+class WspmPicardDesc(ctypes.Structure):
+    _fields_ = [("mesh", ctypes.POINTER(WspmMesh)), ("pat", ctypes.POINTER(WspmPattern)),
+                ("soil_model", c_int32), ("phi", c_double * 6), ("Ks_elem", c_void_p), ("bc_val", c_void_p),
+                ("quad_points", c_double * 48), ("weights", c_double * 16), ("nq", c_int32),
+                ("solver", c_int32), ("precond", c_int32), ("krylov_tol", c_double), ("krylov_maxiter", c_int32),
+                ("restart", c_int32),
+                ("mixed", c_int32), ("inner_tol", c_double), ("inner_maxiter", c_int32), ("refine_maxiter", c_int32),
+                ("picard_tol", c_double), ("picard_maxiter", c_int32), ("picard_relative", c_int32),
+                ("h_n", c_void_p), ("theta_n", c_void_p), ("h_m", c_void_p), ("x", c_void_p),
+                ("K", c_void_p), ("C", c_void_p), ("theta_m", c_void_p),
+                ("vals", c_void_p), ("vals32", c_void_p), ("rhs", c_void_p), ("dinv", c_void_p),
+                ("work", c_void_p), ("work_doubles", c_int64), ("dt_dev", c_void_p),
+                ("result", c_void_p), ("result_f64", c_void_p)]
+
+
+P = ctypes.POINTER
+_SIGS = {
+    "wspm_soil_van_genuchten": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_soil_exponential": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_assemble_richards": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p,
+                                         c_void_p, c_void_p, P(c_double), P(c_double), c_int32, c_double, c_void_p,
+                                         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_spmv_f64": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_spmv_f32": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_apply_dirichlet": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
+    "wspm_jacobi_dinv": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p]),
+    "wspm_krylov_workspace_doubles": (c_int64, [c_int32, c_int32, c_int32]),
+    "wspm_krylov_solve": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,
+                                    c_double, c_int32, c_int32, c_void_p, c_int64, c_void_p, c_void_p]),
+    "wspm_cg_iterations": (c_int32, [P(WspmPattern), c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
+                                     c_void_p, c_int64, c_void_p]),
+    "wspm_picard_workspace_doubles": (c_int64, [c_int32, c_int32]),
+    "wspm_picard_create": (c_int32, [P(WspmPicardDesc), P(c_void_p)]),
+    "wspm_picard_step": (c_int32, [c_void_p, c_void_p]),
+    "wspm_picard_step_host": (c_int32, [c_void_p, c_void_p]),
+    "wspm_picard_destroy": (c_int32, [c_void_p]),
+    "wspm_version": (ctypes.c_char_p, []),
+    "wspm_status_string": (ctypes.c_char_p, [c_int32]),
+}
+EXPORTED = tuple(_SIGS)
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libwspm.so not built at {LIB_PATH}; run __graft_entry__.build() "
+                           "or python jax-wspm_b200/wspm_b200/build.py")
+    try:
+        lib = ctypes.CDLL(LIB_PATH)
+    except OSError as e:
+        raise RuntimeError(f"failed to load {LIB_PATH}: {e}") from e
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+class WspmError(RuntimeError):
+    def __init__(self, fn, code):
+        msg = lib.wspm_status_string(code).decode()
+        super().__init__(f"{fn} failed: {msg} (status {code})")
+        self.code = code
+
+
+def check(fn, code):
+    if code != WSPM_OK:
+        raise WspmError(fn, code)
+    return code
+
+
+def dptr(t):
+    """Device address of a torch tensor (or None -> NULL)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def dbl_array(values):
+    arr = (c_double * max(len(values), 1))(*[float(v) for v in values])
+    return arr

@@ -1,0 +1,221 @@
+"""Device-resident mesh + pattern and thin tensor wrappers of the C ABI.
+
+``DeviceMesh`` uploads a mesh and its SELL-32 pattern once (torch tensors on
+the current CUDA device) and keeps the ``wspm_mesh`` / ``wspm_pattern``
+structs that the C ABI reads.  The functions below take and return torch
+tensors and call libwspm.so on the current torch stream; they never copy
+data to the host.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, dptr, lib
+from .pattern import Pattern
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _require_cuda(t, dtype, name, numel=None):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if numel is not None and t.numel() != numel:
+        raise ValueError(f"{name} must have {numel} elements, got {t.numel()}")
+    return t
+
+
+class DeviceMesh:
+    """Mesh + pattern on the GPU.  ``points`` (N, dim) float64, ``elements`` (E, dim+1)."""
+
+    def __init__(self, points, elements, device=None, pattern=None):
+        points = np.ascontiguousarray(points, dtype=np.float64)
+        elements = np.ascontiguousarray(elements, dtype=np.int64)
+        if elements.ndim != 2 or elements.shape[1] != points.shape[1] + 1:
+            raise ValueError("elements must have dim+1 columns")
+        if elements.size and (elements.min() < 0 or elements.max() >= points.shape[0]):
+            raise ValueError("Element indices out of bounds")
+        self.device = torch.device(device if device is not None else "cuda")
+        self.points_host, self.elements_host = points, elements
+        self.n_nodes, self.dim = points.shape
+        self.n_elems, self.nv = elements.shape
+        self.pattern = pattern if pattern is not None else Pattern(elements, self.n_nodes)
+        pat = self.pattern
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+        self.conn = t(elements.astype(np.int32))
+        self.coords = t(points)
+        self.slice_ptr = t(pat.slice_ptr)
+        self.slice_width = t(pat.slice_width)
+        self.cols = t(pat.cols)
+        self.diag_pos = t(pat.diag_pos)
+        self.inc_ptr = t(pat.inc_ptr)
+        self.inc_width = t(pat.inc_width)
+        self.inc_elem = t(pat.inc_elem)
+        self.inc_slots = t(pat.inc_slots.view(np.int32))
+        self.sell_index = t(pat.sell_index)
+        self.c_mesh = _lib.WspmMesh(self.n_nodes, self.n_elems, self.dim, self.nv, self.conn.data_ptr(),
+                                    self.coords.data_ptr())
+        self.c_pat = _lib.WspmPattern(pat.n_rows, pat.n_slices, pat.max_width, pat.max_inc, pat.nnz_padded,
+                                      self.slice_ptr.data_ptr(), self.slice_width.data_ptr(), self.cols.data_ptr(),
+                                      self.diag_pos.data_ptr(), self.inc_ptr.data_ptr(),
+                                      self.inc_width.data_ptr(), self.inc_elem.data_ptr(),
+                                      self.inc_slots.data_ptr())
+
+    @property
+    def nnz_padded(self):
+        return self.pattern.nnz_padded
+
+    def empty_vals(self, dtype=torch.float64):
+        return torch.empty(self.pattern.nnz_padded, dtype=dtype, device=self.device)
+
+    def vec(self, fill=None, dtype=torch.float64):
+        if fill is None:
+            return torch.empty(self.n_nodes, dtype=dtype, device=self.device)
+        return torch.full((self.n_nodes,), float(fill), dtype=dtype, device=self.device)
+
+
+class SparseMatrix:
+    """Global matrix in SELL-32 form on the GPU (drop-in for the reference's BCOO)."""
+
+    def __init__(self, dmesh, vals):
+        self.dmesh = dmesh
+        self.vals = vals
+        self.shape = (dmesh.n_nodes, dmesh.n_nodes)
+
+    @property
+    def nse(self):
+        return self.dmesh.pattern.nnz
+
+    def __matmul__(self, x):
+        return spmv(self.dmesh, self.vals, x)
+
+    def csr_values(self):
+        return self.vals[self.dmesh.sell_index]
+
+    def to_scipy(self):
+        return self.dmesh.pattern.to_scipy(self.vals.detach().cpu().numpy())
+
+    def todense(self):
+        return torch.from_numpy(self.to_scipy().toarray())
+
+    def diagonal(self):
+        return jacobi_dinv(self.dmesh, self.vals).reciprocal()
+
+
+# ---------------------------------------------------------------- soil
+def soil(model, h, phi):
+    """(C, K, theta) on the device; model "vg" (6 params) or "exp" (4 params)."""
+    _require_cuda(h, torch.float64, "h")
+    C, K, th = torch.empty_like(h), torch.empty_like(h), torch.empty_like(h)
+    arr = _lib.dbl_array(phi)
+    if model == "vg":
+        fn = lib.wspm_soil_van_genuchten
+    elif model == "exp":
+        fn = lib.wspm_soil_exponential
+    else:
+        raise ValueError(f"unknown soil model {model!r}")
+    check("soil", fn(dptr(h), h.numel(), arr, dptr(C), dptr(K), dptr(th), _stream()))
+    return C, K, th
+
+
+# ---------------------------------------------------------------- assembly
+def assemble_richards(dm, theta_m, theta_n, h_m, K, C, quad_points, weights, dt, bc_val=None, Ks_elem=None,
+                      want_f32=False, want_dinv=True):
+    """(vals, rhs, dinv, vals32) of the Richards system (Dirichlet rows fused when bc_val is given)."""
+    n = dm.n_nodes
+    for name, t in (("theta_m", theta_m), ("theta_n", theta_n), ("h_m", h_m), ("K", K), ("C", C)):
+        _require_cuda(t, torch.float64, name, n)
+    if bc_val is not None:
+        _require_cuda(bc_val, torch.float64, "bc_val", n)
+    if Ks_elem is not None:
+        _require_cuda(Ks_elem, torch.float64, "Ks_elem", dm.n_elems)
+    q = np.ascontiguousarray(quad_points, dtype=np.float64).ravel()
+    w = np.ascontiguousarray(weights, dtype=np.float64).ravel()
+    vals = dm.empty_vals()
+    vals32 = dm.empty_vals(torch.float32) if want_f32 else None
+    rhs = dm.vec()
+    dinv = dm.vec() if want_dinv else None
+    check("assemble_richards", lib.wspm_assemble_richards(
+        ctypes.byref(dm.c_mesh), ctypes.byref(dm.c_pat), dptr(theta_m), dptr(theta_n), dptr(h_m), dptr(K), dptr(C),
+        dptr(Ks_elem), _lib.dbl_array(q), _lib.dbl_array(w), len(w), float(dt), dptr(bc_val), dptr(vals),
+        dptr(vals32), dptr(rhs), dptr(dinv), _stream()))
+    return vals, rhs, dinv, vals32
+
+
+def spmv(dm, vals, x):
+    if vals.dtype == torch.float64:
+        _require_cuda(x, torch.float64, "x", dm.n_nodes)
+        y = torch.empty_like(x)
+        check("spmv_f64", lib.wspm_spmv_f64(ctypes.byref(dm.c_pat), dptr(vals), dptr(x), dptr(y), _stream()))
+    else:
+        _require_cuda(x, torch.float32, "x", dm.n_nodes)
+        y = torch.empty_like(x)
+        check("spmv_f32", lib.wspm_spmv_f32(ctypes.byref(dm.c_pat), dptr(vals), dptr(x), dptr(y), _stream()))
+    return y
+
+
+def jacobi_dinv(dm, vals):
+    dinv = dm.vec()
+    check("jacobi_dinv", lib.wspm_jacobi_dinv(ctypes.byref(dm.c_pat), dptr(vals), dptr(dinv), _stream()))
+    return dinv
+
+
+def merge_dirichlet(n, sets):
+    """Merge (nodes, values) sets applied in order; later sets win (boundary.py:38-53 order)."""
+    val = np.full(n, np.nan)
+    for nodes, v in sets:
+        nodes = np.asarray(nodes, dtype=np.int64)
+        val[nodes] = np.broadcast_to(np.asarray(v, dtype=np.float64), nodes.shape)
+    return val
+
+
+def apply_dirichlet(dm, nodes, values, vals, rhs):
+    """In place: rows ``nodes`` -> e_i, rhs[nodes] = values (nodes unique)."""
+    nodes_t = torch.as_tensor(np.asarray(nodes, dtype=np.int32), device=dm.device)
+    vals_t = torch.as_tensor(np.asarray(values, dtype=np.float64), device=dm.device)
+    if torch.unique(nodes_t).numel() != nodes_t.numel():
+        raise ValueError("Dirichlet nodes must be unique; merge overlapping sets first")
+    check("apply_dirichlet", lib.wspm_apply_dirichlet(ctypes.byref(dm.c_pat), dptr(nodes_t), dptr(vals_t),
+                                                      nodes_t.numel(), dptr(vals), dptr(rhs), _stream()))
+    return vals, rhs
+
+
+class KrylovWorkspace:
+    """Reusable device workspace for stand-alone solves (keeps solve graphs cached)."""
+
+    def __init__(self, dm):
+        self.dm = dm
+        self.buffers = {}
+        self.result = torch.zeros(4, dtype=torch.int32, device=dm.device)
+
+    def get(self, solver, restart):
+        key = (solver, restart if solver == "gmres" else 0)
+        if key not in self.buffers:
+            need = lib.wspm_krylov_workspace_doubles(self.dm.n_nodes, _lib.SOLVERS[solver], int(restart))
+            if need < 0:
+                raise ValueError(f"unsupported Krylov configuration {solver} restart={restart}")
+            self.buffers[key] = torch.empty(int(need), dtype=torch.float64, device=self.dm.device)
+        return self.buffers[key]
+
+
+def krylov_solve(dm, vals, b, x0, solver="cg", dinv=None, tol=1e-10, atol=0.0, maxiter=100, restart=30,
+                 workspace=None, x_out=None):
+    """Solve A x = b from x0 on the device; returns (x, status_tensor[4] on device)."""
+    if solver not in _lib.SOLVERS:
+        raise ValueError(f"Unsupported solver type: {solver}")
+    _require_cuda(b, torch.float64, "b", dm.n_nodes)
+    ws = workspace if workspace is not None else KrylovWorkspace(dm)
+    work = ws.get(solver, restart)
+    x = x_out if x_out is not None else torch.empty_like(b)
+    x.copy_(x0)
+    check("krylov_solve", lib.wspm_krylov_solve(
+        ctypes.byref(dm.c_pat), dptr(vals), dptr(b), dptr(x), dptr(dinv), _lib.SOLVERS[solver], float(tol),
+        float(atol), int(maxiter), int(restart), dptr(work), work.numel(), dptr(ws.result), _stream()))
+    return x, ws.result

@@ -1,0 +1,111 @@
+"""Sparsity pattern of the P1 global matrix in SELL-32 layout (host, NumPy).
+
+Built once per mesh.  Replaces the reference's per-iteration COO fill +
+``BCOO.sum_duplicates`` (src/numerics/assembly_re_v2.py:114-152): the
+pattern (which node pairs share an element) never changes, so it is derived
+once and every assembly writes values straight into fixed slots.
+
+Layout (all int arrays little-endian, ready for device upload):
+  rows are grouped in slices of 32; slice s has width w_s = max row length in
+  the slice; entry k of row i is at slice_ptr[i//32] + 32*k + i%32.  Columns
+  of a row are ascending; padding entries point at the row itself.
+  The node -> element incidence uses the same sliced layout; each incidence
+  packs the local vertex of the row's node (2 bits) and, for every vertex j
+  of the element, the position of that vertex's column in the row (6 bits).
+"""
+import numpy as np
+
+SLICE = 32
+
+
+class Pattern:
+    """Host arrays of a SELL-32 pattern + node->element incidence."""
+
+    def __init__(self, elements, n_nodes):
+        el = np.ascontiguousarray(elements, dtype=np.int64)
+        E, nv = el.shape
+        N = int(n_nodes)
+        self.n_rows, self.n_elems, self.nv = N, E, nv
+        # --- unique (row, col) pairs, ascending
+        rows = np.repeat(el, nv, axis=1).ravel()
+        cols = np.tile(el, (1, nv)).ravel()
+        keys = np.unique(rows * N + cols)
+        r = keys // N
+        c = keys - r * N
+        counts = np.bincount(r, minlength=N)
+        if np.any(counts == 0):
+            raise ValueError("mesh has nodes that belong to no element")
+        rowptr = np.zeros(N + 1, dtype=np.int64)
+        np.cumsum(counts, out=rowptr[1:])
+        self.csr_indptr, self.csr_indices = rowptr, c.astype(np.int32)
+        self.nnz = int(keys.size)
+        pos = np.arange(keys.size, dtype=np.int64) - rowptr[r]
+        # --- slices
+        ns = (N + SLICE - 1) // SLICE
+        self.n_slices = ns
+        pad_counts = np.zeros(ns * SLICE, dtype=np.int64)
+        pad_counts[:N] = counts
+        width = pad_counts.reshape(ns, SLICE).max(axis=1)
+        if width.max() > 63:
+            raise ValueError("row length above 63 is not supported by the SELL-32 kernels")
+        self.slice_width = width.astype(np.int32)
+        self.slice_ptr = np.zeros(ns + 1, dtype=np.int64)
+        np.cumsum(width * SLICE, out=self.slice_ptr[1:])
+        self.nnz_padded = int(self.slice_ptr[-1])
+        self.max_width = int(width.max())
+        lane = r % SLICE
+        self.sell_index = self.slice_ptr[r // SLICE] + SLICE * pos + lane      # CSR entry -> SELL slot
+        sell_cols = np.empty(self.nnz_padded, dtype=np.int32)
+        # padding: column = own row
+        all_rows = np.arange(ns * SLICE, dtype=np.int64)
+        for_pad = np.minimum(all_rows, N - 1)
+        slot_row = np.repeat(for_pad.reshape(ns, SLICE), width, axis=0)      # (sum w, 32)
+        sell_cols[:] = slot_row.ravel().astype(np.int32)
+        sell_cols[self.sell_index] = c.astype(np.int32)
+        self.cols = sell_cols
+        self.diag_pos = np.empty(N, dtype=np.int32)
+        dmask = r == c
+        self.diag_pos[r[dmask]] = pos[dmask].astype(np.int32)
+        # --- incidence: for each (node, element) in ascending element order
+        inc_node = el.ravel()
+        inc_elem = np.repeat(np.arange(E, dtype=np.int64), nv)
+        inc_li = np.tile(np.arange(nv, dtype=np.int64), E)
+        order = np.lexsort((inc_elem, inc_node))
+        inc_node, inc_elem, inc_li = inc_node[order], inc_elem[order], inc_li[order]
+        deg = np.bincount(inc_node, minlength=N)
+        dptr = np.zeros(N + 1, dtype=np.int64)
+        np.cumsum(deg, out=dptr[1:])
+        ipos = np.arange(inc_node.size, dtype=np.int64) - dptr[inc_node]
+        pad_deg = np.zeros(ns * SLICE, dtype=np.int64)
+        pad_deg[:N] = deg
+        iwidth = pad_deg.reshape(ns, SLICE).max(axis=1)
+        self.inc_width = iwidth.astype(np.int32)
+        self.inc_ptr = np.zeros(ns + 1, dtype=np.int64)
+        np.cumsum(iwidth * SLICE, out=self.inc_ptr[1:])
+        self.max_inc = int(iwidth.max())
+        islot = self.inc_ptr[inc_node // SLICE] + SLICE * ipos + inc_node % SLICE
+        inc_e = np.full(int(self.inc_ptr[-1]), -1, dtype=np.int32)
+        inc_e[islot] = inc_elem.astype(np.int32)
+        packed = inc_li.astype(np.uint32)
+        node_rows = inc_node
+        for j in range(nv):
+            colj = el[inc_elem, j]
+            kj = np.searchsorted(keys, node_rows * N + colj) - rowptr[node_rows]
+            packed |= (kj.astype(np.uint32) & 63) << np.uint32(2 + 6 * j)
+        inc_s = np.zeros(int(self.inc_ptr[-1]), dtype=np.uint32)
+        inc_s[islot] = packed
+        self.inc_elem, self.inc_slots = inc_e, inc_s
+
+    # ---- conversions used by tests and by the reference-API shims ----------
+    def sell_from_csr_values(self, data):
+        out = np.zeros(self.nnz_padded, dtype=np.asarray(data).dtype)
+        out[self.sell_index] = data
+        return out
+
+    def csr_values_from_sell(self, vals):
+        return np.asarray(vals)[self.sell_index]
+
+    def to_scipy(self, vals):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.csr_values_from_sell(vals), self.csr_indices, self.csr_indptr),
+                             shape=(self.n_rows, self.n_rows))

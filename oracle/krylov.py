@@ -124,7 +124,8 @@ def gmres(A, b, x0, tol=1e-10, atol=0.0, restart=30, maxiter=100, dinv=None):
     b_norm = float(np.sqrt(b @ b))
     atol_eff = max(tol * b_norm, atol)
     Mb_norm = float(np.sqrt(M(b) @ M(b)))
-    ptol = Mb_norm * min(1.0, atol_eff / b_norm) if b_norm > 0 else 0.0
+    # jnp.minimum propagates NaN: b == 0 gives a NaN tolerance and no iterations
+    ptol = Mb_norm * min(1.0, atol_eff / b_norm) if b_norm > 0 else float('nan')
     x = np.array(x0, dtype=np.float64, copy=True)
     unit, rnorm = _safe_normalize(M(b - matvec(x)))
     eps = np.finfo(np.float64).eps

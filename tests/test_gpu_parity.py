@@ -1,0 +1,310 @@
+"""Parity of the CUDA path (libwspm.so through the C ABI) with the oracle.
+
+Tolerances: element/assembly values and SpMV are compared to 1e-13 relative
+(to the largest entry); Krylov solutions, which differ from the oracle's only
+by summation order, to a few times the solver tolerance; whole Picard runs
+against the reference's own goldens (CSV metrics 5e-4 relative, Picard
+iteration totals exactly; Test3D npz fields 1e-8 relative).
+"""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from oracle import analytic, assembly as oasm, krylov as okry, picard as opic, soil as osoil  # noqa: E402
+from wspm_b200 import mesh  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def dev():
+    from wspm_b200 import device
+    return device
+
+
+def cu(a, dtype=torch.float64):
+    return torch.as_tensor(np.asarray(a), dtype=dtype, device="cuda")
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+VG = (3.35, 0.368, 0.102, 2.0, 0.5, 0.0922)
+EXP = (0.164, 0.45, 0.15, 0.1)
+
+
+@pytest.mark.parametrize("model,phi", [("vg", VG), ("exp", EXP), ("vg", (3.6, 0.43, 0.078, 1.56, 1 - 1 / 1.56, 0.2496))])
+def test_soil_models(model, phi):
+    rng = np.random.default_rng(1)
+    h = np.concatenate([-10 ** rng.uniform(-4, 1.5, 5000), [0.0, 1e-300, -0.0, 0.5, -1e-300]])
+    C, K, th = dev().soil(model, cu(h), phi)
+    ref = (osoil.van_genuchten_model if model == "vg" else osoil.exponential_model)(h, phi)
+    # theta and C are well conditioned; K = Ks Se^.5 (1-(1-Se^(1/m))^m)^2 cancels as Se -> 1, amplifying
+    # the last-ulp differences between two correct pow() implementations by ~1/(1-Se^(1/m))
+    amp = np.ones_like(h)
+    if model == "vg":
+        m = phi[4]
+        se = np.clip((ref[2] - phi[2]) / (phi[1] - phi[2]), 0, 1)
+        amp = 1.0 + 1.0 / np.maximum(1.0 - se ** (1.0 / m), 1e-300)
+    for name, got, want in zip("CKt", (C, K, th), ref):
+        rtol = 4e-14 * (amp if name == "K" else 1.0)
+        got = host(got)
+        bad = np.abs(got - want) > rtol * np.abs(want)
+        assert not bad.any(), (name, h[bad][:4], got[bad][:4], want[bad][:4])
+
+
+def _assembly_case(kind):
+    rng = np.random.default_rng(2)
+    if kind == "tri-exp":
+        pts, el = mesh.structured_triangles(25, 15.24)
+        model, phi, Ks = "exp", EXP, None
+        h = -15.24 + rng.uniform(0, 10, len(pts))
+    elif kind == "tri-vg-ks":
+        pts, el = mesh.structured_triangles(40, 1.0)
+        model, phi = "vg", VG[:5] + (1.0,)
+        Ks = 0.0922 * np.exp(rng.standard_normal(len(el)))
+        h = -rng.uniform(0.05, 2.0, len(pts))
+    elif kind == "tri-ragged":
+        pts, el = mesh.structured_triangles(17, 1.0)
+        perm = rng.permutation(len(pts))
+        inv = np.argsort(perm)
+        pts, el = pts[perm], inv[el][rng.permutation(len(el))]
+        model, phi, Ks = "vg", VG, None
+        h = -rng.uniform(0.05, 2.0, len(pts))
+    else:
+        pts, el = mesh.kuhn_tetrahedra(6, 15.24)
+        model, phi, Ks = "exp", EXP, None
+        h = -15.24 + rng.uniform(0, 10, len(pts))
+    return pts, el, model, phi, Ks, h
+
+
+@pytest.mark.parametrize("kind", ["tri-exp", "tri-vg-ks", "tri-ragged", "tet-exp"])
+def test_assembly_matches_oracle(kind):
+    from wspm_b200.engine import default_rule
+    pts, el, model, phi, Ks, h = _assembly_case(kind)
+    D = dev()
+    dm = D.DeviceMesh(pts, el)
+    fn = osoil.van_genuchten_model if model == "vg" else osoil.exponential_model
+    C, K, th_m = fn(h, phi)
+    th_n = fn(h - 0.01, phi)[2]
+    dt = 3e-3
+    A_ref, b_ref = oasm.assemble_richards(el, len(pts), pts, th_m, th_n, h, K, C, dt, Ks_elem=Ks)
+    Q, W = default_rule(pts.shape[1])
+    vals, rhs, dinv, vals32 = D.assemble_richards(dm, cu(th_m), cu(th_n), cu(h), cu(K), cu(C), Q, W, dt,
+                                                  Ks_elem=None if Ks is None else cu(Ks), want_f32=True)
+    A = dm.pattern.to_scipy(host(vals))
+    scale = np.abs(A_ref.data).max()
+    assert np.abs((A - A_ref).toarray()).max() <= 1e-13 * scale
+    np.testing.assert_allclose(host(rhs), b_ref, rtol=0, atol=1e-13 * np.abs(b_ref).max())
+    np.testing.assert_allclose(host(dinv), okry.jacobi_inverse_diagonal(A_ref), rtol=1e-13)
+    np.testing.assert_allclose(host(vals32), host(vals).astype(np.float32), rtol=0, atol=0)
+    # padding slots stay exactly zero
+    mask = np.ones(dm.nnz_padded, bool)
+    mask[dm.pattern.sell_index] = False
+    assert np.all(host(vals)[mask] == 0.0)
+
+
+def test_assembly_with_dirichlet_rows_and_apply_dirichlet():
+    from wspm_b200.engine import default_rule
+    pts, el = mesh.structured_triangles(25, 15.24)
+    top, bottom = opic.boundary_nodes_2d(pts, "Test1")
+    h = -15.24 * np.ones(len(pts))
+    C, K, th = osoil.exponential_model(h, EXP)
+    hup = opic.upper_bc("Test1", pts[top, 0], EXP[0], np.exp(EXP[0] * h[top]))
+    nodes, values = opic.dirichlet_arrays(len(pts), [(top, hup), (bottom, -15.0)])
+    A_ref, b_ref = oasm.assemble_richards(el, len(pts), pts, th, th, h, K, C, 1e-3)
+    A_ref, b_ref = oasm.apply_dirichlet_rows(A_ref, b_ref, nodes, values)
+    D = dev()
+    dm = D.DeviceMesh(pts, el)
+    bc = D.merge_dirichlet(len(pts), [(top, hup), (bottom, -15.0)])
+    Q, W = default_rule(2)
+    vals, rhs, dinv, _ = D.assemble_richards(dm, cu(th), cu(th), cu(h), cu(K), cu(C), Q, W, 1e-3, bc_val=cu(bc))
+    A = dm.pattern.to_scipy(host(vals))
+    assert np.abs((A - A_ref).toarray()).max() <= 1e-13 * np.abs(A_ref.data).max()
+    np.testing.assert_allclose(host(rhs), b_ref, rtol=1e-13, atol=1e-13)
+    # the stand-alone Dirichlet op on an un-constrained assembly gives the same system
+    vals2, rhs2, _, _ = D.assemble_richards(dm, cu(th), cu(th), cu(h), cu(K), cu(C), Q, W, 1e-3)
+    D.apply_dirichlet(dm, nodes, values, vals2, rhs2)
+    np.testing.assert_array_equal(host(vals2), host(vals))
+    np.testing.assert_array_equal(host(rhs2), host(rhs))
+    np.testing.assert_allclose(host(D.jacobi_dinv(dm, vals)), host(dinv), rtol=0)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_spmv(dtype):
+    rng = np.random.default_rng(3)
+    pts, el = mesh.kuhn_tetrahedra(7)
+    D = dev()
+    dm = D.DeviceMesh(pts, el)
+    data = rng.standard_normal(dm.pattern.nnz)
+    x = rng.standard_normal(len(pts))
+    vals = cu(dm.pattern.sell_from_csr_values(data), dtype)
+    y = host(D.spmv(dm, vals, cu(x, dtype)))
+    A = dm.pattern.to_scipy(dm.pattern.sell_from_csr_values(data))
+    tol = 1e-13 if dtype == torch.float64 else 2e-5
+    np.testing.assert_allclose(y, A @ x, rtol=0, atol=tol * np.abs(A).sum(axis=1).max() * np.abs(x).max())
+
+
+def _linear_system(n=30, dirichlet=True):
+    from wspm_b200.engine import default_rule
+    pts, el = mesh.structured_triangles(n, 15.24)
+    rng = np.random.default_rng(4)
+    h = -15.24 + rng.uniform(0, 12, len(pts))
+    C, K, th = osoil.exponential_model(h, EXP)
+    A, b = oasm.assemble_richards(el, len(pts), pts, th, th - 1e-3, h, K, C, 5e-3)
+    if dirichlet:
+        top, bottom = opic.boundary_nodes_2d(pts, "Test1")
+        nodes, values = opic.dirichlet_arrays(len(pts), [(top, -1.0), (bottom, -15.0)])
+        A, b = oasm.apply_dirichlet_rows(A, b, nodes, values)
+    return pts, el, A, b, h
+
+
+@pytest.mark.parametrize("solver,precond", [("cg", "jacobi"), ("cg", "none"), ("bicgstab", "none"),
+                                            ("bicgstab", "jacobi"), ("gmres", "jacobi"), ("gmres", "none")])
+def test_krylov_solve_matches_oracle(solver, precond):
+    pts, el, A, b, h = _linear_system()
+    D = dev()
+    dm = D.DeviceMesh(pts, el)
+    vals = cu(dm.pattern.sell_from_csr_values(A.data))
+    dinv = D.jacobi_dinv(dm, vals) if precond == "jacobi" else None
+    x_ref, k_ref = okry.solve_system(A, b, h, solver, precond, tol=1e-10, maxiter=400, restart=30)
+    x, res = D.krylov_solve(dm, vals, cu(b), cu(h), solver=solver, dinv=dinv, tol=1e-10, maxiter=400, restart=30)
+    status, iters = host(res)[:2]
+    assert status == 0
+    assert abs(int(iters) - k_ref) <= max(2, k_ref // 20)
+    exact = np.linalg.solve(A.toarray(), b)
+    err = np.linalg.norm(host(x) - exact) / np.linalg.norm(exact)
+    err_ref = np.linalg.norm(x_ref - exact) / np.linalg.norm(exact)
+    assert err <= max(10 * err_ref, 1e-9)
+    np.testing.assert_allclose(host(x), x_ref, rtol=1e-7, atol=1e-7)
+
+
+def test_krylov_maxiter_status_is_reported():
+    pts, el, A, b, h = _linear_system(dirichlet=False)
+    D = dev()
+    dm = D.DeviceMesh(pts, el)
+    vals = cu(dm.pattern.sell_from_csr_values(A.data))
+    x, res = D.krylov_solve(dm, vals, cu(b), cu(h), solver="cg", tol=1e-14, maxiter=3)
+    status, iters = host(res)[:2]
+    x_ref, k_ref = okry.cg(A, b, h, tol=1e-14, maxiter=3)
+    assert status == 1 and iters == 3 == k_ref
+    np.testing.assert_allclose(host(x), x_ref, rtol=1e-11)
+
+
+def test_zero_rhs_gmres_returns_x0():
+    pts, el, A, b, h = _linear_system(n=8)
+    D = dev()
+    dm = D.DeviceMesh(pts, el)
+    vals = cu(dm.pattern.sell_from_csr_values(A.data))
+    x, res = D.krylov_solve(dm, vals, cu(np.zeros_like(b)), cu(h), solver="gmres", tol=1e-10)
+    np.testing.assert_array_equal(host(x), h)
+    assert host(res)[1] == 0
+
+
+def _engine_test_case(case, n, solver, precond, **kw):
+    from wspm_b200.device import DeviceMesh, merge_dirichlet
+    from wspm_b200.engine import PicardEngine
+    pts, tri = mesh.structured_triangles(n, 15.24)
+    top, bottom = opic.boundary_nodes_2d(pts, case)
+    h0 = -15.24 * np.ones(len(pts))
+    hup = opic.upper_bc(case, pts[top, 0], EXP[0], np.exp(EXP[0] * h0[top]))
+    bc = merge_dirichlet(len(pts), [(top, hup), (bottom, -15.0)])
+    eng = PicardEngine(DeviceMesh(pts, tri), "exp", EXP, bc_val=bc, solver=solver, precond=precond, **kw)
+    return pts, tri, eng, h0
+
+
+@pytest.mark.parametrize("case", ["Test1", "Test2", "Test3"])
+def test_picard_engine_reproduces_csv_golden_mesh25(case):
+    import json
+    rows = [r for r in json.load(open(os.path.join(GOLD, "re2d_metrics.json")))
+            if r["test_case"] == case and r["mesh"] == 25 and r["solver"] == "cg" and r["precond"] == "jacobi"]
+    pts, tri, eng, h0 = _engine_test_case(case, 25, "cg", "jacobi", picard_tol=1e-4, picard_maxiter=30,
+                                          picard_relative=False)
+    res = eng.run(h0, 1e-3, 0.25, theta_at_end=False)
+    m = analytic.final_errors(pts, res["pressure_head"][-1], res["theta"][-1], res["times"][-1], int(case[-1]))
+    assert res["iterations"].sum() == rows[0]["iterations"]
+    np.testing.assert_allclose(list(m.values()), rows[0]["metrics"], rtol=5e-4)
+
+
+def test_picard_engine_matches_oracle_vg_unit_square():
+    """The VG unit-square workload (50x50, h0 = -1, top -0.1, cg+jacobi, relative Picard 1e-6)."""
+    from wspm_b200.device import DeviceMesh, merge_dirichlet
+    from wspm_b200.engine import PicardEngine
+    pts, tri = mesh.structured_triangles(50, 1.0)
+    top = np.where(pts[:, 1] == 1.0)[0]
+    prob, h0 = opic.vg_dirichlet_case(pts, tri, top)
+    ref = opic.run_time_loop(prob, h0, 1e-4, 0.02)
+    bc = merge_dirichlet(len(pts), [(top, -0.1)])
+    eng = PicardEngine(DeviceMesh(pts, tri), "vg", opic.VG_UNIT_PHI, bc_val=bc, solver="cg", precond="jacobi")
+    res = eng.run(h0, 1e-4, 0.02)
+    np.testing.assert_array_equal(res["iterations"], ref["iterations"])
+    np.testing.assert_allclose(res["pressure_head"], ref["pressure_head"], rtol=1e-9, atol=1e-10)
+    np.testing.assert_allclose(res["theta"], ref["theta"], rtol=1e-9, atol=1e-11)
+
+
+@pytest.mark.parametrize("solver", ["bicgstab", "gmres"])
+def test_picard_engine_test3d_golden(solver):
+    from wspm_b200.device import DeviceMesh, merge_dirichlet
+    from wspm_b200.engine import PicardEngine
+    g = np.load(os.path.join(GOLD, f"test3d_{solver}.npz"))
+    pts, tets = mesh.kuhn_tetrahedra(20, 15.24)
+    top, bottom = opic.boundary_nodes_3d(pts)
+    h0 = -15.24 * np.ones(len(pts))
+    hup = opic.upper_bc("Test3D", pts[top, 0], EXP[0], np.exp(EXP[0] * h0[top]), y=pts[top, 1])
+    bc = merge_dirichlet(len(pts), [(top, hup), (bottom, -15.0)])
+    eng = PicardEngine(DeviceMesh(pts, tets), "exp", EXP, bc_val=bc, solver=solver, precond="none",
+                       picard_tol=1e-4, picard_maxiter=30, picard_relative=False)
+    res = eng.run(h0, 1e-4, 0.1, theta_at_end=False)
+    np.testing.assert_array_equal(res["iterations"], g["iterations"])
+    np.testing.assert_allclose(res["dt_values"], g["dt_values"], rtol=0)
+    for k, s in enumerate(g["steps"]):
+        np.testing.assert_allclose(res["pressure_head"][s], g["pressure_head"][k], rtol=1e-8, atol=1e-8)
+
+
+def test_mixed_precision_refinement_reaches_fp64_residual():
+    from wspm_b200.device import DeviceMesh, merge_dirichlet, spmv
+    from wspm_b200.engine import PicardEngine
+    pts, tri = mesh.structured_triangles(96, 1.0)
+    rng = np.random.default_rng(5)
+    Ks = 0.0922 * np.exp(rng.standard_normal(len(tri)))
+    top = np.where(pts[:, 1] == 1.0)[0]
+    bc = merge_dirichlet(len(pts), [(top, -0.1)])
+    phi = opic.VG_UNIT_PHI[:5] + (1.0,)
+    dm = DeviceMesh(pts, tri)
+    out = {}
+    for mixed in (False, True):
+        eng = PicardEngine(dm, "vg", phi, Ks_elem=Ks, bc_val=bc, solver="cg", precond="jacobi", krylov_tol=1e-8,
+                           krylov_maxiter=5000, mixed=mixed)
+        res = eng.run(-np.ones(len(pts)), 1e-4, 1e-3, fixed_dt=True, max_steps=3)
+        assert np.all(res["status"] == 0)
+        # true residual of the last linear system
+        r = eng.rhs - spmv(dm, eng.vals, eng.x)
+        assert float(torch.linalg.norm(r) / torch.linalg.norm(eng.rhs)) <= 1.01e-8
+        out[mixed] = res
+    np.testing.assert_array_equal(out[True]["iterations"], out[False]["iterations"])
+    np.testing.assert_allclose(out[True]["pressure_head"], out[False]["pressure_head"], rtol=1e-6, atol=1e-7)
+
+
+def test_picard_step_is_bitwise_repeatable():
+    pts, tri, eng, h0 = _engine_test_case("Test2", 50, "cg", "jacobi")
+    a = eng.run(h0, 1e-3, 0.02)
+    b = eng.run(h0, 1e-3, 0.02)
+    np.testing.assert_array_equal(a["pressure_head"], b["pressure_head"])
+    np.testing.assert_array_equal(a["iterations"], b["iterations"])
+
+
+@pytest.mark.parametrize("solver,precond,mixed", [("cg", "jacobi", False), ("cg", "jacobi", True),
+                                                  ("bicgstab", "none", False), ("gmres", "jacobi", False)])
+def test_host_loop_mode_matches_device_loop(solver, precond, mixed):
+    """The host-driven step (for profiling tools) runs the same kernels: results are bitwise equal."""
+    pts, tri, eng, h0 = _engine_test_case("Test1", 25, solver, precond, mixed=mixed)
+    a = eng.run(h0, 1e-3, 0.02)
+    eng.host_loop = True
+    b = eng.run(h0, 1e-3, 0.02)
+    np.testing.assert_array_equal(a["iterations"], b["iterations"])
+    np.testing.assert_array_equal(a["krylov_iterations"], b["krylov_iterations"])
+    np.testing.assert_array_equal(a["pressure_head"], b["pressure_head"])

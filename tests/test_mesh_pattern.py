@@ -1,0 +1,109 @@
+"""Mesh generators against the reference meshes, and SELL-32 pattern invariants (CPU)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from wspm_b200 import mesh
+from wspm_b200.pattern import Pattern
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+DIGESTS = json.load(open(os.path.join(GOLD, "mesh_digests.json")))
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("n", [25, 50, 100, 200])
+def test_structured_triangles_match_reference_files(n):
+    p, t = mesh.structured_triangles(n, 15.24)
+    assert sha(p) == DIGESTS[f"richards/p{n}"]["sha256"]
+    assert sha(t) == DIGESTS[f"richards/t{n}"]["sha256"]
+
+
+@pytest.mark.parametrize("n", [25, 50, 100])
+def test_unit_square_matches_nitrogen_meshes(n):
+    p, t = mesh.structured_triangles(n, 1.0)
+    assert sha(p) == DIGESTS[f"nitrogen/p_{n}"]["sha256"]
+    assert sha(t) == DIGESTS[f"nitrogen/t_{n}"]["sha256"]
+
+
+def test_kuhn_tetrahedra_match_reference_file():
+    p, t = mesh.kuhn_tetrahedra(20, 15.24)
+    assert sha(p) == DIGESTS["richards/p_3D"]["sha256"]
+    assert sha(t) == DIGESTS["richards/t_3D"]["sha256"]
+    J = p[t[:, 1:]] - p[t[:, :1]]
+    assert np.all(np.linalg.det(J) > 0)
+
+
+@pytest.mark.parametrize("n", [1, 3, 8, 33])
+def test_nnz_formula_2d(n):
+    p, t = mesh.structured_triangles(n)
+    P = Pattern(t, len(p))
+    assert P.nnz == 7 * n * n + 6 * n + 1
+
+
+@pytest.mark.parametrize("n", [1, 2, 5])
+def test_nnz_formula_3d(n):
+    p, t = mesh.kuhn_tetrahedra(n)
+    P = Pattern(t, len(p))
+    assert P.nnz == (n + 1) ** 3 + 2 * (3 * n * (n + 1) ** 2 + 3 * n * n * (n + 1) + n ** 3)
+
+
+@pytest.mark.parametrize("kind", ["tri", "tet", "ragged"])
+def test_pattern_roundtrip_and_incidence(kind):
+    rng = np.random.default_rng(0)
+    if kind == "tri":
+        p, t = mesh.structured_triangles(7)
+    elif kind == "tet":
+        p, t = mesh.kuhn_tetrahedra(3)
+    else:  # unstructured: permuted nodes and elements (ragged slices)
+        p, t = mesh.structured_triangles(9)
+        perm = rng.permutation(len(p))
+        inv = np.argsort(perm)
+        p, t = p[perm], inv[t][rng.permutation(len(t))]
+    P = Pattern(t, len(p))
+    nv = t.shape[1]
+    rows = np.repeat(t, nv, axis=1).ravel()
+    cols = np.tile(t, (1, nv)).ravel()
+    ref = sp.coo_matrix((np.ones(rows.size), (rows, cols)), shape=(len(p), len(p))).tocsr()
+    ref.sum_duplicates()
+    ref.sort_indices()
+    np.testing.assert_array_equal(P.csr_indptr, ref.indptr)
+    np.testing.assert_array_equal(P.csr_indices, ref.indices)
+    vals = rng.standard_normal(P.nnz)
+    np.testing.assert_array_equal(P.csr_values_from_sell(P.sell_from_csr_values(vals)), vals)
+    # every incidence decodes to the right columns, elements ascending per node
+    for i in range(len(p)):
+        s, lane = divmod(i, 32)
+        prev = -1
+        for k in range(P.inc_width[s]):
+            o = P.inc_ptr[s] + 32 * k + lane
+            e = P.inc_elem[o]
+            if e < 0:
+                break
+            assert e > prev
+            prev = e
+            pk = int(P.inc_slots[o])
+            assert t[e, pk & 3] == i
+            for j in range(nv):
+                kj = (pk >> (2 + 6 * j)) & 63
+                assert P.cols[P.slice_ptr[s] + 32 * kj + lane] == t[e, j]
+        assert P.cols[P.slice_ptr[s] + 32 * P.diag_pos[i] + lane] == i
+
+
+def test_loader_errors(tmp_path):
+    pf, tf = tmp_path / "p.csv", tmp_path / "t.csv"
+    with pytest.raises(FileNotFoundError):
+        mesh.load_csv_mesh(str(pf), str(tf), 2)
+    pf.write_text("0,0\n1,0\n0,1\n")
+    tf.write_text("1,2,4\n")
+    with pytest.raises(ValueError, match="out of bounds"):
+        mesh.load_csv_mesh(str(pf), str(tf), 2)
+    tf.write_text("1,2,3\n")
+    pts, el = mesh.load_csv_mesh(str(pf), str(tf), 2)
+    assert el.tolist() == [[0, 1, 2]]

@@ -1,0 +1,74 @@
+"""The oracle against the reference's own golden artefacts (CPU).
+
+Pins oracle/ to resultsRE2D CSV rows (Picard totals + six analytical-error
+metrics, 5 significant digits) and to the Test3D npz fields (1e-12).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import analytic, picard
+from wspm_b200 import mesh
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+ROWS = json.load(open(os.path.join(GOLD, "re2d_metrics.json")))
+
+# Unpreconditioned BiCGSTAB at mesh 50 hits its 100-iteration cap in one Picard
+# iteration of the reference run: Krylov-internal behaviour, not pinned.
+UNPINNED = {("Test1", 50, "bicgstab", "none")}
+
+
+def golden_rows(meshes, solvers=("cg", "bicgstab", "gmres", "direct"), preconds=("none", "jacobi")):
+    seen, out = set(), []
+    for r in ROWS:
+        key = (r["test_case"], r["mesh"], r["solver"], r["precond"])
+        if r["mesh"] in meshes and r["solver"] in solvers and r["precond"] in preconds and key not in seen:
+            seen.add(key)
+            out.append(r)
+    return out
+
+
+def run_golden_profile(case, n, solver, precond):
+    pts, tri = mesh.structured_triangles(n, 15.24)
+    prob, h0 = picard.test_case_2d(pts, tri, case, solver=solver, precond=precond,
+                                   picard_tol=1e-4, picard_max=30, picard_relative=False)
+    res = picard.run_time_loop(prob, h0, 1e-3, 0.25, theta_at_end=False)
+    m = analytic.final_errors(pts, res["pressure_head"][-1], res["theta"][-1], res["times"][-1], int(case[-1]))
+    return res, list(m.values())
+
+
+@pytest.mark.parametrize("row", golden_rows({25}), ids=lambda r: f"{r['test_case']}-{r['mesh']}-{r['solver']}-{r['precond']}")
+def test_oracle_reproduces_csv_mesh25(row):
+    res, metrics = run_golden_profile(row["test_case"], row["mesh"], row["solver"], row["precond"])
+    assert res["iterations"].sum() == row["iterations"]
+    np.testing.assert_allclose(metrics, row["metrics"], rtol=5e-4)
+
+
+@pytest.mark.parametrize("row", golden_rows({50}, solvers=("cg", "gmres"), preconds=("jacobi",)),
+                         ids=lambda r: f"{r['test_case']}-{r['mesh']}-{r['solver']}-{r['precond']}")
+def test_oracle_reproduces_csv_mesh50(row):
+    res, metrics = run_golden_profile(row["test_case"], row["mesh"], row["solver"], row["precond"])
+    assert res["iterations"].sum() == row["iterations"]
+    np.testing.assert_allclose(metrics, row["metrics"], rtol=5e-4)
+
+
+def test_unpinned_row_is_documented():
+    rows = {(r["test_case"], r["mesh"], r["solver"], r["precond"]) for r in ROWS}
+    assert UNPINNED <= rows
+
+
+@pytest.mark.parametrize("solver", ["bicgstab", "gmres"])
+def test_oracle_reproduces_test3d_npz(solver):
+    g = np.load(os.path.join(GOLD, f"test3d_{solver}.npz"))
+    pts, tets = mesh.kuhn_tetrahedra(20, 15.24)
+    prob, h0 = picard.test_case_3d(pts, tets, solver=solver, precond="none")
+    res = picard.run_time_loop(prob, h0, 1e-4, 0.1, theta_at_end=False)
+    np.testing.assert_array_equal(res["iterations"], g["iterations"])
+    np.testing.assert_allclose(res["dt_values"], g["dt_values"], rtol=0, atol=0)
+    np.testing.assert_allclose(res["times"], g["times"], rtol=1e-15)
+    for k, s in enumerate(g["steps"]):
+        np.testing.assert_allclose(res["pressure_head"][s], g["pressure_head"][k], rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(res["theta"][s], g["theta"][k], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(res["errors"], g["errors"], rtol=1e-6)
