@@ -13,7 +13,8 @@
  *  - Sparse matrices use the SELL-32 layout described by wspm_pattern: rows
  *    are grouped in slices of 32; entry k of row i lives at
  *    slice_ptr[i/32] + 32*k + i%32.  Padding entries have column = own row
- *    and value 0.
+ *    and value 0.  Structured meshes may use the DIA variant (see
+ *    wspm_pattern.n_diags).
  *  - Meshes: conn is element-major int32 [E*nv] (0-based), coords is
  *    node-major float64 [N*dim].
  *
@@ -75,6 +76,15 @@ typedef struct wspm_pattern {
     const int32_t *inc_elem;  /* element id, -1 = padding                    */
     const uint32_t *inc_slots;/* bits 0-1: local vertex of the row's node;
                                  bits 2+6j..7+6j: row position of vertex j   */
+    /* DIA layout (n_diags > 0): the matrix holds n_diags diagonals with column
+     * offsets diag_offsets[k]; entry k of row i is at k*ld + i with
+     * ld = 32*n_slices (slice_ptr/slice_width/cols then describe the same
+     * layout: width n_diags everywhere).  Used when every row's column
+     * offsets belong to one small set (structured meshes): no column-index
+     * stream is read by the sparse kernels.                               */
+    int32_t n_diags;
+    int32_t pad_;
+    const int32_t *diag_offsets;
 } wspm_pattern;
 
 /* ---- soil models -------------------------------------------------------- */
@@ -107,6 +117,53 @@ int wspm_assemble_richards(const wspm_mesh *mesh, const wspm_pattern *pat,
                            double dt, const double *bc_val,
                            double *vals, float *vals32, double *rhs, double *dinv,
                            void *stream);
+
+/* ---- transport ------------------------------------------------------------ */
+/* calculate_fluxes_and_dispersion_FE, src/models/transport_utilities.py:118-192
+ * (triangles): nodal Darcy flux from the mean element gradient of h over the
+ * node's triangles, van Genuchten theta/K (phi as for wspm_soil_van_genuchten)
+ * and the dispersion tensor.  Outputs [n_nodes] each.                      */
+int wspm_flux_dispersion_2d(const wspm_mesh *mesh, const wspm_pattern *pat, const double *h,
+                            const double *phi, double DL, double DT, double Dm,
+                            double *qx, double *qz, double *aq, double *Dxx, double *Dxz,
+                            double *Dzz, double *theta, void *stream);
+
+/* Advection-dispersion-reaction system on triangles:
+ *   lumped == 0: assemble_global_matrices_solute, src/numerics/assembly_solute.py:88-186,
+ *                then A = M/dt + K and b = M c_n / dt (coupled_solver_v2.py:164-185);
+ *   lumped == 1: assemble_nitrogen_species{1,2,3}_sparse, src/numerics/assembly_nitrogen.py:311-606,
+ *                lump_sparse_mass_matrix and A = M/dt + K, b = M c_n/dt + F
+ *                (src/solvers/nitrogen_solver.py:36-66, 151-235).
+ * K = -dispersion - advection + mu*theta*N N^T, M = -(theta + sorption) N N^T,
+ * F = -mu_up * theta * c_up * N (c_up may be NULL: no source).            */
+int wspm_assemble_adr_2d(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta,
+                         const double *qx, const double *qz, const double *Dxx, const double *Dxz,
+                         const double *Dzz, const double *c_n, const double *c_up, double mu,
+                         double sorption, double mu_up, int32_t lumped,
+                         const double *quad_points, const double *weights, int32_t nq, double dt,
+                         double *vals, double *rhs, double *dinv, void *stream);
+
+/* Boundary edges (consecutive boundary nodes, 2-point Gauss rule), grouped per
+ * boundary node so that each node sums its at most two edges in edge order.
+ * Built on the host (wspm_b200.device.BoundaryEdges); device arrays.       */
+typedef struct wspm_edges {
+    int32_t n_bnodes;
+    int32_t pad_;
+    const int32_t *node;      /* [n_bnodes]                                   */
+    const int32_t *e_cnt;     /* [n_bnodes] edges of this node (0..2)         */
+    const int32_t *e_local;   /* [2 n_bnodes] 0 if the node is the edge's I   */
+    const int32_t *e_other;   /* [2 n_bnodes] the edge's other node           */
+    const int32_t *e_kother;  /* [2 n_bnodes] row position of the other node  */
+    const double  *e_jac;     /* [2 n_bnodes] (x_J - x_I) / 2                 */
+} wspm_edges;
+
+#define WSPM_EDGE_NEUMANN          0  /* apply_neumann_bcs, boundary.py:108-128 (rhs)          */
+#define WSPM_EDGE_DRAINAGE_WATER   1  /* apply_freedrainage_water_bcs, boundary.py:132-173     */
+#define WSPM_EDGE_CAUCHY           2  /* apply_cauchy_bcs_sparse, boundary.py:217-277          */
+#define WSPM_EDGE_DRAINAGE_SOLUTE  3  /* apply_freedrainage_nitrogen_bcs_sparse, :336-421     */
+int wspm_apply_edge_terms(const wspm_pattern *pat, const wspm_edges *edges, int32_t mode,
+                          double flux, double c_in, const double *K, const double *theta,
+                          double *vals, double *rhs, void *stream);
 
 /* ---- sparse kernels ----------------------------------------------------- */
 /* y = A x (BCOO matvec inside jax.scipy.sparse.linalg, SELL-32 here).       */
@@ -178,6 +235,11 @@ typedef struct wspm_picard_desc {
     double  picard_tol;
     int32_t picard_maxiter;
     int32_t picard_relative;   /* 1: ||h-h_m||/||h||, 0: ||h-h_m||           */
+    /* optional boundary-edge right-hand-side terms applied after assembly, in
+     * this order (coupled_solver_v2.py:106-116, nitrogen_solver.py:116-127)  */
+    const wspm_edges *neumann;  /* NULL = none                                */
+    double  neumann_flux;
+    const wspm_edges *drainage; /* free drainage of water, NULL = none        */
     /* state (device, caller-owned, n_nodes doubles unless noted) */
     double *h_n;               /* in: previous step; out: this step's head   */
     double *theta_n;           /* scratch: theta(h_n)                        */

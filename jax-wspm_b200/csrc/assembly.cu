@@ -49,6 +49,8 @@ struct RichardsAsmArgs {
     double mcoef[4];   // lumped-mass coefficients per vertex
     double inv_dt;
     const double *dt_dev;   // when set, dt is read from device memory (graph replay)
+    int n_diags;            // > 0: DIA layout, entry k of row i at k*ld + i
+    int64_t ld;
     double *vals;
     float *vals32;
     double *rhs, *dinv;
@@ -110,13 +112,16 @@ __global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = i >> 5, lane = i & 31;
     if (s >= ((a.n_rows + kSlice - 1) >> 5)) return;
-    const int width = a.slice_width[s];
+    const bool dia = a.n_diags > 0;
+    const int width = dia ? a.n_diags : a.slice_width[s];
+    // entry k of this row lives at vb + kstride * k
+    const int64_t vb = dia ? (int64_t)i : a.slice_ptr[s] + lane;
+    const int64_t kstride = dia ? a.ld : (int64_t)kSlice;
     if (i >= a.n_rows) {
         // padding rows of the last slice: keep their slots defined (zero)
-        const int64_t pb = a.slice_ptr[s] + lane;
         for (int k = 0; k < width; ++k) {
-            a.vals[pb + (int64_t)kSlice * k] = 0.0;
-            if (a.vals32) a.vals32[pb + (int64_t)kSlice * k] = 0.0f;
+            a.vals[vb + kstride * k] = 0.0;
+            if (a.vals32) a.vals32[vb + kstride * k] = 0.0f;
         }
         return;
     }
@@ -175,11 +180,10 @@ __global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
     }
     a.rhs[i] = rhs_i;
     if (a.dinv) a.dinv[i] = 1.0 / (diag != 0.0 ? diag : 1.0);
-    const int64_t vb = a.slice_ptr[s] + lane;
     for (int k = 0; k < width; ++k) {
         const double v = acc[k * stride];
-        a.vals[vb + (int64_t)kSlice * k] = v;
-        if (a.vals32) a.vals32[vb + (int64_t)kSlice * k] = (float)v;
+        a.vals[vb + kstride * k] = v;
+        if (a.vals32) a.vals32[vb + kstride * k] = (float)v;
     }
 }
 
@@ -220,6 +224,8 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     for (int j = 0; j < 4; ++j) { a.s[j] = s[j]; a.mcoef[j] = mc[j]; }
     a.inv_dt = 1.0 / dt;
     a.dt_dev = dt_dev;
+    a.n_diags = pat->n_diags;
+    a.ld = (int64_t)pat->n_slices * kSlice;
     a.vals = vals; a.vals32 = vals32; a.rhs = rhs; a.dinv = dinv;
     const int threads = 128;
     const int blocks = (pat->n_slices * kSlice + threads - 1) / threads;

@@ -16,17 +16,25 @@ int launch_richards_assembly(const wspm_mesh *mesh, const wspm_pattern *pat, con
                              const double *bc_val, double *vals, float *vals32, double *rhs, double *dinv,
                              cudaStream_t st);
 
+int launch_flux_dispersion(const wspm_mesh *mesh, const wspm_pattern *pat, const double *h, const SoilParams &sp,
+                           double DL, double DT, double Dm, double *qx, double *qz, double *aq, double *Dxx,
+                           double *Dxz, double *Dzz, double *theta, cudaStream_t st);
+int launch_adr(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta, const double *qx,
+               const double *qz, const double *Dxx, const double *Dxz, const double *Dzz, const double *c_n,
+               const double *c_up, double mu, double sorption, double mu_up, int lumped, const double *Q,
+               const double *W, int nq, double dt, double *vals, double *rhs, double *dinv, cudaStream_t st);
+int launch_edge_terms(const wspm_pattern *pat, const wspm_edges *e, int mode, double flux, double c_in,
+                      const double *K, const double *theta, double *vals, double *rhs, cudaStream_t st);
+
 __global__ void dirichlet_rows_kernel(Sell A, const int32_t *__restrict__ diag_pos, const int32_t *__restrict__ nodes,
                                       const double *__restrict__ values, int n_bc, double *vals, double *rhs) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_bc) return;
     const int i = nodes[t];
     if (i < 0 || i >= A.n_rows) return;
-    const int s = i >> 5, lane = i & 31;
-    const int w = A.slice_width[s];
-    const int64_t base = A.slice_ptr[s] + lane;
+    const int w = row_width(A, i);
     const int dp = diag_pos[i];
-    for (int k = 0; k < w; ++k) vals[base + (int64_t)kSlice * k] = (k == dp) ? 1.0 : 0.0;
+    for (int k = 0; k < w; ++k) vals[entry_pos(A, i, k)] = (k == dp) ? 1.0 : 0.0;
     rhs[i] = values[t];
 }
 
@@ -34,7 +42,7 @@ __global__ void jacobi_kernel(Sell A, const int32_t *__restrict__ diag_pos, cons
                               double *dinv) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n_rows) return;
-    const double d = vals[A.slice_ptr[i >> 5] + (i & 31) + (int64_t)kSlice * diag_pos[i]];
+    const double d = vals[entry_pos(A, i, diag_pos[i])];
     dinv[i] = 1.0 / (d != 0.0 ? d : 1.0);
 }
 
@@ -145,7 +153,8 @@ extern "C" int wspm_soil_exponential(const double *h, int64_t n, const double *p
 
 static bool pattern_ok(const wspm_pattern *p) {
     return p && p->n_rows > 0 && p->n_slices == (p->n_rows + 31) / 32 && p->slice_ptr && p->slice_width &&
-           p->cols && p->diag_pos && p->max_width > 0 && p->max_width <= 63;
+           p->cols && p->diag_pos && p->max_width > 0 && p->max_width <= 63 &&
+           (p->n_diags == 0 || (p->n_diags == p->max_width && p->diag_offsets));
 }
 
 extern "C" int wspm_assemble_richards(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
@@ -164,6 +173,54 @@ extern "C" int wspm_assemble_richards(const wspm_mesh *mesh, const wspm_pattern 
     quadrature_constants(mesh->dim, quad_points, weights, nq, s, mc);
     return launch_richards_assembly(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, s, mc, dt, bc_val, vals, vals32,
                                     rhs, dinv, (cudaStream_t)stream);
+}
+
+static bool incidence_ok(const wspm_pattern *p) {
+    return p->inc_ptr && p->inc_width && p->inc_elem && p->inc_slots;
+}
+
+extern "C" int wspm_flux_dispersion_2d(const wspm_mesh *mesh, const wspm_pattern *pat, const double *h,
+                                       const double *phi, double DL, double DT, double Dm, double *qx, double *qz,
+                                       double *aq, double *Dxx, double *Dxz, double *Dzz, double *theta,
+                                       void *stream) {
+    if (!mesh || !pattern_ok(pat) || !incidence_ok(pat) || mesh->dim != 2 || mesh->nv != 3 ||
+        mesh->n_nodes != pat->n_rows || !mesh->conn || !mesh->coords || !h || !phi)
+        return WSPM_BAD_ARG;
+    if (!qx || !qz || !aq || !Dxx || !Dxz || !Dzz || !theta) return WSPM_BAD_ARG;
+    SoilParams sp;
+    sp.model = WSPM_SOIL_VAN_GENUCHTEN;
+    for (int j = 0; j < 6; ++j) sp.p[j] = phi[j];
+    return launch_flux_dispersion(mesh, pat, h, sp, DL, DT, Dm, qx, qz, aq, Dxx, Dxz, Dzz, theta,
+                                  (cudaStream_t)stream);
+}
+
+extern "C" int wspm_assemble_adr_2d(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta,
+                                    const double *qx, const double *qz, const double *Dxx, const double *Dxz,
+                                    const double *Dzz, const double *c_n, const double *c_up, double mu,
+                                    double sorption, double mu_up, int32_t lumped, const double *quad_points,
+                                    const double *weights, int32_t nq, double dt, double *vals, double *rhs,
+                                    double *dinv, void *stream) {
+    if (!mesh || !pattern_ok(pat) || !incidence_ok(pat) || mesh->dim != 2 || mesh->nv != 3 ||
+        mesh->n_nodes != pat->n_rows || !mesh->conn || !mesh->coords)
+        return WSPM_BAD_ARG;
+    if (!theta || !qx || !qz || !Dxx || !Dxz || !Dzz || !c_n || !vals || !rhs) return WSPM_BAD_ARG;
+    if (!quad_points || !weights || nq <= 0 || nq > 16 || !(dt > 0.0) || !isfinite(dt)) return WSPM_BAD_ARG;
+    return launch_adr(mesh, pat, theta, qx, qz, Dxx, Dxz, Dzz, c_n, c_up, mu, sorption, mu_up, lumped, quad_points,
+                      weights, nq, dt, vals, rhs, dinv, (cudaStream_t)stream);
+}
+
+extern "C" int wspm_apply_edge_terms(const wspm_pattern *pat, const wspm_edges *edges, int32_t mode, double flux,
+                                     double c_in, const double *K, const double *theta, double *vals, double *rhs,
+                                     void *stream) {
+    if (!pattern_ok(pat) || !edges || !rhs || mode < 0 || mode > 3) return WSPM_BAD_ARG;
+    if (edges->n_bnodes < 0) return WSPM_BAD_ARG;
+    if (edges->n_bnodes > 0 && (!edges->node || !edges->e_cnt || !edges->e_local || !edges->e_other ||
+                                !edges->e_kother || !edges->e_jac))
+        return WSPM_BAD_ARG;
+    if ((mode == WSPM_EDGE_DRAINAGE_WATER || mode == WSPM_EDGE_DRAINAGE_SOLUTE) && !K) return WSPM_BAD_ARG;
+    if (mode == WSPM_EDGE_DRAINAGE_SOLUTE && !theta) return WSPM_BAD_ARG;
+    if (mode >= WSPM_EDGE_CAUCHY && !vals) return WSPM_BAD_ARG;
+    return launch_edge_terms(pat, edges, mode, flux, c_in, K, theta, vals, rhs, (cudaStream_t)stream);
 }
 
 extern "C" int wspm_spmv_f64(const wspm_pattern *pat, const double *vals, const double *x, double *y,

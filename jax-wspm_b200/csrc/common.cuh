@@ -102,23 +102,72 @@ __device__ __forceinline__ void final_sum(const T *partials, T (&out)[NV], unsig
 
 __device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
 
-// Row i of a SELL-32 matrix times x, with x supplied by the functor xf(col).
-// MW > 0: all column indices and values of the row are loaded before the
-// gathers and FMAs (memory-level parallelism); requires row width <= MW.
+// Matrix layout shared by every sparse kernel.
+//   SELL-32: entry k of row i at slice_ptr[i/32] + 32k + i%32, column cols[...].
+//   DIA (n_diags > 0): entry k of row i at k*ld + i, column i + diag_off[k]
+//   (out-of-range columns hold value 0 and are clamped for the gather).
+struct Sell {
+    int n_rows;
+    int n_slices;
+    int max_width;
+    const int64_t *slice_ptr;
+    const int32_t *slice_width;
+    const int32_t *cols;
+    int n_diags;
+    const int32_t *diag_off;
+    int64_t ld;
+};
+
+__device__ __forceinline__ int64_t entry_pos(const Sell &A, int i, int k) {
+    return A.n_diags > 0 ? (int64_t)k * A.ld + i : __ldg(A.slice_ptr + (i >> 5)) + (int64_t)kSlice * k + (i & 31);
+}
+
+__device__ __forceinline__ int row_width(const Sell &A, int i) {
+    return A.n_diags > 0 ? A.n_diags : __ldg(A.slice_width + (i >> 5));
+}
+
+// Row i of A times x, with x supplied by the functor xf(col).  MW > 0: all
+// column indices and values of the row are loaded before the gathers and
+// FMAs (memory-level parallelism); requires row width <= MW.
 template <typename T, int MW, typename XF>
-__device__ __forceinline__ T sell_row_dot(const int64_t *__restrict__ slice_ptr, const int32_t *__restrict__ slice_width,
-                                          const int32_t *__restrict__ cols, const T *__restrict__ vals, int i, XF xf) {
-    const int s = i >> 5, lane = i & 31;
-    const int w = __ldg(slice_width + s);
-    const int64_t base = __ldg(slice_ptr + s) + lane;
+__device__ __forceinline__ T sell_row_dot(const Sell &A, const T *__restrict__ vals, int i, XF xf) {
     T acc = T(0);
+    if (A.n_diags > 0) {
+        const int nd = A.n_diags;
+        const int last = A.n_rows - 1;
+        if constexpr (MW > 0) {
+            T v[MW];
+            int c[MW];
+#pragma unroll
+            for (int k = 0; k < MW; ++k) {
+                if (k < nd) {
+                    v[k] = __ldg(vals + (int64_t)k * A.ld + i);
+                    const int cc = i + __ldg(A.diag_off + k);
+                    c[k] = cc < 0 ? 0 : (cc > last ? last : cc);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < MW; ++k)
+                if (k < nd) acc = fma(v[k], xf(c[k]), acc);
+        } else {
+            for (int k = 0; k < nd; ++k) {
+                int cc = i + __ldg(A.diag_off + k);
+                cc = cc < 0 ? 0 : (cc > last ? last : cc);
+                acc = fma(__ldg(vals + (int64_t)k * A.ld + i), xf(cc), acc);
+            }
+        }
+        return acc;
+    }
+    const int s = i >> 5, lane = i & 31;
+    const int w = __ldg(A.slice_width + s);
+    const int64_t base = __ldg(A.slice_ptr + s) + lane;
     if constexpr (MW > 0) {
         int c[MW];
         T v[MW];
 #pragma unroll
         for (int k = 0; k < MW; ++k) {
             if (k < w) {
-                c[k] = __ldg(cols + base + (int64_t)kSlice * k);
+                c[k] = __ldg(A.cols + base + (int64_t)kSlice * k);
                 v[k] = __ldg(vals + base + (int64_t)kSlice * k);
             }
         }
@@ -128,7 +177,7 @@ __device__ __forceinline__ T sell_row_dot(const int64_t *__restrict__ slice_ptr,
     } else {
         for (int k = 0; k < w; ++k) {
             const int64_t o = base + (int64_t)kSlice * k;
-            acc = fma(__ldg(vals + o), xf(__ldg(cols + o)), acc);
+            acc = fma(__ldg(vals + o), xf(__ldg(A.cols + o)), acc);
         }
     }
     return acc;

@@ -35,7 +35,7 @@ __device__ __forceinline__ void set_cond(cudaGraphConditionalHandle h, int use, 
 
 template <typename T, int MW, typename XF>
 __device__ __forceinline__ T sell_row(const Sell &A, const T *__restrict__ vals, int i, XF xf) {
-    return sell_row_dot<T, MW>(A.slice_ptr, A.slice_width, A.cols, vals, i, xf);
+    return sell_row_dot<T, MW>(A, vals, i, xf);
 }
 
 // ---------------------------------------------------------------- SpMV

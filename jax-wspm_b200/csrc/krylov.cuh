@@ -5,19 +5,11 @@
 
 namespace wspm {
 
-struct Sell {
-    int n_rows;
-    int n_slices;
-    int max_width;
-    const int64_t *slice_ptr;
-    const int32_t *slice_width;
-    const int32_t *cols;
-};
-
 inline Sell make_sell(const wspm_pattern *p) {
     Sell s;
     s.n_rows = p->n_rows; s.n_slices = p->n_slices; s.max_width = p->max_width;
     s.slice_ptr = p->slice_ptr; s.slice_width = p->slice_width; s.cols = p->cols;
+    s.n_diags = p->n_diags; s.diag_off = p->diag_offsets; s.ld = (int64_t)p->n_slices * kSlice;
     return s;
 }
 

@@ -23,6 +23,8 @@ namespace wspm {
 int launch_soil(const SoilParams &sp, const double *h, int64_t n, double *C, double *K, double *theta,
                 cudaStream_t st);
 void quadrature_constants(int dim, const double *Q, const double *W, int nq, double s[4], double m[4]);
+int launch_edge_terms(const wspm_pattern *pat, const wspm_edges *e, int mode, double flux, double c_in,
+                      const double *K, const double *theta, double *vals, double *rhs, cudaStream_t st);
 int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
                                     const double *theta_n, const double *h_m, const double *K, const double *C,
                                     const double *Ks_elem, const double s[4], const double mc[4],
@@ -135,8 +137,7 @@ __global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const doubl
                                                              cudaGraphConditionalHandle cond, int use_cond) {
     double v[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
-        const double acc = sell_row_dot<double, MW>(A.slice_ptr, A.slice_width, A.cols, vals, i,
-                                                    [&](int c) { return x[c]; });
+        const double acc = sell_row_dot<double, MW>(A, vals, i, [&](int c) { return x[c]; });
         const double ri = b[i] - acc;
         r[i] = ri;
         if (is_init && dinv32) dinv32[i] = (float)dinv[i];
@@ -181,6 +182,7 @@ struct PicardPlan {
     wspm_mesh mesh;
     wspm_pattern pat;
     wspm_picard_desc d;
+    wspm_edges neumann, drainage;   // copies (n_bnodes == 0: unused)
     SoilParams sp_field;   // soil for the assembly (Ks = 1 when Ks_elem is given)
     SoilParams sp_theta;   // soil for theta_n
     double s[4], mc[4];
@@ -242,6 +244,10 @@ static int build_picard_graph(PicardPlan *P) {
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                         P->s, P->mc, d.dt_dev, d.bc_val, d.vals, d.mixed ? d.vals32 : nullptr,
                                         d.rhs, d.dinv, bs);
+        launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
+                          bs);
+        launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
+                          bs);
         const KrylovState *ks = nullptr;
         const KrylovState *irs = nullptr;
         if (d.mixed) {
@@ -346,6 +352,10 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem, P->s,
                                         P->mc, d.dt_dev, d.bc_val, d.vals, d.mixed ? d.vals32 : nullptr, d.rhs,
                                         d.dinv, st);
+        launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
+                          st);
+        launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
+                          st);
         const KrylovState *ks = nullptr, *irs = nullptr;
         if (d.mixed) {
             copy_kernel_d(d.h_m, d.x, n, st);
@@ -449,6 +459,10 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     P->mesh = *d.mesh;
     P->pat = *d.pat;
     P->d = d;
+    P->neumann = d.neumann ? *d.neumann : wspm_edges();
+    P->drainage = d.drainage ? *d.drainage : wspm_edges();
+    P->d.neumann = nullptr;
+    P->d.drainage = nullptr;
     P->d.mesh = &P->mesh;
     P->d.pat = &P->pat;
     P->sp_field.model = d.soil_model;

@@ -28,7 +28,13 @@ class WspmPattern(ctypes.Structure):
     _fields_ = [("n_rows", c_int32), ("n_slices", c_int32), ("max_width", c_int32), ("max_inc", c_int32),
                 ("nnz_padded", c_int64),
                 ("slice_ptr", c_void_p), ("slice_width", c_void_p), ("cols", c_void_p), ("diag_pos", c_void_p),
-                ("inc_ptr", c_void_p), ("inc_width", c_void_p), ("inc_elem", c_void_p), ("inc_slots", c_void_p)]
+                ("inc_ptr", c_void_p), ("inc_width", c_void_p), ("inc_elem", c_void_p), ("inc_slots", c_void_p),
+                ("n_diags", c_int32), ("pad_", c_int32), ("diag_offsets", c_void_p)]
+
+
+class WspmEdges(ctypes.Structure):
+    _fields_ = [("n_bnodes", c_int32), ("pad_", c_int32), ("node", c_void_p), ("e_cnt", c_void_p),
+                ("e_local", c_void_p), ("e_other", c_void_p), ("e_kother", c_void_p), ("e_jac", c_void_p)]
 
 
 class WspmPicardDesc(ctypes.Structure):
@@ -39,6 +45,8 @@ class WspmPicardDesc(ctypes.Structure):
                 ("restart", c_int32),
                 ("mixed", c_int32), ("inner_tol", c_double), ("inner_maxiter", c_int32), ("refine_maxiter", c_int32),
                 ("picard_tol", c_double), ("picard_maxiter", c_int32), ("picard_relative", c_int32),
+                ("neumann", ctypes.POINTER(WspmEdges)), ("neumann_flux", c_double),
+                ("drainage", ctypes.POINTER(WspmEdges)),
                 ("h_n", c_void_p), ("theta_n", c_void_p), ("h_m", c_void_p), ("x", c_void_p),
                 ("K", c_void_p), ("C", c_void_p), ("theta_m", c_void_p),
                 ("vals", c_void_p), ("vals32", c_void_p), ("rhs", c_void_p), ("dinv", c_void_p),
@@ -53,6 +61,15 @@ _SIGS = {
     "wspm_assemble_richards": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p,
                                          c_void_p, c_void_p, P(c_double), P(c_double), c_int32, c_double, c_void_p,
                                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_flux_dispersion_2d": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, P(c_double), c_double, c_double,
+                                          c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                          c_void_p, c_void_p]),
+    "wspm_assemble_adr_2d": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double, c_double,
+                                       c_int32, P(c_double), P(c_double), c_int32, c_double, c_void_p, c_void_p,
+                                       c_void_p, c_void_p]),
+    "wspm_apply_edge_terms": (c_int32, [P(WspmPattern), P(WspmEdges), c_int32, c_double, c_double, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_spmv_f64": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_spmv_f32": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_apply_dirichlet": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),

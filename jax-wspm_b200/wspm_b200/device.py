@@ -35,7 +35,7 @@ def _require_cuda(t, dtype, name, numel=None):
 class DeviceMesh:
     """Mesh + pattern on the GPU.  ``points`` (N, dim) float64, ``elements`` (E, dim+1)."""
 
-    def __init__(self, points, elements, device=None, pattern=None):
+    def __init__(self, points, elements, device=None, pattern=None, layout="auto", extra_pairs=None):
         points = np.ascontiguousarray(points, dtype=np.float64)
         elements = np.ascontiguousarray(elements, dtype=np.int64)
         if elements.ndim != 2 or elements.shape[1] != points.shape[1] + 1:
@@ -46,7 +46,8 @@ class DeviceMesh:
         self.points_host, self.elements_host = points, elements
         self.n_nodes, self.dim = points.shape
         self.n_elems, self.nv = elements.shape
-        self.pattern = pattern if pattern is not None else Pattern(elements, self.n_nodes)
+        self.pattern = pattern if pattern is not None else Pattern(elements, self.n_nodes, layout=layout,
+                                                                   extra_pairs=extra_pairs)
         pat = self.pattern
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self.conn = t(elements.astype(np.int32))
@@ -60,13 +61,15 @@ class DeviceMesh:
         self.inc_elem = t(pat.inc_elem)
         self.inc_slots = t(pat.inc_slots.view(np.int32))
         self.sell_index = t(pat.sell_index)
+        self.diag_offsets = t(pat.diag_offsets if pat.n_diags else np.zeros(1, dtype=np.int32))
         self.c_mesh = _lib.WspmMesh(self.n_nodes, self.n_elems, self.dim, self.nv, self.conn.data_ptr(),
                                     self.coords.data_ptr())
         self.c_pat = _lib.WspmPattern(pat.n_rows, pat.n_slices, pat.max_width, pat.max_inc, pat.nnz_padded,
                                       self.slice_ptr.data_ptr(), self.slice_width.data_ptr(), self.cols.data_ptr(),
                                       self.diag_pos.data_ptr(), self.inc_ptr.data_ptr(),
                                       self.inc_width.data_ptr(), self.inc_elem.data_ptr(),
-                                      self.inc_slots.data_ptr())
+                                      self.inc_slots.data_ptr(), pat.n_diags, 0,
+                                      self.diag_offsets.data_ptr() if pat.n_diags else None)
 
     @property
     def nnz_padded(self):
@@ -219,3 +222,91 @@ def krylov_solve(dm, vals, b, x0, solver="cg", dinv=None, tol=1e-10, atol=0.0, m
         ctypes.byref(dm.c_pat), dptr(vals), dptr(b), dptr(x), dptr(dinv), _lib.SOLVERS[solver], float(tol),
         float(atol), int(maxiter), int(restart), dptr(work), work.numel(), dptr(ws.result), _stream()))
     return x, ws.result
+
+
+# ---------------------------------------------------------------- transport
+def edge_pairs(nodes):
+    """Consecutive pairs of a boundary-node list (the reference's edges: boundary.py loops i -> (n[i], n[i+1]))."""
+    nodes = np.asarray(nodes, dtype=np.int64)
+    return np.stack([nodes[:-1], nodes[1:]], axis=1) if nodes.size > 1 else np.zeros((0, 2), dtype=np.int64)
+
+
+class BoundaryEdges:
+    """Boundary edges of a node list, grouped per boundary node for ``wspm_apply_edge_terms``.
+
+    The edges are the consecutive pairs of ``nodes`` in the given order (the
+    reference sorts node sets by id, boundary.py:482-547); the edge Jacobian is
+    (x_J - x_I) / 2 as in the reference (horizontal edges).
+    """
+
+    def __init__(self, dm, nodes):
+        nodes = np.asarray(nodes, dtype=np.int64)
+        nb = nodes.size if nodes.size > 1 else 0
+        self.nodes = nodes
+        x = dm.points_host[:, 0]
+        cnt = np.zeros(max(nb, 1), dtype=np.int32)
+        loc = np.zeros(2 * max(nb, 1), dtype=np.int32)
+        oth = np.zeros(2 * max(nb, 1), dtype=np.int32)
+        kot = np.zeros(2 * max(nb, 1), dtype=np.int32)
+        jac = np.zeros(2 * max(nb, 1), dtype=np.float64)
+        for t in range(nb):
+            c = 0
+            if t > 0:                                  # edge t-1 = (nodes[t-1], nodes[t]): this node is J
+                I, J = nodes[t - 1], nodes[t]
+                loc[2 * t + c], oth[2 * t + c], jac[2 * t + c] = 1, I, (x[J] - x[I]) / 2
+                kot[2 * t + c] = dm.pattern.slot([J], [I])[0]
+                c += 1
+            if t < nb - 1:                             # edge t = (nodes[t], nodes[t+1]): this node is I
+                I, J = nodes[t], nodes[t + 1]
+                loc[2 * t + c], oth[2 * t + c], jac[2 * t + c] = 0, J, (x[J] - x[I]) / 2
+                kot[2 * t + c] = dm.pattern.slot([I], [J])[0]
+                c += 1
+            cnt[t] = c
+        t_ = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dm.device)  # noqa: E731
+        self._keep = [t_(nodes[:max(nb, 1)].astype(np.int32) if nb else np.zeros(1, np.int32)), t_(cnt), t_(loc),
+                      t_(oth), t_(kot), t_(jac)]
+        node_t, cnt_t, loc_t, oth_t, kot_t, jac_t = self._keep
+        self.c = _lib.WspmEdges(nb, 0, node_t.data_ptr(), cnt_t.data_ptr(), loc_t.data_ptr(), oth_t.data_ptr(),
+                                kot_t.data_ptr(), jac_t.data_ptr())
+        self.n_bnodes = nb
+
+
+EDGE_NEUMANN, EDGE_DRAINAGE_WATER, EDGE_CAUCHY, EDGE_DRAINAGE_SOLUTE = 0, 1, 2, 3
+
+
+def apply_edge_terms(dm, edges, mode, rhs, vals=None, flux=0.0, c_in=0.0, K=None, theta=None):
+    """In place: boundary-edge contributions to rhs (and to vals for the matrix modes)."""
+    check("apply_edge_terms", lib.wspm_apply_edge_terms(ctypes.byref(dm.c_pat), ctypes.byref(edges.c), int(mode),
+                                                        float(flux), float(c_in), dptr(K), dptr(theta), dptr(vals),
+                                                        dptr(rhs), _stream()))
+    return vals, rhs
+
+
+def flux_dispersion(dm, h, phi, DL, DT, Dm):
+    """(qx, qz, |q|, Dxx, Dxz, Dzz, theta) per node (transport_utilities.py:118-192)."""
+    _require_cuda(h, torch.float64, "h", dm.n_nodes)
+    out = [torch.empty_like(h) for _ in range(7)]
+    check("flux_dispersion_2d", lib.wspm_flux_dispersion_2d(
+        ctypes.byref(dm.c_mesh), ctypes.byref(dm.c_pat), dptr(h), _lib.dbl_array(phi), float(DL), float(DT),
+        float(Dm), *[dptr(t) for t in out], _stream()))
+    return tuple(out)
+
+
+def assemble_adr(dm, theta, qx, qz, Dxx, Dxz, Dzz, c_n, dt, quad_points, weights, mu=0.0, sorption=0.0,
+                 mu_up=0.0, c_up=None, lumped=False, want_dinv=True):
+    """(vals, rhs, dinv): A = M/dt + K and b = M c_n/dt + F (consistent or row-lumped mass)."""
+    n = dm.n_nodes
+    for name, t in (("theta", theta), ("qx", qx), ("qz", qz), ("Dxx", Dxx), ("Dxz", Dxz), ("Dzz", Dzz),
+                    ("c_n", c_n)):
+        _require_cuda(t, torch.float64, name, n)
+    if c_up is not None:
+        _require_cuda(c_up, torch.float64, "c_up", n)
+    q = np.ascontiguousarray(quad_points, dtype=np.float64).ravel()
+    w = np.ascontiguousarray(weights, dtype=np.float64).ravel()
+    vals, rhs = dm.empty_vals(), dm.vec()
+    dinv = dm.vec() if want_dinv else None
+    check("assemble_adr_2d", lib.wspm_assemble_adr_2d(
+        ctypes.byref(dm.c_mesh), ctypes.byref(dm.c_pat), dptr(theta), dptr(qx), dptr(qz), dptr(Dxx), dptr(Dxz),
+        dptr(Dzz), dptr(c_n), dptr(c_up), float(mu), float(sorption), float(mu_up), int(bool(lumped)),
+        _lib.dbl_array(q), _lib.dbl_array(w), len(w), float(dt), dptr(vals), dptr(rhs), dptr(dinv), _stream()))
+    return vals, rhs, dinv

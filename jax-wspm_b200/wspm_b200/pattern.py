@@ -12,16 +12,26 @@ Layout (all int arrays little-endian, ready for device upload):
   The node -> element incidence uses the same sliced layout; each incidence
   packs the local vertex of the row's node (2 bits) and, for every vertex j
   of the element, the position of that vertex's column in the row (6 bits).
+
+DIA variant (``layout="dia"``, chosen by ``"auto"`` when the matrix has at
+most ``DIA_MAX`` distinct column offsets, i.e. on structured meshes): entry k
+of row i is the k-th diagonal, stored at k*ld + i (ld = 32 * n_slices), with
+column i + offsets[k]; rows hold zeros where a diagonal has no entry.  The
+sparse kernels then read no column indices at all.
 """
 import numpy as np
 
 SLICE = 32
+DIA_MAX = 16
 
 
 class Pattern:
-    """Host arrays of a SELL-32 pattern + node->element incidence."""
+    """Host arrays of a SELL-32 (or DIA) pattern + node->element incidence."""
 
-    def __init__(self, elements, n_nodes):
+    def __init__(self, elements, n_nodes, layout="auto", extra_pairs=None):
+        """``extra_pairs`` (k, 2): node pairs that must have matrix slots although no element
+        contains both (boundary edges whose end points are not an element edge); both (i, j) and
+        (j, i) are added."""
         el = np.ascontiguousarray(elements, dtype=np.int64)
         E, nv = el.shape
         N = int(n_nodes)
@@ -29,6 +39,10 @@ class Pattern:
         # --- unique (row, col) pairs, ascending
         rows = np.repeat(el, nv, axis=1).ravel()
         cols = np.tile(el, (1, nv)).ravel()
+        if extra_pairs is not None and len(extra_pairs):
+            ep = np.asarray(extra_pairs, dtype=np.int64).reshape(-1, 2)
+            rows = np.concatenate([rows, ep[:, 0], ep[:, 1]])
+            cols = np.concatenate([cols, ep[:, 1], ep[:, 0]])
         keys = np.unique(rows * N + cols)
         r = keys // N
         c = keys - r * N
@@ -40,32 +54,56 @@ class Pattern:
         self.csr_indptr, self.csr_indices = rowptr, c.astype(np.int32)
         self.nnz = int(keys.size)
         pos = np.arange(keys.size, dtype=np.int64) - rowptr[r]
-        # --- slices
         ns = (N + SLICE - 1) // SLICE
         self.n_slices = ns
-        pad_counts = np.zeros(ns * SLICE, dtype=np.int64)
-        pad_counts[:N] = counts
-        width = pad_counts.reshape(ns, SLICE).max(axis=1)
-        if width.max() > 63:
-            raise ValueError("row length above 63 is not supported by the SELL-32 kernels")
-        self.slice_width = width.astype(np.int32)
-        self.slice_ptr = np.zeros(ns + 1, dtype=np.int64)
-        np.cumsum(width * SLICE, out=self.slice_ptr[1:])
-        self.nnz_padded = int(self.slice_ptr[-1])
-        self.max_width = int(width.max())
-        lane = r % SLICE
-        self.sell_index = self.slice_ptr[r // SLICE] + SLICE * pos + lane      # CSR entry -> SELL slot
-        sell_cols = np.empty(self.nnz_padded, dtype=np.int32)
-        # padding: column = own row
-        all_rows = np.arange(ns * SLICE, dtype=np.int64)
-        for_pad = np.minimum(all_rows, N - 1)
-        slot_row = np.repeat(for_pad.reshape(ns, SLICE), width, axis=0)      # (sum w, 32)
-        sell_cols[:] = slot_row.ravel().astype(np.int32)
-        sell_cols[self.sell_index] = c.astype(np.int32)
-        self.cols = sell_cols
-        self.diag_pos = np.empty(N, dtype=np.int32)
-        dmask = r == c
-        self.diag_pos[r[dmask]] = pos[dmask].astype(np.int32)
+        offs = np.unique(c - r)
+        if layout not in ("auto", "sell", "dia"):
+            raise ValueError(f"unknown layout {layout!r}")
+        self.layout = "dia" if (layout == "dia" or (layout == "auto" and offs.size <= DIA_MAX)) else "sell"
+        if self.layout == "dia":
+            if offs.size > 63:
+                raise ValueError("too many diagonals for the DIA layout")
+            nd = int(offs.size)
+            ld = ns * SLICE
+            self.ld = ld
+            self.diag_offsets = offs.astype(np.int32)
+            self.slice_width = np.full(ns, nd, dtype=np.int32)
+            self.slice_ptr = (np.arange(ns + 1, dtype=np.int64) * SLICE)
+            self.nnz_padded = nd * ld
+            self.max_width = nd
+            kpos = np.searchsorted(offs, c - r)
+            self.sell_index = kpos * ld + r
+            all_i = np.arange(ld, dtype=np.int64)
+            self.cols = np.clip(all_i[None, :] + offs[:, None], 0, N - 1).astype(np.int32).ravel()
+            self.diag_pos = np.full(N, int(np.searchsorted(offs, 0)), dtype=np.int32)
+            self._slot = lambda rows, cols_: np.searchsorted(offs, cols_ - rows)
+        else:
+            self.ld = 0
+            self.diag_offsets = np.zeros(0, dtype=np.int32)
+            pad_counts = np.zeros(ns * SLICE, dtype=np.int64)
+            pad_counts[:N] = counts
+            width = pad_counts.reshape(ns, SLICE).max(axis=1)
+            if width.max() > 63:
+                raise ValueError("row length above 63 is not supported by the SELL-32 kernels")
+            self.slice_width = width.astype(np.int32)
+            self.slice_ptr = np.zeros(ns + 1, dtype=np.int64)
+            np.cumsum(width * SLICE, out=self.slice_ptr[1:])
+            self.nnz_padded = int(self.slice_ptr[-1])
+            self.max_width = int(width.max())
+            lane = r % SLICE
+            self.sell_index = self.slice_ptr[r // SLICE] + SLICE * pos + lane      # CSR entry -> SELL slot
+            sell_cols = np.empty(self.nnz_padded, dtype=np.int32)
+            all_rows = np.arange(ns * SLICE, dtype=np.int64)
+            for_pad = np.minimum(all_rows, N - 1)                                   # padding: own row
+            slot_row = np.repeat(for_pad.reshape(ns, SLICE), width, axis=0)
+            sell_cols[:] = slot_row.ravel().astype(np.int32)
+            sell_cols[self.sell_index] = c.astype(np.int32)
+            self.cols = sell_cols
+            self.diag_pos = np.empty(N, dtype=np.int32)
+            dmask = r == c
+            self.diag_pos[r[dmask]] = pos[dmask].astype(np.int32)
+            self._slot = lambda rows, cols_: np.searchsorted(keys, rows * N + cols_) - rowptr[rows]
+        self.n_diags = int(self.diag_offsets.size)
         # --- incidence: for each (node, element) in ascending element order
         inc_node = el.ravel()
         inc_elem = np.repeat(np.arange(E, dtype=np.int64), nv)
@@ -90,11 +128,21 @@ class Pattern:
         node_rows = inc_node
         for j in range(nv):
             colj = el[inc_elem, j]
-            kj = np.searchsorted(keys, node_rows * N + colj) - rowptr[node_rows]
+            kj = self._slot(node_rows, colj)
             packed |= (kj.astype(np.uint32) & 63) << np.uint32(2 + 6 * j)
         inc_s = np.zeros(int(self.inc_ptr[-1]), dtype=np.uint32)
         inc_s[islot] = packed
         self.inc_elem, self.inc_slots = inc_e, inc_s
+
+    def slot(self, i, j):
+        """Row position k of column j in row i (i, j arrays)."""
+        return np.asarray(self._slot(np.asarray(i, dtype=np.int64), np.asarray(j, dtype=np.int64)))
+
+    def entry_pos(self, i, k):
+        """Storage index of entry k of row i."""
+        if self.layout == "dia":
+            return k * self.ld + i
+        return self.slice_ptr[i // SLICE] + SLICE * k + i % SLICE
 
     # ---- conversions used by tests and by the reference-API shims ----------
     def sell_from_csr_values(self, data):

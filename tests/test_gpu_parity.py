@@ -43,13 +43,16 @@ def test_soil_models(model, phi):
     h = np.concatenate([-10 ** rng.uniform(-4, 1.5, 5000), [0.0, 1e-300, -0.0, 0.5, -1e-300]])
     C, K, th = dev().soil(model, cu(h), phi)
     ref = (osoil.van_genuchten_model if model == "vg" else osoil.exponential_model)(h, phi)
-    # theta and C are well conditioned; K = Ks Se^.5 (1-(1-Se^(1/m))^m)^2 cancels as Se -> 1, amplifying
-    # the last-ulp differences between two correct pow() implementations by ~1/(1-Se^(1/m))
+    # theta and C are well conditioned; K = Ks Se^.5 (1-(1-Se^(1/m))^m)^2 cancels at both ends, amplifying
+    # the last-ulp differences between two correct pow() implementations
+    # (wet end, Se^(1/m) -> 1) and as Se -> 0 (1 - (1 - u)^m ~ m u loses the digits of u)
     amp = np.ones_like(h)
     if model == "vg":
         m = phi[4]
         se = np.clip((ref[2] - phi[2]) / (phi[1] - phi[2]), 0, 1)
-        amp = 1.0 + 1.0 / np.maximum(1.0 - se ** (1.0 / m), 1e-300)
+        u = se ** (1.0 / m)
+        t = 1.0 - (1.0 - u) ** m
+        amp = 1.0 + 1.0 / np.maximum(1.0 - u, 1e-300) + 1.0 / np.maximum(t, 1e-300)
     for name, got, want in zip("CKt", (C, K, th), ref):
         rtol = 4e-14 * (amp if name == "K" else 1.0)
         got = host(got)
@@ -82,12 +85,13 @@ def _assembly_case(kind):
     return pts, el, model, phi, Ks, h
 
 
-@pytest.mark.parametrize("kind", ["tri-exp", "tri-vg-ks", "tri-ragged", "tet-exp"])
-def test_assembly_matches_oracle(kind):
+@pytest.mark.parametrize("kind,layout", [("tri-exp", "dia"), ("tri-exp", "sell"), ("tri-vg-ks", "auto"),
+                                         ("tri-ragged", "auto"), ("tet-exp", "dia"), ("tet-exp", "sell")])
+def test_assembly_matches_oracle(kind, layout):
     from wspm_b200.engine import default_rule
     pts, el, model, phi, Ks, h = _assembly_case(kind)
     D = dev()
-    dm = D.DeviceMesh(pts, el)
+    dm = D.DeviceMesh(pts, el, layout=layout)
     fn = osoil.van_genuchten_model if model == "vg" else osoil.exponential_model
     C, K, th_m = fn(h, phi)
     th_n = fn(h - 0.01, phi)[2]
@@ -108,7 +112,8 @@ def test_assembly_matches_oracle(kind):
     assert np.all(host(vals)[mask] == 0.0)
 
 
-def test_assembly_with_dirichlet_rows_and_apply_dirichlet():
+@pytest.mark.parametrize("layout", ["dia", "sell"])
+def test_assembly_with_dirichlet_rows_and_apply_dirichlet(layout):
     from wspm_b200.engine import default_rule
     pts, el = mesh.structured_triangles(25, 15.24)
     top, bottom = opic.boundary_nodes_2d(pts, "Test1")
@@ -119,7 +124,7 @@ def test_assembly_with_dirichlet_rows_and_apply_dirichlet():
     A_ref, b_ref = oasm.assemble_richards(el, len(pts), pts, th, th, h, K, C, 1e-3)
     A_ref, b_ref = oasm.apply_dirichlet_rows(A_ref, b_ref, nodes, values)
     D = dev()
-    dm = D.DeviceMesh(pts, el)
+    dm = D.DeviceMesh(pts, el, layout=layout)
     bc = D.merge_dirichlet(len(pts), [(top, hup), (bottom, -15.0)])
     Q, W = default_rule(2)
     vals, rhs, dinv, _ = D.assemble_richards(dm, cu(th), cu(th), cu(h), cu(K), cu(C), Q, W, 1e-3, bc_val=cu(bc))
@@ -135,11 +140,12 @@ def test_assembly_with_dirichlet_rows_and_apply_dirichlet():
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-def test_spmv(dtype):
+@pytest.mark.parametrize("layout", ["dia", "sell"])
+def test_spmv(dtype, layout):
     rng = np.random.default_rng(3)
     pts, el = mesh.kuhn_tetrahedra(7)
     D = dev()
-    dm = D.DeviceMesh(pts, el)
+    dm = D.DeviceMesh(pts, el, layout=layout)
     data = rng.standard_normal(dm.pattern.nnz)
     x = rng.standard_normal(len(pts))
     vals = cu(dm.pattern.sell_from_csr_values(data), dtype)
@@ -163,12 +169,14 @@ def _linear_system(n=30, dirichlet=True):
     return pts, el, A, b, h
 
 
-@pytest.mark.parametrize("solver,precond", [("cg", "jacobi"), ("cg", "none"), ("bicgstab", "none"),
-                                            ("bicgstab", "jacobi"), ("gmres", "jacobi"), ("gmres", "none")])
-def test_krylov_solve_matches_oracle(solver, precond):
+@pytest.mark.parametrize("solver,precond,layout", [("cg", "jacobi", "dia"), ("cg", "jacobi", "sell"),
+                                                   ("cg", "none", "dia"), ("bicgstab", "none", "sell"),
+                                                   ("bicgstab", "jacobi", "dia"), ("gmres", "jacobi", "dia"),
+                                                   ("gmres", "none", "sell")])
+def test_krylov_solve_matches_oracle(solver, precond, layout):
     pts, el, A, b, h = _linear_system()
     D = dev()
-    dm = D.DeviceMesh(pts, el)
+    dm = D.DeviceMesh(pts, el, layout=layout)
     vals = cu(dm.pattern.sell_from_csr_values(A.data))
     dinv = D.jacobi_dinv(dm, vals) if precond == "jacobi" else None
     x_ref, k_ref = okry.solve_system(A, b, h, solver, precond, tol=1e-10, maxiter=400, restart=30)
@@ -205,7 +213,7 @@ def test_zero_rhs_gmres_returns_x0():
     assert host(res)[1] == 0
 
 
-def _engine_test_case(case, n, solver, precond, **kw):
+def _engine_test_case(case, n, solver, precond, layout="auto", **kw):
     from wspm_b200.device import DeviceMesh, merge_dirichlet
     from wspm_b200.engine import PicardEngine
     pts, tri = mesh.structured_triangles(n, 15.24)
@@ -213,7 +221,8 @@ def _engine_test_case(case, n, solver, precond, **kw):
     h0 = -15.24 * np.ones(len(pts))
     hup = opic.upper_bc(case, pts[top, 0], EXP[0], np.exp(EXP[0] * h0[top]))
     bc = merge_dirichlet(len(pts), [(top, hup), (bottom, -15.0)])
-    eng = PicardEngine(DeviceMesh(pts, tri), "exp", EXP, bc_val=bc, solver=solver, precond=precond, **kw)
+    eng = PicardEngine(DeviceMesh(pts, tri, layout=layout), "exp", EXP, bc_val=bc, solver=solver, precond=precond,
+                       **kw)
     return pts, tri, eng, h0
 
 
@@ -222,8 +231,8 @@ def test_picard_engine_reproduces_csv_golden_mesh25(case):
     import json
     rows = [r for r in json.load(open(os.path.join(GOLD, "re2d_metrics.json")))
             if r["test_case"] == case and r["mesh"] == 25 and r["solver"] == "cg" and r["precond"] == "jacobi"]
-    pts, tri, eng, h0 = _engine_test_case(case, 25, "cg", "jacobi", picard_tol=1e-4, picard_maxiter=30,
-                                          picard_relative=False)
+    pts, tri, eng, h0 = _engine_test_case(case, 25, "cg", "jacobi", layout="sell" if case == "Test3" else "auto",
+                                          picard_tol=1e-4, picard_maxiter=30, picard_relative=False)
     res = eng.run(h0, 1e-3, 0.25, theta_at_end=False)
     m = analytic.final_errors(pts, res["pressure_head"][-1], res["theta"][-1], res["times"][-1], int(case[-1]))
     assert res["iterations"].sum() == rows[0]["iterations"]

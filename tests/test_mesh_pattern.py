@@ -40,6 +40,15 @@ def test_kuhn_tetrahedra_match_reference_file():
     assert np.all(np.linalg.det(J) > 0)
 
 
+def test_auto_layout_choice():
+    p, t = mesh.structured_triangles(12)
+    P = Pattern(t, len(p))
+    assert P.layout == "dia" and P.n_diags == 7
+    p, t = mesh.kuhn_tetrahedra(4)
+    P = Pattern(t, len(p))
+    assert P.layout == "dia" and P.n_diags == 15
+
+
 @pytest.mark.parametrize("n", [1, 3, 8, 33])
 def test_nnz_formula_2d(n):
     p, t = mesh.structured_triangles(n)
@@ -54,8 +63,9 @@ def test_nnz_formula_3d(n):
     assert P.nnz == (n + 1) ** 3 + 2 * (3 * n * (n + 1) ** 2 + 3 * n * n * (n + 1) + n ** 3)
 
 
-@pytest.mark.parametrize("kind", ["tri", "tet", "ragged"])
-def test_pattern_roundtrip_and_incidence(kind):
+@pytest.mark.parametrize("kind,layout", [("tri", "sell"), ("tri", "dia"), ("tet", "sell"), ("tet", "dia"),
+                                         ("ragged", "sell"), ("ragged", "auto")])
+def test_pattern_roundtrip_and_incidence(kind, layout):
     rng = np.random.default_rng(0)
     if kind == "tri":
         p, t = mesh.structured_triangles(7)
@@ -66,7 +76,9 @@ def test_pattern_roundtrip_and_incidence(kind):
         perm = rng.permutation(len(p))
         inv = np.argsort(perm)
         p, t = p[perm], inv[t][rng.permutation(len(t))]
-    P = Pattern(t, len(p))
+    P = Pattern(t, len(p), layout=layout)
+    if kind == "ragged":
+        assert P.layout == "sell"          # permuted numbering: offsets are not a small set
     nv = t.shape[1]
     rows = np.repeat(t, nv, axis=1).ravel()
     cols = np.tile(t, (1, nv)).ravel()
@@ -92,8 +104,8 @@ def test_pattern_roundtrip_and_incidence(kind):
             assert t[e, pk & 3] == i
             for j in range(nv):
                 kj = (pk >> (2 + 6 * j)) & 63
-                assert P.cols[P.slice_ptr[s] + 32 * kj + lane] == t[e, j]
-        assert P.cols[P.slice_ptr[s] + 32 * P.diag_pos[i] + lane] == i
+                assert P.cols[P.entry_pos(i, kj)] == t[e, j]
+        assert P.cols[P.entry_pos(i, P.diag_pos[i])] == i
 
 
 def test_loader_errors(tmp_path):
