@@ -207,6 +207,27 @@ int wspm_krylov_solve(const wspm_pattern *pat, const double *vals,
 int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const void *vals, const void *b, void *x,
                        const void *dinv, int32_t iters, double *work, int64_t work_doubles, void *stream);
 
+/* Allocation-free Jacobi-CG solve.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory -- typically code running
+ * inside a JAX program (the reference's runtime), whose allocator reserves
+ * most of the GPU's memory up front, or code where cudaMalloc is not allowed
+ * (inside a stream capture) or too slow.  Same solve as wspm_krylov_solve with
+ * WSPM_SOLVER_CG (x holds x0 on entry, the solution on exit; dinv == NULL:
+ * no preconditioner; result = {status, iterations, 0, 0}), but the Krylov
+ * vectors and solver state live in a static device array inside the library
+ * instead of a caller-supplied workspace, and nothing is allocated.
+ * Limits: at most WSPM_NOALLOC_MAX_ROWS rows (larger systems return
+ * WSPM_BAD_ARG before anything is launched); the scratch (about 11 MB) is held
+ * by every GPU that loads the library until the process exits.  All calls on
+ * a device share that one array: calls that overlap on the GPU (two streams,
+ * or two host threads on one device) race and corrupt each other.  The first
+ * call on each device looks up the array's address and caches it; make that
+ * first call before any stream capture.                                    */
+#define WSPM_NOALLOC_MAX_ROWS 262144
+int wspm_cg_solve_noalloc(const wspm_pattern *pat, const double *vals, const double *b, double *x,
+                          const double *dinv, double tol, double atol, int32_t maxiter,
+                          int32_t *result, void *stream);
+
 /* ---- Picard time step (device-resident loop in a CUDA graph) ------------- */
 /* RichardsSolver.solve_timestep, src/solvers/richards_solver_v2.py:107-168
  * (relative Picard error) and RichardsSolver3D.solve_timestep,

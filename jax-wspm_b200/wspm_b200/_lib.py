@@ -15,6 +15,7 @@ WSPM_BAD_ARG, WSPM_CUDA_ERROR, WSPM_UNSUPPORTED = 10, 11, 12
 SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2}
 PRECONDS = {"none": 0, None: 0, "jacobi": 1}
 SOIL_VG, SOIL_EXP = 0, 1
+NOALLOC_MAX_ROWS = 262144     # WSPM_NOALLOC_MAX_ROWS in include/wspm.h
 
 c_int32, c_int64, c_double, c_void_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -79,6 +80,8 @@ _SIGS = {
                                     c_double, c_int32, c_int32, c_void_p, c_int64, c_void_p, c_void_p]),
     "wspm_cg_iterations": (c_int32, [P(WspmPattern), c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                                      c_void_p, c_int64, c_void_p]),
+    "wspm_cg_solve_noalloc": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double,
+                                        c_int32, c_void_p, c_void_p]),
     "wspm_picard_workspace_doubles": (c_int64, [c_int32, c_int32]),
     "wspm_picard_create": (c_int32, [P(WspmPicardDesc), P(c_void_p)]),
     "wspm_picard_step": (c_int32, [c_void_p, c_void_p]),
