@@ -287,6 +287,34 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def cg_probe(args):
+    """Small profiling target: one soil + assembly launch, then N iterations of the persistent CG kernel."""
+    import ctypes
+    import torch
+    from wspm_b200 import _lib
+    from wspm_b200.device import DeviceMesh, assemble_richards, merge_dirichlet, soil
+    from wspm_b200.engine import default_rule
+    torch.cuda.set_device(0)
+    pts, tri, Ks, top = workload(args.n, args.seed)
+    N = len(pts)
+    dm = DeviceMesh(pts, tri)
+    h = torch.full((N,), -1.0, dtype=torch.float64, device="cuda")
+    C, K, th = soil("vg", h, VG_PHI_UNIT_KS)
+    bc = torch.as_tensor(merge_dirichlet(N, [(top, -0.1)]), device="cuda")
+    Q, W = default_rule(2)
+    vals, rhs, dinv, vals32 = assemble_richards(dm, th, th, h, K, C, Q, W, 1e-4, bc_val=bc,
+                                                Ks_elem=torch.as_tensor(Ks, device="cuda"), want_f32=True)
+    fp32 = args.cg_probe == "fp32"
+    v, b, x, d = (vals32, rhs.float(), h.float(), dinv.float()) if fp32 else (vals, rhs, h.clone(), dinv)
+    work = torch.empty(int(_lib.lib.wspm_krylov_workspace_doubles(N, 0, 0)), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check("cg_iterations", _lib.lib.wspm_cg_iterations(
+        ctypes.byref(dm.c_pat), int(fp32), _lib.dptr(v), _lib.dptr(b), _lib.dptr(x), _lib.dptr(d), args.probe_iters,
+        _lib.dptr(work), work.numel(), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    print(f"cg probe {args.cg_probe}: {args.probe_iters} iterations, |x| = {float(torch.linalg.norm(x.double())):.6e}")
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -298,12 +326,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--inner-tol", type=float, default=1e-5,
                     help="floor of the relative tolerance of each FP32 solve in the refinement loop")
+    ap.add_argument("--cg-probe", choices=["fp64", "fp32"], default=None,
+                    help="profiling target: assemble the workload once and run --probe-iters CG iterations "
+                         "through wspm_cg_iterations, then exit (no JSON line)")
+    ap.add_argument("--probe-iters", type=int, default=4)
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Picard/Krylov loops from the host (same kernels; for ncu, which cannot "
                          "profile kernels inside conditional graphs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.cg_probe:
+        return cg_probe(args)
 
     import torch
     from wspm_b200.device import DeviceMesh, merge_dirichlet

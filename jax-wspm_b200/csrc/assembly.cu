@@ -105,8 +105,52 @@ __device__ __forceinline__ void p1_geometry(const double *__restrict__ coords, c
     }
 }
 
+// Same as p1_geometry, from vertex coordinates already in registers.
 template <int DIM>
-__global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
+__device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM], double (&G)[DIM][DIM + 1],
+                                                double &detJ) {
+    if constexpr (DIM == 2) {
+        const double J00 = X[1][0] - X[0][0], J01 = X[1][1] - X[0][1];
+        const double J10 = X[2][0] - X[0][0], J11 = X[2][1] - X[0][1];
+        detJ = J00 * J11 - J01 * J10;
+        const double id = 1.0 / detJ;
+        G[0][1] = J11 * id;  G[1][1] = -J10 * id;
+        G[0][2] = -J01 * id; G[1][2] = J00 * id;
+        G[0][0] = -(G[0][1] + G[0][2]);
+        G[1][0] = -(G[1][1] + G[1][2]);
+    } else {
+        double J[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) J[r][c] = X[r + 1][c] - X[0][c];
+        const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+        const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+        const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+        detJ = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+        const double id = 1.0 / detJ;
+        double inv[3][3];
+        inv[0][0] = c00 * id;
+        inv[1][0] = c01 * id;
+        inv[2][0] = c02 * id;
+        inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+        inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+        inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+        inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+        inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+        inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            G[d][1] = inv[d][0];
+            G[d][2] = inv[d][1];
+            G[d][3] = inv[d][2];
+            G[d][0] = -((inv[d][0] + inv[d][1]) + inv[d][2]);
+        }
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128, 4) richards_rows_kernel(RichardsAsmArgs a) {
     constexpr int NV = DIM + 1;
     extern __shared__ double acc_sm[];   // [max_width][blockDim.x]
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -144,36 +188,69 @@ __global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
         double bsum = 0.0;
         const int deg = a.inc_width[s];
         const int64_t ib = a.inc_ptr[s] + lane;
-        for (int k = 0; k < deg; ++k) {
-            const int e = a.inc_elem[ib + (int64_t)kSlice * k];
-            if (e < 0) break;
-            const uint32_t packed = a.inc_slots[ib + (int64_t)kSlice * k];
-            const int li = packed & 3;
-            int nd[NV];
+        // incidences in chunks of CH: the chunk's element ids, then its connectivity, then the
+        // vertex data are each loaded together, so a row pays 3 dependent memory round trips
+        // per chunk instead of per element
+        constexpr int CH = DIM == 2 ? 4 : 2;
+#pragma unroll 1
+        for (int k0 = 0; k0 < deg; k0 += CH) {
+            int ev[CH];
+            uint32_t pk[CH];
 #pragma unroll
-            for (int j = 0; j < NV; ++j) nd[j] = a.conn[(int64_t)e * NV + j];
-            double G[DIM][NV], detJ;
-            p1_geometry<DIM>(a.coords, nd, G, detJ);
-            double Kbar = 0.0;
-#pragma unroll
-            for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], a.K[nd[j]], Kbar);
-            if (a.Ks_elem) Kbar *= a.Ks_elem[e];
-            const double kd = Kbar * detJ;
-            const double Ml = a.mcoef[li] * detJ;
-            double gli[DIM];
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) gli[d] = G[d][li];
-#pragma unroll
-            for (int j = 0; j < NV; ++j) {
-                double gg = 0.0;
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) gg = fma(gli[d], G[d][j], gg);
-                double v = kd * gg;
-                if (j == li) v += inv_dt * (Ml * Ci);
-                const int kpos = (packed >> (2 + 6 * j)) & 63;
-                acc[kpos * stride] += v;
+            for (int c = 0; c < CH; ++c) {
+                ev[c] = -1;
+                pk[c] = 0u;
+                if (k0 + c < deg) {
+                    ev[c] = __ldg(a.inc_elem + ib + (int64_t)kSlice * (k0 + c));
+                    pk[c] = __ldg(a.inc_slots + ib + (int64_t)kSlice * (k0 + c));
+                }
             }
-            bsum += -kd * gli[DIM - 1] - inv_dt * (Ml * storage);
+            int nd[CH][NV];
+            double kse[CH];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const int e = ev[c] < 0 ? 0 : ev[c];
+#pragma unroll
+                for (int j = 0; j < NV; ++j) nd[c][j] = __ldg(a.conn + (int64_t)e * NV + j);
+                kse[c] = a.Ks_elem ? __ldg(a.Ks_elem + e) : 1.0;
+            }
+            double xyz[CH][NV][DIM], Kv[CH][NV];
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) xyz[c][j][d] = __ldg(a.coords + (int64_t)DIM * nd[c][j] + d);
+                    Kv[c][j] = __ldg(a.K + nd[c][j]);
+                }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                if (ev[c] < 0) continue;
+                const uint32_t packed = pk[c];
+                const int li = packed & 3;
+                double G[DIM][NV], detJ;
+                p1_geometry_xyz<DIM>(xyz[c], G, detJ);
+                double Kbar = 0.0;
+#pragma unroll
+                for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], Kv[c][j], Kbar);
+                if (a.Ks_elem) Kbar *= kse[c];
+                const double kd = Kbar * detJ;
+                const double Ml = a.mcoef[li] * detJ;
+                double gli[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) gli[d] = G[d][li];
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+                    double gg = 0.0;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) gg = fma(gli[d], G[d][j], gg);
+                    double v = kd * gg;
+                    if (j == li) v += inv_dt * (Ml * Ci);
+                    const int kpos = (packed >> (2 + 6 * j)) & 63;
+                    acc[kpos * stride] += v;
+                }
+                bsum += -kd * gli[DIM - 1] - inv_dt * (Ml * storage);
+            }
         }
         rhs_i = bsum;
         diag = acc[dpos * stride];

@@ -83,18 +83,17 @@ static int build_solve_graph(const wspm_pattern *pat, const double *vals, const 
     WSPM_CUDA_TRY(cudaGraphCreate(&g, 0));
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
     if (e == cudaSuccess) {
-        cudaGraphConditionalHandle h;
-        e = make_cond_handle(cs, &h);
+        cudaGraphConditionalHandle h = cudaGraphConditionalHandle();
+        // CG is one persistent kernel (no loop node); the other solvers loop in a WHILE node
+        if (solver != WSPM_SOLVER_CG) e = make_cond_handle(cs, &h);
         KrylovState *kst = nullptr;
         if (solver == WSPM_SOLVER_CG) {
             CgBuffers<double> w = carve_cg<double>(work, n, &used);
             kst = w.st;
             state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)kst, (int)(sizeof(KrylovState) / 4));
-            cg_enqueue_init<double>(A, vals, b, nullptr, x, x, dinv, w, tol, atol, maxiter, false, h, 1, cs);
-            if (e == cudaSuccess)
-                e = capture_while(cs, h, [&](cudaStream_t bs) {
-                    cg_enqueue_body<double>(A, vals, x, dinv, w, maxiter, h, 1, bs);
-                });
+            if (cg_persistent_enqueue<double>(A, vals, b, nullptr, x, dinv, w, tol, atol, maxiter, false, nullptr,
+                                              cs) != WSPM_OK && e == cudaSuccess)
+                e = cudaErrorLaunchFailure;
         } else if (solver == WSPM_SOLVER_BICGSTAB) {
             BicgBuffers w = carve_bicgstab(work, n, &used);
             kst = w.st;
@@ -308,25 +307,17 @@ extern "C" int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const v
     const Sell A = make_sell(pat);
     cudaStream_t st = (cudaStream_t)stream;
     int64_t used = 0;
-    const int bodies = (iters + 1) / 2;
+    // tolerance 0: the solve runs exactly `iters` iterations (the persistent CG kernel of the solver path)
     if (fp32) {
         CgBuffers<float> w = carve_cg<float>(work, pat->n_rows, &used);
         state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
-        cg_enqueue_init<float>(A, (const float *)vals, (const float *)b, nullptr, (const float *)x, (float *)x,
-                               (const float *)dinv, w, 0.0, 0.0, iters, false, cudaGraphConditionalHandle(), 0, st);
-        for (int k = 0; k < bodies; ++k)
-            cg_enqueue_body<float>(A, (const float *)vals, (float *)x, (const float *)dinv, w, iters,
-                                   cudaGraphConditionalHandle(), 0, st);
-    } else {
-        CgBuffers<double> w = carve_cg<double>(work, pat->n_rows, &used);
-        state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
-        cg_enqueue_init<double>(A, (const double *)vals, (const double *)b, nullptr, (const double *)x, (double *)x,
-                                (const double *)dinv, w, 0.0, 0.0, iters, false, cudaGraphConditionalHandle(), 0, st);
-        for (int k = 0; k < bodies; ++k)
-            cg_enqueue_body<double>(A, (const double *)vals, (double *)x, (const double *)dinv, w, iters,
-                                    cudaGraphConditionalHandle(), 0, st);
+        return cg_persistent_enqueue<float>(A, (const float *)vals, (const float *)b, nullptr, (float *)x,
+                                            (const float *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
     }
-    return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+    CgBuffers<double> w = carve_cg<double>(work, pat->n_rows, &used);
+    state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
+    return cg_persistent_enqueue<double>(A, (const double *)vals, (const double *)b, nullptr, (double *)x,
+                                         (const double *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
 }
 
 extern "C" const char *wspm_version(void) { return "wspm-b200 0.1 (sm_100a)"; }

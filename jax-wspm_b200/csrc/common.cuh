@@ -126,29 +126,36 @@ __device__ __forceinline__ int row_width(const Sell &A, int i) {
     return A.n_diags > 0 ? A.n_diags : __ldg(A.slice_width + (i >> 5));
 }
 
-// Row i of A times x, with x supplied by the functor xf(col).  MW > 0: all
-// column indices and values of the row are loaded before the gathers and
-// FMAs (memory-level parallelism); requires row width <= MW.
+// Row i of A times x, with x supplied by the functor xf(col).  MW > 0: the
+// row's entries are processed in groups of 4 whose column/value loads and
+// gathers are issued together (memory-level parallelism with a bounded
+// register footprint); requires row width <= MW.
 template <typename T, int MW, typename XF>
 __device__ __forceinline__ T sell_row_dot(const Sell &A, const T *__restrict__ vals, int i, XF xf) {
+    constexpr int G = 4;
     T acc = T(0);
     if (A.n_diags > 0) {
         const int nd = A.n_diags;
         const int last = A.n_rows - 1;
         if constexpr (MW > 0) {
-            T v[MW];
-            int c[MW];
+#pragma unroll 1
+            for (int k0 = 0; k0 < MW; k0 += G) {
+                if (k0 >= nd) break;
+                T v[G];
+                int c[G];
 #pragma unroll
-            for (int k = 0; k < MW; ++k) {
-                if (k < nd) {
-                    v[k] = __ldg(vals + (int64_t)k * A.ld + i);
-                    const int cc = i + __ldg(A.diag_off + k);
-                    c[k] = cc < 0 ? 0 : (cc > last ? last : cc);
+                for (int g = 0; g < G; ++g) {
+                    const int k = k0 + g;
+                    if (k < nd) {
+                        v[g] = __ldg(vals + (int64_t)k * A.ld + i);
+                        const int cc = i + __ldg(A.diag_off + k);
+                        c[g] = cc < 0 ? 0 : (cc > last ? last : cc);
+                    }
                 }
-            }
 #pragma unroll
-            for (int k = 0; k < MW; ++k)
-                if (k < nd) acc = fma(v[k], xf(c[k]), acc);
+                for (int g = 0; g < G; ++g)
+                    if (k0 + g < nd) acc = fma(v[g], xf(c[g]), acc);
+            }
         } else {
             for (int k = 0; k < nd; ++k) {
                 int cc = i + __ldg(A.diag_off + k);
@@ -162,18 +169,23 @@ __device__ __forceinline__ T sell_row_dot(const Sell &A, const T *__restrict__ v
     const int w = __ldg(A.slice_width + s);
     const int64_t base = __ldg(A.slice_ptr + s) + lane;
     if constexpr (MW > 0) {
-        int c[MW];
-        T v[MW];
+#pragma unroll 1
+        for (int k0 = 0; k0 < MW; k0 += G) {
+            if (k0 >= w) break;
+            T v[G];
+            int c[G];
 #pragma unroll
-        for (int k = 0; k < MW; ++k) {
-            if (k < w) {
-                c[k] = __ldg(A.cols + base + (int64_t)kSlice * k);
-                v[k] = __ldg(vals + base + (int64_t)kSlice * k);
+            for (int g = 0; g < G; ++g) {
+                const int k = k0 + g;
+                if (k < w) {
+                    c[g] = __ldg(A.cols + base + (int64_t)kSlice * k);
+                    v[g] = __ldg(vals + base + (int64_t)kSlice * k);
+                }
             }
-        }
 #pragma unroll
-        for (int k = 0; k < MW; ++k)
-            if (k < w) acc = fma(v[k], xf(c[k]), acc);
+            for (int g = 0; g < G; ++g)
+                if (k0 + g < w) acc = fma(v[g], xf(c[g]), acc);
+        }
     } else {
         for (int k = 0; k < w; ++k) {
             const int64_t o = base + (int64_t)kSlice * k;

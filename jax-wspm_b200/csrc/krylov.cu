@@ -214,6 +214,280 @@ template void cg_enqueue_body<double>(const Sell &, const double *, double *, co
 template void cg_enqueue_body<float>(const Sell &, const float *, float *, const float *, const CgBuffers<float> &,
                                      int, cudaGraphConditionalHandle, int, cudaStream_t);
 
+// ---------------------------------------------------------------- persistent CG
+// One cooperative launch runs the whole (preconditioned) CG solve.  Block b owns
+// a contiguous range of rows; each iteration is two phases separated by grid
+// barriers:
+//   phase 1: p_new = z + beta p_old ; q = A p_new (gathers z, p_old) ; partial p.q
+//   phase 2: x += alpha p ; r -= alpha q ; z = M r ; partials r.z, r.r
+// After a barrier every block sums all blocks' partials in the same fixed order,
+// so every block holds bitwise identical alpha/beta and takes the same
+// convergence decision (no broadcast, no atomics on the scalars).  Vectors that
+// other blocks write during the kernel are gathered with ld.global.cg (L2) so
+// that no stale L1 line is ever read.  Barrier waits are bounded: on timeout the
+// block records an error and every block leaves the loop at its next check.
+struct GridBarrier {
+    unsigned int count;
+    unsigned int gen;
+    int error;
+    int pad;
+};
+
+constexpr long long kBarrierSpinLimit = 20000000LL;   // ~ seconds; a legitimate wait is microseconds
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Returns false when the barrier failed (timeout anywhere in the grid).
+__device__ __forceinline__ bool grid_barrier(GridBarrier *gb, unsigned int nblocks, unsigned int &gen_local) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int g = gen_local;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(&gb->count, 1u);
+        if (arrived == nblocks - 1) {
+            gb->count = 0u;
+            __threadfence();
+            atomicExch(&gb->gen, g + 1u);
+        } else {
+            long long spins = 0;
+            while (ld_acquire_u32(&gb->gen) == g) {
+                if (++spins > kBarrierSpinLimit) {
+                    atomicExch(&gb->error, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        gen_local = g + 1u;
+        ok = (*(volatile int *)&gb->error) == 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Fixed-order sum of nb partials (layout [NV][nb]) by the whole block; result broadcast to all threads.
+template <typename T, int NV>
+__device__ __forceinline__ void block_reduce_partials(const T *partials, int nb, T (&out)[NV]) {
+    __shared__ T bc[NV];
+    T acc[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        T a = T(0);
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) a += __ldcg(partials + (int64_t)j * nb + b);
+        acc[j] = a;
+    }
+    block_sum<T, NV>(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) bc[j] = acc[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) out[j] = bc[j];
+    __syncthreads();
+}
+
+template <typename T>
+struct PcgArgs {
+    Sell A;
+    const T *vals;
+    const T *b;            // right-hand side (or NULL with b64)
+    const double *b64;     // FP64 right-hand side converted on the fly (refinement loop)
+    T *x;                  // x0 on entry unless zero_x0, solution on exit
+    const T *dinv;         // Jacobi 1/diag, NULL = none
+    T *r, *z, *p0, *p1, *q;
+    T *part;               // [2 phases][4][gridDim]
+    KrylovState *st;
+    GridBarrier *bar;
+    double tol, atol;
+    const double *tol_dev; // when set, the relative tolerance is read here
+    int maxiter, zero_x0;
+};
+
+// One large block per SM (fewer barrier arrivals and partials): 1024 threads in
+// FP32 (64 registers), 768 in FP64 (up to 85 registers), no spills.
+template <typename T>
+constexpr int pcg_block() { return sizeof(T) == 4 ? 1024 : 768; }
+
+template <typename T, int MW>
+__global__ void __launch_bounds__(pcg_block<T>(), 1) cg_persistent_kernel(PcgArgs<T> a) {
+    const int n = a.A.n_rows;
+    const int nb = gridDim.x;
+    const int chunk = (((n + nb - 1) / nb) + kSlice - 1) & ~(kSlice - 1);
+    const int r0 = blockIdx.x * chunk;
+    const int r1 = min(n, r0 + chunk);
+    // barrier generation at entry (the barrier words persist across solves; count is 0 between kernels)
+    unsigned int gen = threadIdx.x == 0 ? ld_acquire_u32(&a.bar->gen) : 0u;
+    T *P1 = a.part;                       // phase-1 partials [4][nb]
+    T *P2 = a.part + 4 * (int64_t)nb;     // phase-2 partials [4][nb]
+    const T *dinv = a.dinv;
+    // ---- init: r = b - A x0, z = M r, p0 = 0
+    {
+        T v[3] = {T(0), T(0), T(0)};
+        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+            const T bi = a.b64 ? (T)a.b64[i] : a.b[i];
+            T ri;
+            if (a.zero_x0) {
+                a.x[i] = T(0);
+                ri = bi;
+            } else {
+                const T *x = a.x;
+                ri = bi - sell_row_dot<T, MW>(a.A, a.vals, i, [&](int c) { return x[c]; });
+            }
+            const T zi = dinv ? dinv[i] * ri : ri;
+            a.r[i] = ri;
+            a.z[i] = zi;
+            a.p0[i] = T(0);
+            v[0] += ri * zi;
+            v[1] += ri * ri;
+            v[2] += bi * bi;
+        }
+        block_sum<T, 3>(v);
+        if (threadIdx.x == 0) {
+            P1[blockIdx.x] = v[0];
+            P1[nb + blockIdx.x] = v[1];
+            P1[2 * nb + blockIdx.x] = v[2];
+        }
+    }
+    bool ok = grid_barrier(a.bar, nb, gen);
+    T tot3[3];
+    block_reduce_partials<T, 3>(P1, nb, tot3);
+    double gamma = (double)tot3[0], rr = (double)tot3[1];
+    const double bs = (double)tot3[2];
+    const double tl = a.tol_dev ? *a.tol_dev : a.tol;
+    const double atol2 = fmax(tl * tl * bs, a.atol * a.atol);
+    double beta = 0.0, alpha = 0.0;
+    int k = 0, status = WSPM_OK;
+    double rs = dinv ? rr : gamma;
+    bool done = !(rs > atol2 && 0 < a.maxiter);
+    if (!isfinite(rs)) { done = true; status = WSPM_NAN; }
+    T *po = a.p0, *pn = a.p1;
+    while (!done && ok) {
+        // ---- phase 1
+        {
+            const T bt = (T)beta;
+            const T *z = a.z;
+            const T *pold = po;
+            T v[1] = {T(0)};
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const T qi = sell_row_dot<T, MW>(a.A, a.vals, i, [&](int c) {
+                    return fma(bt, __ldcg(pold + c), __ldcg(z + c));
+                });
+                const T pi = fma(bt, pold[i], z[i]);
+                pn[i] = pi;
+                a.q[i] = qi;
+                v[0] += pi * qi;
+            }
+            block_sum<T, 1>(v);
+            if (threadIdx.x == 0) P1[blockIdx.x] = v[0];
+        }
+        ok = grid_barrier(a.bar, nb, gen);
+        if (!ok) break;
+        T pq[1];
+        block_reduce_partials<T, 1>(P1, nb, pq);
+        alpha = (double)((T)gamma / pq[0]);
+        // ---- phase 2
+        {
+            const T al = (T)alpha;
+            T v[2] = {T(0), T(0)};
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                a.x[i] = fma(al, pn[i], a.x[i]);
+                const T ri = fma(-al, a.q[i], a.r[i]);
+                a.r[i] = ri;
+                const T zi = dinv ? dinv[i] * ri : ri;
+                a.z[i] = zi;
+                v[0] += ri * zi;
+                v[1] += ri * ri;
+            }
+            block_sum<T, 2>(v);
+            if (threadIdx.x == 0) {
+                P2[blockIdx.x] = v[0];
+                P2[nb + blockIdx.x] = v[1];
+            }
+        }
+        ok = grid_barrier(a.bar, nb, gen);
+        if (!ok) break;
+        T t2[2];
+        block_reduce_partials<T, 2>(P2, nb, t2);
+        const double gamma_new = (double)t2[0];
+        beta = (double)(t2[0] / (T)gamma);
+        gamma = gamma_new;
+        rr = (double)t2[1];
+        ++k;
+        rs = dinv ? rr : gamma;
+        if (!(rs > atol2)) done = true;
+        else if (k >= a.maxiter) { done = true; status = WSPM_MAXITER; }
+        if (!isfinite(rs) || !isfinite(alpha)) { done = true; status = WSPM_NAN; }
+        T *t = po; po = pn; pn = t;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        KrylovState *st = a.st;
+        st->gamma = gamma; st->rr = rr; st->bs = bs; st->atol2 = atol2;
+        st->alpha = alpha; st->beta = beta;
+        st->k = k;
+        st->status = ok ? status : WSPM_CUDA_ERROR;
+        st->done = 1;
+    }
+}
+
+// Grid size for the persistent kernel: every block must be resident at once.
+template <typename T, int MW>
+static int pcg_grid(int n) {
+    static int cached[2] = {0, 0};
+    int &c = cached[sizeof(T) == 8 ? 1 : 0];
+    if (c == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, cg_persistent_kernel<T, MW>, pcg_block<T>(), 0);
+        c = sms * (per > 0 ? per : 1);
+    }
+    const int need = (n + pcg_block<T>() - 1) / pcg_block<T>();
+    int g = need < c ? need : c;
+    if (g > kMaxPartials) g = kMaxPartials;
+    return g < 1 ? 1 : g;
+}
+
+template <typename T>
+int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
+                          const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
+                          const double *tol_dev, cudaStream_t st) {
+    PcgArgs<T> a;
+    a.A = A; a.vals = vals; a.b = b; a.b64 = b64; a.x = x; a.dinv = dinv;
+    a.r = w.r; a.z = w.z; a.p0 = w.p0; a.p1 = w.p1; a.q = w.q; a.part = w.partials; a.st = w.st;
+    a.bar = (GridBarrier *)&w.st->ticket[0];
+    a.tol = tol; a.atol = atol; a.tol_dev = tol_dev; a.maxiter = maxiter; a.zero_x0 = zero_x0 ? 1 : 0;
+    cudaError_t e = cudaSuccess;
+    WSPM_WIDTH_DISPATCH(A.max_width, {
+        const int grid = pcg_grid<T, MW>(A.n_rows);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(pcg_block<T>());
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, cg_persistent_kernel<T, MW>, a);
+    });
+    return e == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+}
+
+template int cg_persistent_enqueue<double>(const Sell &, const double *, const double *, const double *, double *,
+                                           const double *, const CgBuffers<double> &, double, double, int, bool,
+                                           const double *, cudaStream_t);
+template int cg_persistent_enqueue<float>(const Sell &, const float *, const float *, const double *, float *,
+                                          const float *, const CgBuffers<float> &, double, double, int, bool,
+                                          const double *, cudaStream_t);
+
 // ---------------------------------------------------------------- BiCGSTAB (FP64)
 template <int MW>
 __global__ void __launch_bounds__(kBlock) bicg_init_kernel(Sell A, const double *__restrict__ vals,

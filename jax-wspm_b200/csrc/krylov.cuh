@@ -59,6 +59,14 @@ template <typename T>
 void cg_enqueue_body(const Sell &A, const T *vals, T *x, const T *dinv, const CgBuffers<T> &w,
                      int maxiter, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
 
+// Whole CG solve in one cooperative launch (x0 in x unless zero_x0); the final
+// scalars, iteration count and status are written to w.st.  The barrier words
+// live in w.st->ticket and must be zero before the launch (state reset).
+template <typename T>
+int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
+                          const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
+                          const double *tol_dev, cudaStream_t st);
+
 struct BicgBuffers {
     double *r, *rhat, *p, *phat, *q, *t;
     double *partials;

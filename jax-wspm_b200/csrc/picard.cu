@@ -38,6 +38,7 @@ struct PicardState {
     int bodies;        // Krylov loop bodies executed (launch accounting)
     int solver;        // WSPM_SOLVER_*
     int cont;          // 1 while the Picard loop continues (read by the host-driven mode)
+    int restart_m;     // GMRES restart length (launch accounting)
     unsigned int ticket[4];
 };
 
@@ -46,7 +47,7 @@ __global__ void state_reset_kernel(unsigned int *words, int n_words) {
 }
 
 __global__ void step_init_kernel(SoilParams sp, int n, const double *__restrict__ h_n, double *theta_n, double *h_m,
-                                 PicardState *ps, double tol, int maxit, int relative, int solver,
+                                 PicardState *ps, double tol, int maxit, int relative, int solver, int restart_m,
                                  cudaGraphConditionalHandle cond, int use_cond) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double c, k, t;
@@ -62,6 +63,7 @@ __global__ void step_init_kernel(SoilParams sp, int n, const double *__restrict_
         ps->bodies = 0;
         ps->solver = solver;
         ps->cont = maxit > 0 ? 1 : 0;
+        ps->restart_m = restart_m;
         for (int j = 0; j < 4; ++j) ps->ticket[j] = 0u;
         if (use_cond) cudaGraphSetConditional(cond, maxit > 0 ? 1u : 0u);
     }
@@ -90,13 +92,16 @@ __global__ void __launch_bounds__(kBlock) picard_update_kernel(int n, const doub
             if (irs) {
                 ps->refine_total += irs->k;
                 ps->krylov_total += irs->steps;   // inner iterations accumulated by the refinement loop
-                ps->bodies += irs->pad0;          // inner CG bodies accumulated by the refinement loop
+                ps->bodies += irs->pad0;          // inner CG launches accumulated by the refinement loop
                 ps->last_krylov_status = irs->status;
             } else {
                 const int kk = ks->k > 0 ? ks->k : 0;
                 ps->krylov_total += kk;
-                // CG bodies hold two iterations; BiCGSTAB one; GMRES bodies are restart cycles
-                ps->bodies += ps->solver == WSPM_SOLVER_CG ? (kk + 1) / 2 : (ps->solver == WSPM_SOLVER_BICGSTAB ? (ks->k < 0 ? 1 : kk) : kk);
+                // Krylov-loop launches: CG is one persistent kernel; BiCGSTAB 4 kernels per
+                // iteration; GMRES 4 m + 4 kernels per restart cycle
+                if (ps->solver == WSPM_SOLVER_CG) ps->bodies += 1;
+                else if (ps->solver == WSPM_SOLVER_BICGSTAB) ps->bodies += 4 * (ks->k < 0 ? 1 : kk);
+                else ps->bodies += (4 * ps->restart_m + 4) * kk;
                 ps->last_krylov_status = ks->status;
             }
             if (ps->last_krylov_status == WSPM_MAXITER) ps->krylov_maxiter_hits += 1;
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const doubl
             } else {
                 irs->k += 1;
                 irs->steps += inner->k;
-                irs->pad0 += (inner->k + 1) / 2;
+                irs->pad0 += 1;
             }
             irs->rr = tot[0];
             // the next FP32 solve aims at the reduction the FP64 residual still needs
@@ -238,7 +243,7 @@ static int build_picard_graph(PicardPlan *P) {
         if (P->irs) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)P->irs, (int)(sizeof(KrylovState) / 4));
     }
     step_init_kernel<<<nb, kBlock, 0, cs>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
-                                            d.picard_maxiter, d.picard_relative, d.solver, hp, 1);
+                                            d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, hp, 1);
     if (e == cudaSuccess) e = capture_while(cs, hp, [&](cudaStream_t bs) {
         launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, bs);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
@@ -260,14 +265,9 @@ static int build_picard_graph(PicardPlan *P) {
                                                                               1, d.krylov_tol, d.inner_tol,
                                                                               d.refine_maxiter, hir, 1));
             capture_while(bs, hir, [&](cudaStream_t ibs) {
-                cudaGraphConditionalHandle hcg;
-                make_cond_handle(ibs, &hcg);
                 const float *dv32 = dinv ? P->dinv32 : nullptr;
-                cg_enqueue_init<float>(A, d.vals32, nullptr, P->r64, P->x32, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
-                                       d.inner_maxiter, true, hcg, 1, ibs, &P->irs->inner_tol);
-                capture_while(ibs, hcg, [&](cudaStream_t cbs) {
-                    cg_enqueue_body<float>(A, d.vals32, P->x32, dv32, P->cg32, d.inner_maxiter, hcg, 1, cbs);
-                });
+                cg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
+                                             d.inner_maxiter, true, &P->irs->inner_tol, ibs);
                 ir_correct_kernel<<<nb, kBlock, 0, ibs>>>(n, d.x, P->x32);
                 WSPM_WIDTH_DISPATCH(A.max_width,
                                     ir_residual_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, d.rhs, d.x, P->r64,
@@ -296,13 +296,9 @@ static int build_picard_graph(PicardPlan *P) {
             });
             ks = P->gm.st;
         } else {
-            cudaGraphConditionalHandle hk;
-            make_cond_handle(bs, &hk);
-            cg_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, dinv, P->cg64, d.krylov_tol, 0.0,
-                                    d.krylov_maxiter, false, hk, 1, bs);
-            capture_while(bs, hk, [&](cudaStream_t kbs) {
-                cg_enqueue_body<double>(A, d.vals, d.x, dinv, P->cg64, d.krylov_maxiter, hk, 1, kbs);
-            });
+            copy_kernel_d(d.h_m, d.x, n, bs);
+            cg_persistent_enqueue<double>(A, d.vals, d.rhs, nullptr, d.x, dinv, P->cg64, d.krylov_tol, 0.0,
+                                          d.krylov_maxiter, false, nullptr, bs);
             ks = P->cg64.st;
         }
         picard_update_kernel<<<nb, kBlock, 0, bs>>>(n, d.x, d.h_m, P->partials, P->ps, ks, irs, hp, 1);
@@ -346,7 +342,7 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
     for (KrylovState *k : sts)
         if (k) state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
     step_init_kernel<<<nb, kBlock, 0, st>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
-                                            d.picard_maxiter, d.picard_relative, d.solver, none, 0);
+                                            d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, none, 0);
     for (int it = 0; it < d.picard_maxiter && rc == WSPM_OK; ++it) {
         launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, st);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem, P->s,
@@ -367,13 +363,8 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
             const float *dv32 = dinv ? P->dinv32 : nullptr;
             for (int r = 0; r <= d.refine_maxiter && rc == WSPM_OK; ++r) {
                 if ((rc = read_flag(&P->irs->done, st, &flag, pinned)) != WSPM_OK || flag) break;
-                cg_enqueue_init<float>(A, d.vals32, nullptr, P->r64, P->x32, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
-                                       d.inner_maxiter, true, none, 0, st, &P->irs->inner_tol);
-                for (int b = 0; b < (d.inner_maxiter + 1) / 2 + 1; b += kChunk) {
-                    if ((rc = read_flag(&P->cg32.st->done, st, &flag, pinned)) != WSPM_OK || flag) break;
-                    for (int c = 0; c < kChunk; ++c)
-                        cg_enqueue_body<float>(A, d.vals32, P->x32, dv32, P->cg32, d.inner_maxiter, none, 0, st);
-                }
+                cg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
+                                             d.inner_maxiter, true, &P->irs->inner_tol, st);
                 ir_correct_kernel<<<nb, kBlock, 0, st>>>(n, d.x, P->x32);
                 WSPM_WIDTH_DISPATCH(A.max_width,
                                     ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.x, P->r64,
@@ -395,10 +386,11 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                                    none, 0, st);
                 kst = P->gm.st;
             } else {
-                cg_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, dinv, P->cg64, d.krylov_tol, 0.0,
-                                        d.krylov_maxiter, false, none, 0, st);
+                copy_kernel_d(d.h_m, d.x, n, st);
+                cg_persistent_enqueue<double>(A, d.vals, d.rhs, nullptr, d.x, dinv, P->cg64, d.krylov_tol, 0.0,
+                                              d.krylov_maxiter, false, nullptr, st);
                 kst = P->cg64.st;
-                max_bodies = (d.krylov_maxiter + 1) / 2;
+                max_bodies = -1;     // the persistent kernel ran the whole solve
             }
             for (int b = 0; b < max_bodies + 1 && rc == WSPM_OK; b += kChunk) {
                 if ((rc = read_flag(&kst->done, st, &flag, pinned)) != WSPM_OK || flag) break;
@@ -408,7 +400,7 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                     else if (d.solver == WSPM_SOLVER_GMRES)
                         gmres_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->gm, d.krylov_maxiter, none, 0, st);
                     else
-                        cg_enqueue_body<double>(A, d.vals, d.x, dinv, P->cg64, d.krylov_maxiter, none, 0, st);
+                        break;
                 }
             }
             ks = kst;

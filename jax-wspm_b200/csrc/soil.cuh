@@ -19,13 +19,19 @@ __device__ __forceinline__ void soil_eval(const SoilParams &sp, double h,
     if (sp.model == WSPM_SOIL_VAN_GENUCHTEN) {
         const double alpha = sp.p[0], thS = sp.p[1], thR = sp.p[2], n = sp.p[3], m = sp.p[4], Ks = sp.p[5];
         if (h < 0.0) {
+            // (a|h|)^(n-1) by pow (exact enough down to |h| ~ 1e-300, where exp(x log a|h|) loses ~|x| ulps),
+            // (a|h|)^n by one multiply, (1 + (a|h|)^n)^-m through log1p/exp and (1 + (a|h|)^n)^(-m-1) by one
+            // division (the reference evaluates six pow() calls)
             const double ah = alpha * fabs(h);
-            const double ahn = pow(ah, n);
-            theta = (thS - thR) * pow(1.0 + ahn, -m) + thR;
+            const double ahn1 = pow(ah, n - 1.0);
+            const double ahn = ahn1 * ah;
+            const double onep = 1.0 + ahn;
+            const double tm = exp(-m * log1p(ahn));
+            theta = (thS - thR) * tm + thR;
             const double Se = (theta - thR) / (thS - thR);
             const double t = 1.0 - pow(1.0 - pow(Se, 1.0 / m), m);
             K = Ks * (sqrt(Se) * (t * t));
-            C = (thS - thR) * alpha * m * n * pow(ah, n - 1.0) * pow(1.0 + ahn, -m - 1.0);
+            C = (thS - thR) * alpha * m * n * ahn1 * (tm / onep);
         } else {
             theta = thS;
             K = Ks;

@@ -16,7 +16,7 @@ import torch
 
 from . import _lib
 from ._lib import check, lib
-from .device import DeviceMesh, soil
+from .device import BoundaryEdges, DeviceMesh, soil
 
 TRI3_POINTS = np.array([[0.166666666666667, 0.166666666666667],
                         [0.166666666666667, 0.666666666666667],
@@ -45,7 +45,7 @@ class PicardEngine:
     def __init__(self, dmesh, soil_model="vg", phi=(), Ks_elem=None, bc_val=None, solver="cg", precond="jacobi",
                  krylov_tol=1e-10, krylov_maxiter=100, restart=30, mixed=False, inner_tol=1e-4,
                  inner_maxiter=2000, refine_maxiter=20, picard_tol=1e-6, picard_maxiter=100, picard_relative=True,
-                 quad=None):
+                 quad=None, neumann_nodes=None, neumann_flux=0.0, drainage_nodes=None):
         if not isinstance(dmesh, DeviceMesh):
             raise TypeError("dmesh must be a DeviceMesh")
         self.dm = dm = dmesh
@@ -98,6 +98,13 @@ class PicardEngine:
             setattr(d, name, getattr(self, name).data_ptr())
         d.vals32 = self.vals32.data_ptr() if self.vals32 is not None else None
         d.work_doubles = self.work.numel()
+        # boundary-edge rhs terms (Neumann flux, free drainage of water), applied after assembly
+        self.neumann = BoundaryEdges(dm, neumann_nodes) if neumann_nodes is not None else None
+        self.drainage = BoundaryEdges(dm, drainage_nodes) if drainage_nodes is not None else None
+        d.neumann = ctypes.pointer(self.neumann.c) if self.neumann is not None else None
+        d.neumann_flux = float(neumann_flux)
+        d.drainage = ctypes.pointer(self.drainage.c) if self.drainage is not None else None
+        self._edge_kernels = sum(1 for e in (self.neumann, self.drainage) if e is not None and e.n_bnodes > 0)
         self.desc = d
         self.plan = ctypes.c_void_p()
         torch.cuda.synchronize(dev)
@@ -130,23 +137,31 @@ class PicardEngine:
         fn = lib.wspm_picard_step_host if self.host_loop else lib.wspm_picard_step
         check("picard_step", fn(self.plan, ctypes.c_void_p(st.cuda_stream)))
 
-    def kernel_launches(self, its, refinements, bodies):
-        """Kernels the step graph launched (from the device counters; graph structure in picard.cu)."""
+    def kernel_launches(self, its, refinements, krylov_launches):
+        """Kernels the step graph launched (device counters; graph structure in picard.cu).
+
+        Per step: state resets, step_init, step_finish.  Per Picard iteration: soil, assembly,
+        edge-term kernels, the x0 copy, the Krylov init kernels, picard_update.  The Krylov
+        loop itself is counted on the device (one persistent kernel per CG solve, 4 kernels per
+        BiCGSTAB iteration, 4m+4 per GMRES cycle); each refinement adds correction + residual.
+        """
         cfg = self.config
+        e = self._edge_kernels
         if cfg["mixed"]:
-            return 5 + 5 * its + 3 * refinements + 4 * bodies
+            return 5 + (5 + e) * its + 2 * refinements + krylov_launches
         if cfg["solver"] == "gmres":
-            m = min(int(cfg["restart"]), self.dm.n_nodes)
-            return 4 + 6 * its + (4 * m + 4) * bodies
-        return 4 + 5 * its + 4 * bodies
+            return 4 + (6 + e) * its + krylov_launches
+        if cfg["solver"] == "bicgstab":
+            return 4 + (5 + e) * its + krylov_launches
+        return 4 + (4 + e) * its + krylov_launches
 
     def read_result(self):
         r = self.result.cpu().numpy()
         f = self.result_f64.cpu().numpy()
         out = {"status": int(r[0]), "iterations": int(r[1]), "krylov_iterations": int(r[2]),
                "refinements": int(r[3]), "krylov_cap_hits": int(r[4]), "krylov_status": int(r[5]),
-               "krylov_bodies": int(r[6]), "error": float(f[0])}
-        out["launches"] = self.kernel_launches(out["iterations"], out["refinements"], out["krylov_bodies"])
+               "krylov_launches": int(r[6]), "error": float(f[0])}
+        out["launches"] = self.kernel_launches(out["iterations"], out["refinements"], out["krylov_launches"])
         return out
 
     def step(self, dt):
