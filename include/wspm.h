@@ -199,13 +199,17 @@ int wspm_krylov_solve(const wspm_pattern *pat, const double *vals,
                       int32_t restart, double *work, int64_t work_doubles,
                       int32_t *result, void *stream);
 
-/* Measurement hook (no reference counterpart): runs exactly `iters` Jacobi-CG
- * iterations (fused kernels K1+K2, no convergence test) from x on the given
- * system as plain launches on `stream`, so the per-iteration time of the
- * dominant kernels can be taken with CUDA events.  fp32 != 0 selects the FP32
- * kernels (vals, b, x, dinv are then float arrays).  `work` as for CG.       */
+/* Measurement hook (no reference counterpart): runs up to `iters` Jacobi-CG
+ * iterations of the persistent CG kernel with tolerance 0 from x on the given
+ * system, as plain launches on `stream`, so the per-iteration time of the
+ * dominant kernel can be taken with CUDA events.  The kernel still stops early
+ * on an exactly zero residual or a non-finite value; `iters_done` (device
+ * int32, may be NULL) receives the iterations actually run, so a timing can be
+ * rejected when it is short.  fp32 != 0 selects the FP32 kernel (vals, b, x,
+ * dinv are then float arrays).  `work` as for CG.                            */
 int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const void *vals, const void *b, void *x,
-                       const void *dinv, int32_t iters, double *work, int64_t work_doubles, void *stream);
+                       const void *dinv, int32_t iters, double *work, int64_t work_doubles,
+                       int32_t *iters_done, void *stream);
 
 /* Allocation-free Jacobi-CG solve.  No counterpart in the reference: it is
  * for callers that cannot allocate device memory -- typically code running

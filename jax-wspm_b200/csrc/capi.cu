@@ -299,25 +299,34 @@ extern "C" int wspm_krylov_solve(const wspm_pattern *pat, const double *vals, co
     return WSPM_OK;
 }
 
+__global__ void copy_k_kernel(const KrylovState *st, int32_t *out) { *out = st->k; }
+
 extern "C" int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const void *vals, const void *b, void *x,
                                   const void *dinv, int32_t iters, double *work, int64_t work_doubles,
-                                  void *stream) {
+                                  int32_t *iters_done, void *stream) {
     if (!pattern_ok(pat) || !vals || !b || !x || !work || iters < 0) return WSPM_BAD_ARG;
     if (work_doubles < cg_workspace_doubles(pat->n_rows, fp32 ? 4 : 8)) return WSPM_BAD_ARG;
     const Sell A = make_sell(pat);
     cudaStream_t st = (cudaStream_t)stream;
     int64_t used = 0;
-    // tolerance 0: the solve runs exactly `iters` iterations (the persistent CG kernel of the solver path)
+    int rc;
+    KrylovState *state;
+    // tolerance 0: the solve runs `iters` iterations unless the residual is exactly 0 or non-finite
     if (fp32) {
         CgBuffers<float> w = carve_cg<float>(work, pat->n_rows, &used);
+        state = w.st;
         state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
-        return cg_persistent_enqueue<float>(A, (const float *)vals, (const float *)b, nullptr, (float *)x,
-                                            (const float *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
+        rc = cg_persistent_enqueue<float>(A, (const float *)vals, (const float *)b, nullptr, (float *)x,
+                                          (const float *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
+    } else {
+        CgBuffers<double> w = carve_cg<double>(work, pat->n_rows, &used);
+        state = w.st;
+        state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
+        rc = cg_persistent_enqueue<double>(A, (const double *)vals, (const double *)b, nullptr, (double *)x,
+                                           (const double *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
     }
-    CgBuffers<double> w = carve_cg<double>(work, pat->n_rows, &used);
-    state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
-    return cg_persistent_enqueue<double>(A, (const double *)vals, (const double *)b, nullptr, (double *)x,
-                                         (const double *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
+    if (rc == WSPM_OK && iters_done) copy_k_kernel<<<1, 1, 0, st>>>(state, iters_done);
+    return rc;
 }
 
 extern "C" const char *wspm_version(void) { return "wspm-b200 0.1 (sm_100a)"; }

@@ -215,22 +215,16 @@ template void cg_enqueue_body<float>(const Sell &, const float *, float *, const
                                      int, cudaGraphConditionalHandle, int, cudaStream_t);
 
 // ---------------------------------------------------------------- persistent CG
-// One cooperative launch runs the whole (preconditioned) CG solve.  Block b owns
-// a contiguous range of rows; each iteration is two phases separated by grid
-// barriers:
-//   phase 1: p_new = z + beta p_old ; q = A p_new (gathers z, p_old) ; partial p.q
-//   phase 2: x += alpha p ; r -= alpha q ; z = M r ; partials r.z, r.r
-// After a barrier every block sums all blocks' partials in the same fixed order,
-// so every block holds bitwise identical alpha/beta and takes the same
-// convergence decision (no broadcast, no atomics on the scalars).  Vectors that
-// other blocks write during the kernel are gathered with ld.global.cg (L2) so
-// that no stale L1 line is ever read.  Barrier waits are bounded: on timeout the
-// block records an error and every block leaves the loop at its next check.
+// Grid barrier of the cooperative CG kernel.  The words live in the solver's
+// KrylovState (count returns to 0 at every barrier; gen only grows).  Waits are
+// bounded: on timeout the block records an error and every block leaves its
+// loop at the next check, so a failed launch ends with WSPM_CUDA_ERROR instead
+// of hanging.
 struct GridBarrier {
     unsigned int count;
     unsigned int gen;
     int error;
-    int pad;
+    unsigned int mono;     // arrivals at counting barriers since the kernel's first grid barrier
 };
 
 constexpr long long kBarrierSpinLimit = 20000000LL;   // ~ seconds; a legitimate wait is microseconds
@@ -271,38 +265,23 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier *gb, unsigned int nbloc
     return ok != 0;
 }
 
-// Fixed-order sum of nb partials (layout [NV][nb]) by the whole block; result broadcast to all threads.
-template <typename T, int NV>
-__device__ __forceinline__ void block_reduce_partials(const T *partials, int nb, T (&out)[NV]) {
-    __shared__ T bc[NV];
-    T acc[NV];
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-        T a = T(0);
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) a += __ldcg(partials + (int64_t)j * nb + b);
-        acc[j] = a;
-    }
-    block_sum<T, NV>(acc);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int j = 0; j < NV; ++j) bc[j] = acc[j];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < NV; ++j) out[j] = bc[j];
-    __syncthreads();
-}
+// Per-block vectors of the resident CG kernel, in the order in which they are
+// given shared memory (the rest live in the global workspace).
+enum RcgVec { kVR = 0, kVP, kVS, kVW, kVX, kVD, kNumRcgVec };
 
 template <typename T>
-struct PcgArgs {
+struct RcgArgs {
     Sell A;
     const T *vals;
     const T *b;            // right-hand side (or NULL with b64)
     const double *b64;     // FP64 right-hand side converted on the fly (refinement loop)
     T *x;                  // x0 on entry unless zero_x0, solution on exit
     const T *dinv;         // Jacobi 1/diag, NULL = none
-    T *r, *z, *p0, *p1, *q;
-    T *part;               // [2 phases][4][gridDim]
+    T *z;                  // preconditioned residual, the only vector other blocks read
+    T *gvec[kNumRcgVec];   // global homes of the vectors kept out of shared memory (row-indexed)
+    int chunk;             // rows per block (multiple of 32)
+    T *part;               // [2 parities][4][gridDim] partial sums, then [3][gridDim] for the init
+    unsigned int *zflag;   // [gridDim] per-block z epoch
     KrylovState *st;
     GridBarrier *bar;
     double tol, atol;
@@ -310,122 +289,361 @@ struct PcgArgs {
     int maxiter, zero_x0;
 };
 
-// One large block per SM (fewer barrier arrivals and partials): 1024 threads in
-// FP32 (64 registers), 768 in FP64 (up to 85 registers), no spills.
-template <typename T>
-constexpr int pcg_block() { return sizeof(T) == 4 ? 1024 : 768; }
+constexpr int kRcgBlock = 512;    // 128 registers: the 2D instances run without spills
 
+__device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Counting barrier: every block adds one arrival; a block passes once the count
+// reaches `target` (= gridDim * barriers passed so far).  One atomic per block
+// and one polled word; bounded like grid_barrier.
+__device__ __forceinline__ bool count_barrier(GridBarrier *gb, unsigned int target) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&gb->mono, 1u);
+        int ok = 1;
+        long long spins = 0;
+        while (ld_acquire_u32(&gb->mono) < target) {
+            if (++spins > kBarrierSpinLimit) { atomicExch(&gb->error, 1); ok = 0; break; }
+            if ((spins & 1023) == 0 && *(volatile int *)&gb->error) { ok = 0; break; }
+            __nanosleep(20);
+        }
+        ok_s = ok && (*(volatile int *)&gb->error) == 0;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// Wait until blocks [lo, hi] (except this one) have published z epoch `epoch`;
+// thread t polls block lo + t (strided), the verdict is OR-reduced by the block.
+__device__ __forceinline__ bool wait_zflags(const unsigned int *zflag, int lo, int hi, unsigned int epoch,
+                                            GridBarrier *gb) {
+    int fail = 0;
+    for (int c = lo + (int)threadIdx.x; c <= hi && !fail; c += blockDim.x) {
+        if (c == (int)blockIdx.x) continue;
+        long long spins = 0;
+        while (ld_acquire_u32(zflag + c) < epoch) {
+            if (++spins > kBarrierSpinLimit) { atomicExch(&gb->error, 1); fail = 1; break; }
+            if ((spins & 1023) == 0 && *(volatile int *)&gb->error) { fail = 1; break; }
+            __nanosleep(20);
+        }
+    }
+    return __syncthreads_or(fail) == 0;
+}
+
+// Fixed-order sum of nb partials (layout [NV][nb]): warp j sums row j with all
+// of a lane's loads in flight at once (one L2 round trip for nb <= 256),
+// broadcast through shared memory with a single block barrier.  Every block
+// runs the identical sequence, so all blocks hold bitwise identical sums.
+template <typename T, int NV>
+__device__ __forceinline__ void reduce_partials_rows(const T *partials, int nb, T (&out)[NV]) {
+    __shared__ T bc[NV];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (wid < NV) {
+        const T *pj = partials + (int64_t)wid * nb;
+        T acc = T(0);
+        for (int b0 = 0; b0 < nb; b0 += 256) {
+            T x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int b = b0 + lane + 32 * u;
+                x[u] = b < nb ? __ldcg(pj + b) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc += x[u];
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) bc[wid] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) out[j] = bc[j];
+}
+
+// Row i of a DIA matrix times z with the values and gathers of a group of
+// diagonals in flight at once (8 in FP32, 4 in FP64), offsets from shared
+// memory; the products are accumulated in diagonal order like sell_row_dot.
+// z is read with plain (L1-cacheable) loads: inside a phase no block writes z,
+// and the acquire that ends the preceding wait (flag or barrier) followed by
+// the block barrier orders every earlier z store before these loads.
 template <typename T, int MW>
-__global__ void __launch_bounds__(pcg_block<T>(), 1) cg_persistent_kernel(PcgArgs<T> a) {
+__device__ __forceinline__ T dia_row_z(const T *__restrict__ vals, int64_t ld, int i, int last, int nd,
+                                       const int *s_off, const T *z) {
+    constexpr int G0 = sizeof(T) == 4 ? 8 : 4;
+    constexpr int G = MW < G0 ? MW : G0;
+    T acc = T(0);
+#pragma unroll
+    for (int k0 = 0; k0 < MW; k0 += G) {
+        if (k0 >= nd) break;
+        T v[G], g[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            const int k = k0 + q;
+            if (k < nd) {
+                v[q] = __ldg(vals + (int64_t)k * ld + i);
+                int c = i + s_off[k];
+                c = c < 0 ? 0 : (c > last ? last : c);
+                g[q] = z[c];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < G; ++q)
+            if (k0 + q < nd) acc = fma(v[q], g[q], acc);
+    }
+    return acc;
+}
+
+// SpMV of z over local rows [l0, l1) of the block starting at row r0: w into
+// wbase[l], partial (w, z) into acc.
+template <typename T, int MW>
+__device__ __forceinline__ void rcg_spmv_rows(int l0, int l1, T &acc, const Sell &A, const T *__restrict__ vals,
+                                              int64_t ld, int r0, int last, int nd, const int *s_off, const T *z,
+                                              bool dia, T *wbase) {
+    for (int l = l0 + threadIdx.x; l < l1; l += blockDim.x) {
+        const int i = r0 + l;
+        T wi;
+        if (dia) wi = dia_row_z<T, (MW > 0 ? MW : 1)>(vals, ld, i, last, nd, s_off, z);
+        else wi = sell_row_dot<T, MW>(A, vals, i, [z](int c) { return z[c]; });
+        wbase[l] = wi;
+        acc = fma(wi, z[i], acc);
+    }
+}
+
+// Whole preconditioned CG solve in one cooperative launch, single-reduction
+// form (Chronopoulos & Gear, J. Comput. Appl. Math. 25 (1989) 153-168):
+//   beta = g/g_old ; alpha = g/(d - beta g/alpha_old)
+//   p = z + beta p ; s = w + beta s ; x += alpha p ; r -= alpha s ; z = M r
+//   w = A z ; g = (r,z), d = (w,z), rho = (r,r)       (one grid reduction)
+// Block b owns rows [b*chunk, (b+1)*chunk).  The first NS of its vectors
+// r, p, s, w, x, M (NS = 6, 4 or 0, whatever fits in shared memory) stay on
+// chip for the whole solve, the others live in the workspace (x: the caller's
+// array).  z is the only vector that crosses blocks.  Per iteration the kernel
+// streams the matrix once and moves z once through L2, instead of the 11
+// vector passes of the textbook iteration.
+//
+// Synchronisation per iteration: after its z update a block publishes a z
+// epoch flag; its SpMV first does the interior rows (DIA: rows whose columns
+// all lie in its own chunk), then waits only for the flags of the blocks its
+// halo rows read, then does the halo rows.  The partial sums go through one
+// counting barrier and are summed by every block in the same fixed order, so
+// all blocks hold bitwise identical scalars and take the same branch.  Partials
+// alternate between two buffers: a block can only start writing reduction e+2
+// after every block has arrived at reduction e+1, i.e. finished reading e.  z is
+// overwritten only after the reduction that follows every block's SpMV.  The
+// stopping rule is the textbook one on ||r_{k+1}||: the iteration count matches
+// the two-reduction form up to rounding.  Every wait is bounded (error flag).
+template <typename T, int MW, int NS>
+__global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char rcg_smem[];
+    __shared__ int s_off[MW > 0 ? MW : 1];
+    T *const sm = reinterpret_cast<T *>(rcg_smem);
     const int n = a.A.n_rows;
     const int nb = gridDim.x;
-    const int chunk = (((n + nb - 1) / nb) + kSlice - 1) & ~(kSlice - 1);
+    const int chunk = a.chunk;
     const int r0 = blockIdx.x * chunk;
     const int r1 = min(n, r0 + chunk);
-    // barrier generation at entry (the barrier words persist across solves; count is 0 between kernels)
+    const int nl = max(0, r1 - r0);
     unsigned int gen = threadIdx.x == 0 ? ld_acquire_u32(&a.bar->gen) : 0u;
-    T *P1 = a.part;                       // phase-1 partials [4][nb]
-    T *P2 = a.part + 4 * (int64_t)nb;     // phase-2 partials [4][nb]
-    const T *dinv = a.dinv;
-    // ---- init: r = b - A x0, z = M r, p0 = 0
+    if (threadIdx.x == 0) {
+        a.zflag[blockIdx.x] = 0u;
+        if (blockIdx.x == 0) a.bar->mono = 0u;
+    }
+    // every argument is copied to a local first: a lambda that captured the
+    // parameter struct itself would force a copy of it into local memory
+    const Sell A = a.A;
+    T *const z = a.z;
+    T *const xg = a.x;
+    const T *const vals = a.vals;
+    const T *const dg = a.dinv;
+    T *const gvR = a.gvec[kVR] + r0, *const gvP = a.gvec[kVP] + r0;
+    T *const gvS = a.gvec[kVS] + r0, *const gvW = a.gvec[kVW] + r0;
+    T *const part = a.part;
+    unsigned int *const zflag = a.zflag;
+    GridBarrier *const bar = a.bar;
+    // vector v at local row l: shared memory for v < NS, else its global home
+#define RCG_G(v) ((v) == kVR ? gvR : (v) == kVP ? gvP : (v) == kVS ? gvS : gvW)
+#define RCG(v, l) (*((v) < NS ? (sm + (v) * chunk + (l)) : (RCG_G(v) + (l))))
+    const int nd = A.n_diags;
+    const bool dia = MW > 0 && nd > 0 && nd <= MW;
+    int lo_i = 0, hi_i = 0, nbr_lo = 0, nbr_hi = nb - 1;
+    if (dia) {
+        int mn = 0, mx = 0;
+        for (int k = 0; k < nd; ++k) {
+            const int o = __ldg(A.diag_off + k);
+            if (threadIdx.x == 0) s_off[k] = o;
+            mn = min(mn, o);
+            mx = max(mx, o);
+        }
+        lo_i = min(nl, -mn);
+        hi_i = max(lo_i, nl - mx);
+        const int rlo = max(0, r0 + mn), rhi = min(n - 1, r1 - 1 + mx);
+        nbr_lo = min(nb - 1, rlo / chunk);
+        nbr_hi = min(nb - 1, rhi / chunk);
+        if (nl == 0) { nbr_lo = 1; nbr_hi = 0; }
+    }
+    const int last = n - 1;
+    const int64_t ld = A.ld;
+    // ---- init: x, M into place; r = b - A x0 ; z = M r
     {
         T v[3] = {T(0), T(0), T(0)};
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+            const int i = r0 + l;
             const T bi = a.b64 ? (T)a.b64[i] : a.b[i];
             T ri;
             if (a.zero_x0) {
-                a.x[i] = T(0);
+                xg[i] = T(0);
+                if (kVX < NS) RCG(kVX, l) = T(0);
                 ri = bi;
             } else {
-                const T *x = a.x;
-                ri = bi - sell_row_dot<T, MW>(a.A, a.vals, i, [&](int c) { return x[c]; });
+                if (kVX < NS) RCG(kVX, l) = xg[i];
+                ri = bi - sell_row_dot<T, MW>(A, vals, i, [xg](int c) { return xg[c]; });
             }
-            const T zi = dinv ? dinv[i] * ri : ri;
-            a.r[i] = ri;
-            a.z[i] = zi;
-            a.p0[i] = T(0);
+            const T di = dg ? dg[i] : T(1);
+            if (kVD < NS) RCG(kVD, l) = di;
+            const T zi = di * ri;
+            RCG(kVR, l) = ri;
+            RCG(kVP, l) = T(0);
+            RCG(kVS, l) = T(0);
+            z[i] = zi;
             v[0] += ri * zi;
             v[1] += ri * ri;
             v[2] += bi * bi;
         }
         block_sum<T, 3>(v);
         if (threadIdx.x == 0) {
-            P1[blockIdx.x] = v[0];
-            P1[nb + blockIdx.x] = v[1];
-            P1[2 * nb + blockIdx.x] = v[2];
+            T *p0 = part + 8 * (int64_t)nb;   // third region: the two parities are reused below
+            p0[blockIdx.x] = v[0];
+            p0[nb + blockIdx.x] = v[1];
+            p0[2 * nb + blockIdx.x] = v[2];
         }
     }
-    bool ok = grid_barrier(a.bar, nb, gen);
-    T tot3[3];
-    block_reduce_partials<T, 3>(P1, nb, tot3);
-    double gamma = (double)tot3[0], rr = (double)tot3[1];
-    const double bs = (double)tot3[2];
+    bool ok = grid_barrier(bar, nb, gen);     // z0 complete everywhere; zflags and mono reset
+    T init3[3];
+    reduce_partials_rows<T, 3>(part + 8 * (int64_t)nb, nb, init3);
+    const double bs = (double)init3[2];
     const double tl = a.tol_dev ? *a.tol_dev : a.tol;
     const double atol2 = fmax(tl * tl * bs, a.atol * a.atol);
-    double beta = 0.0, alpha = 0.0;
+    double gamma = (double)init3[0], rr = (double)init3[1];
+    double beta = 0.0, alpha = 0.0, gamma_old = 1.0, delta = 0.0;
     int k = 0, status = WSPM_OK;
-    double rs = dinv ? rr : gamma;
+    double rs = dg ? rr : gamma;
     bool done = !(rs > atol2 && 0 < a.maxiter);
     if (!isfinite(rs)) { done = true; status = WSPM_NAN; }
-    T *po = a.p0, *pn = a.p1;
+    unsigned int red = 0;      // counting barriers passed
+    T *const wbase = kVW < NS ? sm + kVW * chunk : gvW;
+#define RCG_SPMV(l0, l1, acc) \
+    rcg_spmv_rows<T, MW>((l0), (l1), (acc), A, vals, ld, r0, last, nd, s_off, z, dia, wbase)
+    // w0 = A z0 and d0 = (w0, z0) when iterating
+    if (!done && ok) {
+        T v[1] = {T(0)};
+        RCG_SPMV(0, nl, v[0]);
+        block_sum<T, 1>(v);
+        T *pp = part + (int64_t)(red & 1) * 4 * nb;
+        if (threadIdx.x == 0) pp[blockIdx.x] = v[0];
+        ++red;
+        ok = count_barrier(bar, red * (unsigned)nb);
+        T d1[1];
+        reduce_partials_rows<T, 1>(pp, nb, d1);
+        delta = (double)d1[0];
+    }
     while (!done && ok) {
-        // ---- phase 1
+        if (k == 0) {
+            beta = 0.0;
+            alpha = (double)((T)gamma / (T)delta);
+        } else {
+            beta = (double)((T)gamma / (T)gamma_old);
+            alpha = (double)((T)gamma / ((T)delta - (T)beta * (T)gamma / (T)alpha));
+        }
+        if (!isfinite(alpha)) { status = WSPM_NAN; break; }
+        T *pp = part + (int64_t)(red & 1) * 4 * nb;
+        // ---- update phase (own rows only); rows in batches of RB with every load issued first
         {
-            const T bt = (T)beta;
-            const T *z = a.z;
-            const T *pold = po;
+            constexpr int RB = sizeof(T) == 4 ? 4 : 2;
+            const T al = (T)alpha, bt = (T)beta;
+            T v[2] = {T(0), T(0)};
+            const int TB = blockDim.x;
+            for (int l0 = threadIdx.x; l0 < nl; l0 += RB * TB) {
+                T zz[RB], pv[RB], sv[RB], wv[RB], xv[RB], rv[RB], dv[RB];
+#pragma unroll
+                for (int q = 0; q < RB; ++q) {
+                    const int l = l0 + q * TB;
+                    if (l < nl) {
+                        zz[q] = z[r0 + l];
+                        pv[q] = RCG(kVP, l); sv[q] = RCG(kVS, l); wv[q] = RCG(kVW, l);
+                        rv[q] = RCG(kVR, l);
+                        xv[q] = kVX < NS ? RCG(kVX, l) : xg[r0 + l];
+                        dv[q] = kVD < NS ? RCG(kVD, l) : (dg ? dg[r0 + l] : T(1));
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < RB; ++q) {
+                    const int l = l0 + q * TB;
+                    if (l < nl) {
+                        const T pi = fma(bt, pv[q], zz[q]);
+                        const T si = fma(bt, sv[q], wv[q]);
+                        RCG(kVP, l) = pi;
+                        RCG(kVS, l) = si;
+                        const T xi = fma(al, pi, xv[q]);
+                        if (kVX < NS) RCG(kVX, l) = xi;
+                        else xg[r0 + l] = xi;
+                        const T ri = fma(-al, si, rv[q]);
+                        RCG(kVR, l) = ri;
+                        const T zi = dv[q] * ri;
+                        z[r0 + l] = zi;
+                        v[0] += ri * zi;
+                        v[1] += ri * ri;
+                    }
+                }
+            }
+            block_sum<T, 2>(v);        // ends with a block barrier: every z store of this block is done
+            if (threadIdx.x == 0) {
+                pp[nb + blockIdx.x] = v[0];
+                pp[2 * nb + blockIdx.x] = v[1];
+                __threadfence();
+                st_release_u32(zflag + blockIdx.x, (unsigned)(k + 1));
+            }
+        }
+        // ---- SpMV phase: interior rows, then halo rows once the neighbours' z is published
+        {
             T v[1] = {T(0)};
-            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                const T qi = sell_row_dot<T, MW>(a.A, a.vals, i, [&](int c) {
-                    return fma(bt, __ldcg(pold + c), __ldcg(z + c));
-                });
-                const T pi = fma(bt, pold[i], z[i]);
-                pn[i] = pi;
-                a.q[i] = qi;
-                v[0] += pi * qi;
+            if (dia) {
+                RCG_SPMV(lo_i, hi_i, v[0]);
+                ok = wait_zflags(zflag, nbr_lo, nbr_hi, (unsigned)(k + 1), bar);
+                if (!ok) break;
+                RCG_SPMV(0, lo_i, v[0]);
+                RCG_SPMV(hi_i, nl, v[0]);
+            } else {
+                ok = wait_zflags(zflag, 0, nb - 1, (unsigned)(k + 1), bar);
+                if (!ok) break;
+                RCG_SPMV(0, nl, v[0]);
             }
             block_sum<T, 1>(v);
-            if (threadIdx.x == 0) P1[blockIdx.x] = v[0];
+            if (threadIdx.x == 0) pp[blockIdx.x] = v[0];
         }
-        ok = grid_barrier(a.bar, nb, gen);
+        ++red;
+        ok = count_barrier(bar, red * (unsigned)nb);
         if (!ok) break;
-        T pq[1];
-        block_reduce_partials<T, 1>(P1, nb, pq);
-        alpha = (double)((T)gamma / pq[0]);
-        // ---- phase 2
-        {
-            const T al = (T)alpha;
-            T v[2] = {T(0), T(0)};
-            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                a.x[i] = fma(al, pn[i], a.x[i]);
-                const T ri = fma(-al, a.q[i], a.r[i]);
-                a.r[i] = ri;
-                const T zi = dinv ? dinv[i] * ri : ri;
-                a.z[i] = zi;
-                v[0] += ri * zi;
-                v[1] += ri * ri;
-            }
-            block_sum<T, 2>(v);
-            if (threadIdx.x == 0) {
-                P2[blockIdx.x] = v[0];
-                P2[nb + blockIdx.x] = v[1];
-            }
-        }
-        ok = grid_barrier(a.bar, nb, gen);
-        if (!ok) break;
-        T t2[2];
-        block_reduce_partials<T, 2>(P2, nb, t2);
-        const double gamma_new = (double)t2[0];
-        beta = (double)(t2[0] / (T)gamma);
-        gamma = gamma_new;
-        rr = (double)t2[1];
+        T t3[3];
+        reduce_partials_rows<T, 3>(pp, nb, t3);
+        gamma_old = gamma;
+        delta = (double)t3[0];
+        gamma = (double)t3[1];
+        rr = (double)t3[2];
         ++k;
-        rs = dinv ? rr : gamma;
+        rs = dg ? rr : gamma;
         if (!(rs > atol2)) done = true;
         else if (k >= a.maxiter) { done = true; status = WSPM_MAXITER; }
-        if (!isfinite(rs) || !isfinite(alpha)) { done = true; status = WSPM_NAN; }
-        T *t = po; po = pn; pn = t;
+        if (!isfinite(rs)) { done = true; status = WSPM_NAN; }
     }
+    if (kVX < NS) {
+        for (int l = threadIdx.x; l < nl; l += blockDim.x) xg[r0 + l] = RCG(kVX, l);
+    }
+#undef RCG
+#undef RCG_G
+#undef RCG_SPMV
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         KrylovState *st = a.st;
         st->gamma = gamma; st->rr = rr; st->bs = bs; st->atol2 = atol2;
@@ -436,47 +654,77 @@ __global__ void __launch_bounds__(pcg_block<T>(), 1) cg_persistent_kernel(PcgArg
     }
 }
 
-// Grid size for the persistent kernel: every block must be resident at once.
-template <typename T, int MW>
-static int pcg_grid(int n) {
-    static int cached[2] = {0, 0};
-    int &c = cached[sizeof(T) == 8 ? 1 : 0];
-    if (c == 0) {
-        int dev = 0, sms = 0, per = 0;
+// Launch geometry of the resident kernel: one block per SM, rows split in
+// contiguous chunks, 6, 4 or 0 per-block vectors in shared memory.
+struct RcgPlan {
+    int grid, chunk, ns;
+    size_t smem_bytes;
+};
+
+template <typename T>
+static RcgPlan rcg_plan(int n) {
+    static int sms = 0, optin = 0;
+    if (sms == 0) {
+        int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, cg_persistent_kernel<T, MW>, pcg_block<T>(), 0);
-        c = sms * (per > 0 ? per : 1);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     }
-    const int need = (n + pcg_block<T>() - 1) / pcg_block<T>();
-    int g = need < c ? need : c;
-    if (g > kMaxPartials) g = kMaxPartials;
-    return g < 1 ? 1 : g;
+    RcgPlan pl;
+    int g = sms > 0 ? sms : 1;
+    const int need = (n + kSlice - 1) / kSlice;            // never more blocks than 32-row groups
+    if (g > need) g = need;
+    if (g > 1024) g = 1024;                                // partials [2][4][g] + [3][g] + flags fit the slot area
+    if (g < 1) g = 1;
+    pl.grid = g;
+    pl.chunk = (((n + g - 1) / g) + kSlice - 1) & ~(kSlice - 1);
+    const int64_t per_vec = (int64_t)pl.chunk * sizeof(T);
+    const int64_t room = (int64_t)optin - 4096;            // static shared memory of the kernel < 4 KB
+    pl.ns = room >= 6 * per_vec ? 6 : (room >= 4 * per_vec ? 4 : 0);
+    pl.smem_bytes = (size_t)(pl.ns * per_vec);
+    return pl;
+}
+
+template <typename T, int MW, int NS>
+static cudaError_t rcg_launch(const RcgPlan &pl, const RcgArgs<T> &a, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(cg_resident_kernel<T, MW, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pl.smem_bytes);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(pl.grid);
+    cfg.blockDim = dim3(kRcgBlock);
+    cfg.dynamicSmemBytes = pl.smem_bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, cg_resident_kernel<T, MW, NS>, a);
 }
 
 template <typename T>
 int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
                           const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
                           const double *tol_dev, cudaStream_t st) {
-    PcgArgs<T> a;
+    RcgArgs<T> a;
     a.A = A; a.vals = vals; a.b = b; a.b64 = b64; a.x = x; a.dinv = dinv;
-    a.r = w.r; a.z = w.z; a.p0 = w.p0; a.p1 = w.p1; a.q = w.q; a.part = w.partials; a.st = w.st;
+    a.z = w.z;
+    a.part = w.partials; a.st = w.st;
     a.bar = (GridBarrier *)&w.st->ticket[0];
+    a.zflag = reinterpret_cast<unsigned int *>(w.partials + 16 * 1024);    // after 11 * grid <= 11264 slots
     a.tol = tol; a.atol = atol; a.tol_dev = tol_dev; a.maxiter = maxiter; a.zero_x0 = zero_x0 ? 1 : 0;
+    // global homes of the vectors that stay off chip (x: the caller's array; M: read in place)
+    a.gvec[kVR] = w.r; a.gvec[kVP] = w.p0; a.gvec[kVS] = w.p1; a.gvec[kVW] = w.q;
+    a.gvec[kVX] = x;
+    a.gvec[kVD] = nullptr;
+    const RcgPlan pl = rcg_plan<T>(A.n_rows);
+    a.chunk = pl.chunk;
     cudaError_t e = cudaSuccess;
     WSPM_WIDTH_DISPATCH(A.max_width, {
-        const int grid = pcg_grid<T, MW>(A.n_rows);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3(pcg_block<T>());
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        e = cudaLaunchKernelEx(&cfg, cg_persistent_kernel<T, MW>, a);
+        if (pl.ns == 6) e = rcg_launch<T, MW, 6>(pl, a, st);
+        else if (pl.ns == 4) e = rcg_launch<T, MW, 4>(pl, a, st);
+        else e = rcg_launch<T, MW, 0>(pl, a, st);
     });
     return e == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }

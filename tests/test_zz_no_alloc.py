@@ -50,6 +50,7 @@ def test_noalloc_cg_matches_workspace_cg_twice():
     x_ref = x_ref.clone()
     ref = res_ref.cpu().numpy().copy()
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    first = None
     for call in range(2):                      # two calls in a row share the static scratch
         x = torch.as_tensor(h, device="cuda").clone()
         result = torch.full((4,), -7, dtype=torch.int32, device="cuda")
@@ -59,4 +60,11 @@ def test_noalloc_cg_matches_workspace_cg_twice():
         torch.cuda.synchronize()
         got = result.cpu().numpy()
         assert got[0] == ref[0] == 0 and got[1] == ref[1], (call, got, ref)
-        np.testing.assert_allclose(x.cpu().numpy(), x_ref.cpu().numpy(), rtol=1e-12, atol=1e-12)
+        # the workspace entry runs the single-reduction CG kernel, this one the two-reduction form: the same
+        # iteration count, iterates equal to the accuracy of a 1e-10 relative-residual solve
+        np.testing.assert_allclose(x.cpu().numpy(), x_ref.cpu().numpy(), rtol=1e-8, atol=1e-9)
+        # the second call on the reused scratch repeats the first bit for bit
+        if first is None:
+            first = x.cpu().numpy().copy()
+        else:
+            np.testing.assert_array_equal(x.cpu().numpy(), first)
