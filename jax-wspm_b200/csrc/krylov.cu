@@ -363,50 +363,113 @@ __device__ __forceinline__ void reduce_partials_rows(const T *partials, int nb, 
     for (int j = 0; j < NV; ++j) out[j] = bc[j];
 }
 
-// Row i of a DIA matrix times z with the values and gathers of a group of
-// diagonals in flight at once (8 in FP32, 4 in FP64), offsets from shared
-// memory; the products are accumulated in diagonal order like sell_row_dot.
-// z is read with plain (L1-cacheable) loads: inside a phase no block writes z,
-// and the acquire that ends the preceding wait (flag or barrier) followed by
-// the block barrier orders every earlier z store before these loads.
+// 16-byte vectors: a thread owns NV consecutive rows (4 in FP32, 2 in FP64) so
+// every matrix diagonal and every per-row vector moves as one 16-byte access.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+    using V = float4;
+    static constexpr int N = 4;
+    __device__ static __forceinline__ void split(const float4 &v, float (&o)[4]) {
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+    __device__ static __forceinline__ float4 join(const float (&o)[4]) { return make_float4(o[0], o[1], o[2], o[3]); }
+};
+template <> struct Vec16<double> {
+    using V = double2;
+    static constexpr int N = 2;
+    __device__ static __forceinline__ void split(const double2 &v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
+    __device__ static __forceinline__ double2 join(const double (&o)[2]) { return make_double2(o[0], o[1]); }
+};
+
+// Row i of A times z with the values and gathers of a group of diagonals in
+// flight at once, accumulated in diagonal order like sell_row_dot (used for
+// the ragged rows that do not fill a 16-byte group).  z is read with plain
+// loads: inside a phase no block writes z, and the acquire that ends the
+// preceding wait (flag or barrier) followed by the block barrier orders every
+// earlier z store before these loads.
 template <typename T, int MW>
 __device__ __forceinline__ T dia_row_z(const T *__restrict__ vals, int64_t ld, int i, int last, int nd,
                                        const int *s_off, const T *z) {
-    constexpr int G0 = sizeof(T) == 4 ? 8 : 4;
-    constexpr int G = MW < G0 ? MW : G0;
     T acc = T(0);
 #pragma unroll
-    for (int k0 = 0; k0 < MW; k0 += G) {
-        if (k0 >= nd) break;
-        T v[G], g[G];
-#pragma unroll
-        for (int q = 0; q < G; ++q) {
-            const int k = k0 + q;
-            if (k < nd) {
-                v[q] = __ldg(vals + (int64_t)k * ld + i);
-                int c = i + s_off[k];
-                c = c < 0 ? 0 : (c > last ? last : c);
-                g[q] = z[c];
-            }
+    for (int k = 0; k < MW; ++k) {
+        if (k < nd) {
+            int c = i + s_off[k];
+            c = c < 0 ? 0 : (c > last ? last : c);
+            acc = fma(__ldg(vals + (int64_t)k * ld + i), z[c], acc);
         }
-#pragma unroll
-        for (int q = 0; q < G; ++q)
-            if (k0 + q < nd) acc = fma(v[q], g[q], acc);
     }
     return acc;
 }
 
-// SpMV of z over local rows [l0, l1) of the block starting at row r0: w into
-// wbase[l], partial (w, z) into acc.
+// Rows i .. i+N-1 (i a multiple of N) of a DIA matrix times z: one 16-byte load
+// per diagonal, issued G diagonals at a time before their first use, then the
+// gathers diagonal by diagonal.  Each row accumulates in diagonal order.
+template <typename T, int MW>
+__device__ __forceinline__ void dia_group_z(const T *__restrict__ vals, int64_t ld, int i, int last, int nd,
+                                            const int *s_off, const T *z, T (&w)[Vec16<T>::N]) {
+    using VT = Vec16<T>;
+    constexpr int N = VT::N;
+    constexpr int G = MW < 4 ? MW : 4;
+#pragma unroll
+    for (int q = 0; q < N; ++q) w[q] = T(0);
+#pragma unroll
+    for (int k0 = 0; k0 < MW; k0 += G) {
+        if (k0 >= nd) break;
+        typename VT::V vv[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+            if (k0 + g < nd) vv[g] = __ldg(reinterpret_cast<const typename VT::V *>(vals + (int64_t)(k0 + g) * ld + i));
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            if (k0 + g < nd) {
+                T e[N];
+                VT::split(vv[g], e);
+                const int o = s_off[k0 + g];
+#pragma unroll
+                for (int q = 0; q < N; ++q) {
+                    int c = i + q + o;
+                    c = c < 0 ? 0 : (c > last ? last : c);
+                    w[q] = fma(e[q], z[c], w[q]);
+                }
+            }
+        }
+    }
+}
+
+// SpMV of z over local rows [l0, l1) of the block starting at row r0 (l0 a
+// multiple of N): w into wbase[l], partial (w, z) into acc.  DIA rows go in
+// 16-byte groups, SELL rows one by one.
 template <typename T, int MW>
 __device__ __forceinline__ void rcg_spmv_rows(int l0, int l1, T &acc, const Sell &A, const T *__restrict__ vals,
                                               int64_t ld, int r0, int last, int nd, const int *s_off, const T *z,
                                               bool dia, T *wbase) {
+    using VT = Vec16<T>;
+    constexpr int N = VT::N;
+    if (dia) {
+        for (int l = l0 + N * (int)threadIdx.x; l < l1; l += N * (int)blockDim.x) {
+            const int i = r0 + l;
+            if (l + N <= l1) {
+                T w[N];
+                dia_group_z<T, (MW > 0 ? MW : 1)>(vals, ld, i, last, nd, s_off, z, w);
+                *reinterpret_cast<typename VT::V *>(wbase + l) = VT::join(w);
+                T zo[N];
+                VT::split(*reinterpret_cast<const typename VT::V *>(z + i), zo);
+#pragma unroll
+                for (int q = 0; q < N; ++q) acc = fma(w[q], zo[q], acc);
+            } else {
+                for (int q = 0; l + q < l1; ++q) {
+                    const T wi = dia_row_z<T, (MW > 0 ? MW : 1)>(vals, ld, i + q, last, nd, s_off, z);
+                    wbase[l + q] = wi;
+                    acc = fma(wi, z[i + q], acc);
+                }
+            }
+        }
+        return;
+    }
     for (int l = l0 + threadIdx.x; l < l1; l += blockDim.x) {
         const int i = r0 + l;
-        T wi;
-        if (dia) wi = dia_row_z<T, (MW > 0 ? MW : 1)>(vals, ld, i, last, nd, s_off, z);
-        else wi = sell_row_dot<T, MW>(A, vals, i, [z](int c) { return z[c]; });
+        const T wi = sell_row_dot<T, MW>(A, vals, i, [z](int c) { return z[c]; });
         wbase[l] = wi;
         acc = fma(wi, z[i], acc);
     }
@@ -422,7 +485,8 @@ __device__ __forceinline__ void rcg_spmv_rows(int l0, int l1, T &acc, const Sell
 // chip for the whole solve, the others live in the workspace (x: the caller's
 // array).  z is the only vector that crosses blocks.  Per iteration the kernel
 // streams the matrix once and moves z once through L2, instead of the 11
-// vector passes of the textbook iteration.
+// vector passes of the textbook iteration.  A thread owns groups of N
+// consecutive rows (16 bytes) in both phases.
 //
 // Synchronisation per iteration: after its z update a block publishes a z
 // epoch flag; its SpMV first does the interior rows (DIA: rows whose columns
@@ -437,6 +501,9 @@ __device__ __forceinline__ void rcg_spmv_rows(int l0, int l1, T &acc, const Sell
 // the two-reduction form up to rounding.  Every wait is bounded (error flag).
 template <typename T, int MW, int NS>
 __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a) {
+    using VT = Vec16<T>;
+    using V = typename VT::V;
+    constexpr int N = VT::N;
     extern __shared__ __align__(16) unsigned char rcg_smem[];
     __shared__ int s_off[MW > 0 ? MW : 1];
     T *const sm = reinterpret_cast<T *>(rcg_smem);
@@ -465,7 +532,8 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     GridBarrier *const bar = a.bar;
     // vector v at local row l: shared memory for v < NS, else its global home
 #define RCG_G(v) ((v) == kVR ? gvR : (v) == kVP ? gvP : (v) == kVS ? gvS : gvW)
-#define RCG(v, l) (*((v) < NS ? (sm + (v) * chunk + (l)) : (RCG_G(v) + (l))))
+#define RCG_P(v, l) ((v) < NS ? (sm + (v) * chunk + (l)) : (RCG_G(v) + (l)))
+#define RCG(v, l) (*RCG_P(v, l))
     const int nd = A.n_diags;
     const bool dia = MW > 0 && nd > 0 && nd <= MW;
     int lo_i = 0, hi_i = 0, nbr_lo = 0, nbr_hi = nb - 1;
@@ -477,8 +545,9 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
             mn = min(mn, o);
             mx = max(mx, o);
         }
-        lo_i = min(nl, -mn);
-        hi_i = max(lo_i, nl - mx);
+        // interior rows [lo_i, hi_i), rounded inwards to whole 16-byte groups
+        lo_i = min(nl, (-mn + N - 1) / N * N);
+        hi_i = max(lo_i, (nl - mx) / N * N);
         const int rlo = max(0, r0 + mn), rhi = min(n - 1, r1 - 1 + mx);
         nbr_lo = min(nb - 1, rlo / chunk);
         nbr_hi = min(nb - 1, rhi / chunk);
@@ -559,40 +628,54 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
         }
         if (!isfinite(alpha)) { status = WSPM_NAN; break; }
         T *pp = part + (int64_t)(red & 1) * 4 * nb;
-        // ---- update phase (own rows only); rows in batches of RB with every load issued first
+        // ---- update phase (own rows only), 16-byte row groups
         {
-            constexpr int RB = sizeof(T) == 4 ? 4 : 2;
             const T al = (T)alpha, bt = (T)beta;
             T v[2] = {T(0), T(0)};
-            const int TB = blockDim.x;
-            for (int l0 = threadIdx.x; l0 < nl; l0 += RB * TB) {
-                T zz[RB], pv[RB], sv[RB], wv[RB], xv[RB], rv[RB], dv[RB];
+            for (int l = N * (int)threadIdx.x; l < nl; l += N * (int)blockDim.x) {
+                if (l + N <= nl) {
+                    T zz[N], pv[N], sv[N], wv[N], xv[N], rv[N], dv[N];
+                    VT::split(*reinterpret_cast<const V *>(z + r0 + l), zz);
+                    VT::split(*reinterpret_cast<const V *>(RCG_P(kVP, l)), pv);
+                    VT::split(*reinterpret_cast<const V *>(RCG_P(kVS, l)), sv);
+                    VT::split(*reinterpret_cast<const V *>(RCG_P(kVW, l)), wv);
+                    VT::split(*reinterpret_cast<const V *>(RCG_P(kVR, l)), rv);
+                    VT::split(*reinterpret_cast<const V *>(kVX < NS ? RCG_P(kVX, l) : xg + r0 + l), xv);
+                    if (kVD < NS) VT::split(*reinterpret_cast<const V *>(RCG_P(kVD, l)), dv);
+                    else if (dg) VT::split(__ldg(reinterpret_cast<const V *>(dg + r0 + l)), dv);
+                    else {
 #pragma unroll
-                for (int q = 0; q < RB; ++q) {
-                    const int l = l0 + q * TB;
-                    if (l < nl) {
-                        zz[q] = z[r0 + l];
-                        pv[q] = RCG(kVP, l); sv[q] = RCG(kVS, l); wv[q] = RCG(kVW, l);
-                        rv[q] = RCG(kVR, l);
-                        xv[q] = kVX < NS ? RCG(kVX, l) : xg[r0 + l];
-                        dv[q] = kVD < NS ? RCG(kVD, l) : (dg ? dg[r0 + l] : T(1));
+                        for (int q = 0; q < N; ++q) dv[q] = T(1);
                     }
-                }
 #pragma unroll
-                for (int q = 0; q < RB; ++q) {
-                    const int l = l0 + q * TB;
-                    if (l < nl) {
-                        const T pi = fma(bt, pv[q], zz[q]);
-                        const T si = fma(bt, sv[q], wv[q]);
-                        RCG(kVP, l) = pi;
-                        RCG(kVS, l) = si;
-                        const T xi = fma(al, pi, xv[q]);
-                        if (kVX < NS) RCG(kVX, l) = xi;
-                        else xg[r0 + l] = xi;
-                        const T ri = fma(-al, si, rv[q]);
-                        RCG(kVR, l) = ri;
-                        const T zi = dv[q] * ri;
-                        z[r0 + l] = zi;
+                    for (int q = 0; q < N; ++q) {
+                        pv[q] = fma(bt, pv[q], zz[q]);
+                        sv[q] = fma(bt, sv[q], wv[q]);
+                        xv[q] = fma(al, pv[q], xv[q]);
+                        rv[q] = fma(-al, sv[q], rv[q]);
+                        zz[q] = dv[q] * rv[q];
+                        v[0] += rv[q] * zz[q];
+                        v[1] += rv[q] * rv[q];
+                    }
+                    *reinterpret_cast<V *>(RCG_P(kVP, l)) = VT::join(pv);
+                    *reinterpret_cast<V *>(RCG_P(kVS, l)) = VT::join(sv);
+                    *reinterpret_cast<V *>(RCG_P(kVR, l)) = VT::join(rv);
+                    *reinterpret_cast<V *>(kVX < NS ? RCG_P(kVX, l) : xg + r0 + l) = VT::join(xv);
+                    *reinterpret_cast<V *>(z + r0 + l) = VT::join(zz);
+                } else {
+                    for (int q = 0; l + q < nl; ++q) {
+                        const int lq = l + q;
+                        const T pi = fma(bt, RCG(kVP, lq), z[r0 + lq]);
+                        const T si = fma(bt, RCG(kVS, lq), RCG(kVW, lq));
+                        RCG(kVP, lq) = pi;
+                        RCG(kVS, lq) = si;
+                        T *xp = kVX < NS ? RCG_P(kVX, lq) : xg + r0 + lq;
+                        *xp = fma(al, pi, *xp);
+                        const T ri = fma(-al, si, RCG(kVR, lq));
+                        RCG(kVR, lq) = ri;
+                        const T di = kVD < NS ? RCG(kVD, lq) : (dg ? dg[r0 + lq] : T(1));
+                        const T zi = di * ri;
+                        z[r0 + lq] = zi;
                         v[0] += ri * zi;
                         v[1] += ri * ri;
                     }
@@ -642,6 +725,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
         for (int l = threadIdx.x; l < nl; l += blockDim.x) xg[r0 + l] = RCG(kVX, l);
     }
 #undef RCG
+#undef RCG_P
 #undef RCG_G
 #undef RCG_SPMV
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -707,6 +791,10 @@ template <typename T>
 int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
                           const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
                           const double *tol_dev, cudaStream_t st) {
+    // the 16-byte row groups need 16-byte aligned arrays
+    const uintptr_t al = (uintptr_t)vals | (uintptr_t)x | (uintptr_t)w.z | (uintptr_t)w.r | (uintptr_t)w.p0 |
+                         (uintptr_t)w.p1 | (uintptr_t)w.q | (uintptr_t)(dinv ? dinv : vals);
+    if (al % 16) return WSPM_BAD_ARG;
     RcgArgs<T> a;
     a.A = A; a.vals = vals; a.b = b; a.b64 = b64; a.x = x; a.dinv = dinv;
     a.z = w.z;
