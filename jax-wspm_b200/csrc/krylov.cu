@@ -437,42 +437,68 @@ __device__ __forceinline__ void dia_group_z(const T *__restrict__ vals, int64_t 
     }
 }
 
-// SpMV of z over local rows [l0, l1) of the block starting at row r0 (l0 a
-// multiple of N): w into wbase[l], partial (w, z) into acc.  DIA rows go in
-// 16-byte groups, SELL rows one by one.
+// SpMV of z over local rows [l0, l1) of the block starting at row r0 (SELL
+// rows, one per thread): w into wbase[l], partial (w, z) into acc.
 template <typename T, int MW>
 __device__ __forceinline__ void rcg_spmv_rows(int l0, int l1, T &acc, const Sell &A, const T *__restrict__ vals,
-                                              int64_t ld, int r0, int last, int nd, const int *s_off, const T *z,
-                                              bool dia, T *wbase) {
-    using VT = Vec16<T>;
-    constexpr int N = VT::N;
-    if (dia) {
-        for (int l = l0 + N * (int)threadIdx.x; l < l1; l += N * (int)blockDim.x) {
-            const int i = r0 + l;
-            if (l + N <= l1) {
-                T w[N];
-                dia_group_z<T, (MW > 0 ? MW : 1)>(vals, ld, i, last, nd, s_off, z, w);
-                *reinterpret_cast<typename VT::V *>(wbase + l) = VT::join(w);
-                T zo[N];
-                VT::split(*reinterpret_cast<const typename VT::V *>(z + i), zo);
-#pragma unroll
-                for (int q = 0; q < N; ++q) acc = fma(w[q], zo[q], acc);
-            } else {
-                for (int q = 0; l + q < l1; ++q) {
-                    const T wi = dia_row_z<T, (MW > 0 ? MW : 1)>(vals, ld, i + q, last, nd, s_off, z);
-                    wbase[l + q] = wi;
-                    acc = fma(wi, z[i + q], acc);
-                }
-            }
-        }
-        return;
-    }
+                                              int r0, const T *z, T *wbase) {
     for (int l = l0 + threadIdx.x; l < l1; l += blockDim.x) {
         const int i = r0 + l;
         const T wi = sell_row_dot<T, MW>(A, vals, i, [z](int c) { return z[c]; });
         wbase[l] = wi;
         acc = fma(wi, z[i], acc);
     }
+}
+
+// SpMV phase of a DIA matrix over the block's rows in 16-byte groups: w into
+// wbase[l], partial (w, z) into acc.  The interior groups (columns inside the
+// block's own chunk) come first in one list with the halo groups; thread t
+// takes list entries t, t + T, ...  With poll, the block waits for its
+// neighbours' z flags before the first round that holds a halo group, so the
+// critical path is ceil(groups / T) rounds whatever the interior/halo split.
+// Returns false when that wait gave up.
+template <typename T, int MW>
+__device__ __forceinline__ bool rcg_spmv_dia(int nl, int lo_i, int hi_i, T &acc, const T *__restrict__ vals,
+                                             int64_t ld, int r0, int last, int nd, const int *s_off, const T *z,
+                                             T *wbase, const unsigned int *zflag, int nbr_lo, int nbr_hi,
+                                             unsigned int epoch, bool poll, GridBarrier *bar) {
+    using VT = Vec16<T>;
+    constexpr int N = VT::N;
+    const int ng = (nl + N - 1) / N;
+    const int gi0 = lo_i / N, gi1 = hi_i / N;
+    const int nint = gi1 - gi0, nlow = gi0;
+    const int TB = blockDim.x;
+    const int rounds = (ng + TB - 1) / TB;
+    const int m_wait = poll ? nint / TB : rounds;
+    for (int m = 0; m < rounds; ++m) {
+        if (m == m_wait && !wait_zflags(zflag, nbr_lo, nbr_hi, epoch, bar)) return false;
+        const int j = (int)threadIdx.x + m * TB;
+        if (j >= ng) continue;
+        int g;
+        if (j < nint) g = gi0 + j;
+        else {
+            const int h = j - nint;
+            g = h < nlow ? h : gi1 + (h - nlow);
+        }
+        const int l = g * N, i = r0 + l;
+        if (l + N <= nl) {
+            T w[N];
+            dia_group_z<T, MW>(vals, ld, i, last, nd, s_off, z, w);
+            *reinterpret_cast<typename VT::V *>(wbase + l) = VT::join(w);
+            T zo[N];
+            VT::split(*reinterpret_cast<const typename VT::V *>(z + i), zo);
+#pragma unroll
+            for (int q = 0; q < N; ++q) acc = fma(w[q], zo[q], acc);
+        } else {
+            for (int q = 0; l + q < nl; ++q) {
+                const T wi = dia_row_z<T, MW>(vals, ld, i + q, last, nd, s_off, z);
+                wbase[l + q] = wi;
+                acc = fma(wi, z[i + q], acc);
+            }
+        }
+    }
+    if (m_wait >= rounds && poll && !wait_zflags(zflag, nbr_lo, nbr_hi, epoch, bar)) return false;
+    return true;
 }
 
 // Whole preconditioned CG solve in one cooperative launch, single-reduction
@@ -603,12 +629,14 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     if (!isfinite(rs)) { done = true; status = WSPM_NAN; }
     unsigned int red = 0;      // counting barriers passed
     T *const wbase = kVW < NS ? sm + kVW * chunk : gvW;
-#define RCG_SPMV(l0, l1, acc) \
-    rcg_spmv_rows<T, MW>((l0), (l1), (acc), A, vals, ld, r0, last, nd, s_off, z, dia, wbase)
+#define RCG_SPMV_DIA(acc, epoch, poll)                                                                       \
+    rcg_spmv_dia<T, (MW > 0 ? MW : 1)>(nl, lo_i, hi_i, (acc), vals, ld, r0, last, nd, s_off, z, wbase, zflag, \
+                                       nbr_lo, nbr_hi, (epoch), (poll), bar)
     // w0 = A z0 and d0 = (w0, z0) when iterating
     if (!done && ok) {
         T v[1] = {T(0)};
-        RCG_SPMV(0, nl, v[0]);
+        if (dia) ok = RCG_SPMV_DIA(v[0], 0u, false);
+        else rcg_spmv_rows<T, MW>(0, nl, v[0], A, vals, r0, z, wbase);
         block_sum<T, 1>(v);
         T *pp = part + (int64_t)(red & 1) * 4 * nb;
         if (threadIdx.x == 0) pp[blockIdx.x] = v[0];
@@ -693,15 +721,12 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
         {
             T v[1] = {T(0)};
             if (dia) {
-                RCG_SPMV(lo_i, hi_i, v[0]);
-                ok = wait_zflags(zflag, nbr_lo, nbr_hi, (unsigned)(k + 1), bar);
+                ok = RCG_SPMV_DIA(v[0], (unsigned)(k + 1), true);
                 if (!ok) break;
-                RCG_SPMV(0, lo_i, v[0]);
-                RCG_SPMV(hi_i, nl, v[0]);
             } else {
                 ok = wait_zflags(zflag, 0, nb - 1, (unsigned)(k + 1), bar);
                 if (!ok) break;
-                RCG_SPMV(0, nl, v[0]);
+                rcg_spmv_rows<T, MW>(0, nl, v[0], A, vals, r0, z, wbase);
             }
             block_sum<T, 1>(v);
             if (threadIdx.x == 0) pp[blockIdx.x] = v[0];
@@ -727,7 +752,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
 #undef RCG
 #undef RCG_P
 #undef RCG_G
-#undef RCG_SPMV
+#undef RCG_SPMV_DIA
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         KrylovState *st = a.st;
         st->gamma = gamma; st->rr = rr; st->bs = bs; st->atol2 = atol2;
