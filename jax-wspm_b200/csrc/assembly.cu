@@ -51,6 +51,8 @@ struct RichardsAsmArgs {
     const double *dt_dev;   // when set, dt is read from device memory (graph replay)
     int n_diags;            // > 0: DIA layout, entry k of row i at k*ld + i
     int64_t ld;
+    const int32_t *diag_off;   // DIA column offsets
+    const int32_t *cols;       // SELL column indices
     double *vals;
     float *vals32;
     double *rhs, *dinv;
@@ -149,14 +151,28 @@ __device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM],
     }
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(128, 4) richards_rows_kernel(RichardsAsmArgs a) {
+// Row kernel.  Every vertex of an element incident to node i is a column of row
+// i, and the incidence word records, per element vertex, its position in the
+// row.  So the kernel first gathers the coordinates and K of the row's columns
+// (all loads in flight together, into shared memory), and the element loop
+// then reads each vertex from there: two dependent memory round trips per row
+// (incidence words; column data and per-element Ks) instead of walking
+// element id -> connectivity -> vertex data per element.  Vertex order inside
+// each element and the element order are unchanged, so every value and the
+// accumulation order are those of the element-walking form.
+template <int DIM, int MW>
+__global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
     constexpr int NV = DIM + 1;
-    extern __shared__ double acc_sm[];   // [max_width][blockDim.x]
+    const int TB = blockDim.x;
+    extern __shared__ double acc_sm[];   // [MW][TB] accumulators, then [MW][NV][TB] column data
+    __shared__ int s_off[MW];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = i >> 5, lane = i & 31;
-    if (s >= ((a.n_rows + kSlice - 1) >> 5)) return;
     const bool dia = a.n_diags > 0;
+    if (dia)
+        for (int k = threadIdx.x; k < a.n_diags; k += blockDim.x) s_off[k] = a.diag_off[k];
+    __syncthreads();
+    if (s >= ((a.n_rows + kSlice - 1) >> 5)) return;
     const int width = dia ? a.n_diags : a.slice_width[s];
     // entry k of this row lives at vb + kstride * k
     const int64_t vb = dia ? (int64_t)i : a.slice_ptr[s] + lane;
@@ -170,69 +186,88 @@ __global__ void __launch_bounds__(128, 4) richards_rows_kernel(RichardsAsmArgs a
         return;
     }
     double *acc = acc_sm + threadIdx.x;
-    const int stride = blockDim.x;
-    for (int k = 0; k < width; ++k) acc[k * stride] = 0.0;
+    double *colv = acc_sm + MW * TB + threadIdx.x;   // column k, component c at colv[(k * NV + c) * TB]
+    for (int k = 0; k < width; ++k) acc[k * TB] = 0.0;
     const int dpos = a.diag_pos[i];
 
     const double inv_dt = a.dt_dev ? 1.0 / *a.dt_dev : a.inv_dt;
     const double bcv = a.bc_val ? a.bc_val[i] : __longlong_as_double(0x7ff8000000000000ULL);
     double rhs_i, diag;
     if (!isnan(bcv)) {
-        acc[dpos * stride] = 1.0;
+        acc[dpos * TB] = 1.0;
         rhs_i = bcv;
         diag = 1.0;
     } else {
         const double Ci = a.C[i];
         const double tm = a.theta_m[i], tn = a.theta_n[i], hi = a.h_m[i];
         const double storage = tm - tn - Ci * hi;
-        double bsum = 0.0;
         const int deg = a.inc_width[s];
         const int64_t ib = a.inc_ptr[s] + lane;
-        // incidences in chunks of CH: the chunk's element ids, then its connectivity, then the
-        // vertex data are each loaded together, so a row pays 3 dependent memory round trips
-        // per chunk instead of per element
-        constexpr int CH = DIM == 2 ? 4 : 2;
-#pragma unroll 1
-        for (int k0 = 0; k0 < deg; k0 += CH) {
-            int ev[CH];
-            uint32_t pk[CH];
+        // column data of the row: coordinates and K, CG columns per batch of loads in flight
+        constexpr int CG = DIM == 2 ? 8 : 4;
+        const int last = a.n_rows - 1;
 #pragma unroll
-            for (int c = 0; c < CH; ++c) {
-                ev[c] = -1;
-                pk[c] = 0u;
-                if (k0 + c < deg) {
-                    ev[c] = __ldg(a.inc_elem + ib + (int64_t)kSlice * (k0 + c));
-                    pk[c] = __ldg(a.inc_slots + ib + (int64_t)kSlice * (k0 + c));
+        for (int k0 = 0; k0 < MW; k0 += CG) {
+            if (k0 >= width) break;
+            double xv[CG][DIM], kv[CG];
+#pragma unroll
+            for (int g = 0; g < CG; ++g) {
+                const int k = k0 + g;
+                if (k < width) {
+                    int c = dia ? i + s_off[k] : __ldg(a.cols + vb + kstride * k);
+                    c = c < 0 ? 0 : (c > last ? last : c);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) xv[g][d] = __ldg(a.coords + (int64_t)DIM * c + d);
+                    kv[g] = __ldg(a.K + c);
                 }
             }
-            int nd[CH][NV];
+#pragma unroll
+            for (int g = 0; g < CG; ++g) {
+                const int k = k0 + g;
+                if (k < width) {
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) colv[(k * NV + d) * TB] = xv[g][d];
+                    colv[(k * NV + DIM) * TB] = kv[g];
+                }
+            }
+        }
+        double bsum = 0.0;
+        // incidences in chunks of CH: ids and slot words, then the per-element Ks, then the math
+        constexpr int CH = 4;
+#pragma unroll 1
+        for (int k0 = 0; k0 < deg; k0 += CH) {
+            uint32_t pk[CH];
+            int ev[CH];
             double kse[CH];
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
-                const int e = ev[c] < 0 ? 0 : ev[c];
-#pragma unroll
-                for (int j = 0; j < NV; ++j) nd[c][j] = __ldg(a.conn + (int64_t)e * NV + j);
-                kse[c] = a.Ks_elem ? __ldg(a.Ks_elem + e) : 1.0;
-            }
-            double xyz[CH][NV][DIM], Kv[CH][NV];
-#pragma unroll
-            for (int c = 0; c < CH; ++c)
-#pragma unroll
-                for (int j = 0; j < NV; ++j) {
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) xyz[c][j][d] = __ldg(a.coords + (int64_t)DIM * nd[c][j] + d);
-                    Kv[c][j] = __ldg(a.K + nd[c][j]);
+                pk[c] = 0u;
+                ev[c] = -1;
+                if (k0 + c < deg) {
+                    pk[c] = __ldg(a.inc_slots + ib + (int64_t)kSlice * (k0 + c));
+                    ev[c] = __ldg(a.inc_elem + ib + (int64_t)kSlice * (k0 + c));   // -1: padding of the slice
                 }
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c) kse[c] = (a.Ks_elem && ev[c] >= 0) ? __ldg(a.Ks_elem + ev[c]) : 1.0;
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
                 if (ev[c] < 0) continue;
                 const uint32_t packed = pk[c];
                 const int li = packed & 3;
+                double X[NV][DIM], Kv[NV];
+#pragma unroll
+                for (int j = 0; j < NV; ++j) {
+                    const int kp = (packed >> (2 + 6 * j)) & 63;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) X[j][d] = colv[(kp * NV + d) * TB];
+                    Kv[j] = colv[(kp * NV + DIM) * TB];
+                }
                 double G[DIM][NV], detJ;
-                p1_geometry_xyz<DIM>(xyz[c], G, detJ);
+                p1_geometry_xyz<DIM>(X, G, detJ);
                 double Kbar = 0.0;
 #pragma unroll
-                for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], Kv[c][j], Kbar);
+                for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], Kv[j], Kbar);
                 if (a.Ks_elem) Kbar *= kse[c];
                 const double kd = Kbar * detJ;
                 const double Ml = a.mcoef[li] * detJ;
@@ -247,18 +282,18 @@ __global__ void __launch_bounds__(128, 4) richards_rows_kernel(RichardsAsmArgs a
                     double v = kd * gg;
                     if (j == li) v += inv_dt * (Ml * Ci);
                     const int kpos = (packed >> (2 + 6 * j)) & 63;
-                    acc[kpos * stride] += v;
+                    acc[kpos * TB] += v;
                 }
                 bsum += -kd * gli[DIM - 1] - inv_dt * (Ml * storage);
             }
         }
         rhs_i = bsum;
-        diag = acc[dpos * stride];
+        diag = acc[dpos * TB];
     }
     a.rhs[i] = rhs_i;
     if (a.dinv) a.dinv[i] = 1.0 / (diag != 0.0 ? diag : 1.0);
     for (int k = 0; k < width; ++k) {
-        const double v = acc[k * stride];
+        const double v = acc[k * TB];
         a.vals[vb + kstride * k] = v;
         if (a.vals32) a.vals32[vb + kstride * k] = (float)v;
     }
@@ -304,18 +339,32 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     a.n_diags = pat->n_diags;
     a.ld = (int64_t)pat->n_slices * kSlice;
     a.vals = vals; a.vals32 = vals32; a.rhs = rhs; a.dinv = dinv;
-    const int threads = 128;
+    a.diag_off = pat->diag_offsets;
+    a.cols = pat->cols;
+    const int mw = pat->max_width <= 8 ? 8 : (pat->max_width <= 16 ? 16 : (pat->max_width <= 32 ? 32 : 64));
+    if (pat->max_width > 63) return WSPM_UNSUPPORTED;      // the incidence word holds 6-bit row positions
+    const int threads = mw <= 16 ? 128 : (mw == 32 ? 64 : 32);
     const int blocks = (pat->n_slices * kSlice + threads - 1) / threads;
-    const size_t smem = (size_t)pat->max_width * threads * sizeof(double);
+    const size_t smem = (size_t)mw * threads * sizeof(double) * (1 + (mesh->dim + 1));
+#define WSPM_ASM_LAUNCH(D, M)                                                                              \
+    do {                                                                                                   \
+        if (smem > 48 * 1024)                                                                              \
+            cudaFuncSetAttribute(richards_rows_kernel<D, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                 (int)smem);                                                               \
+        richards_rows_kernel<D, M><<<blocks, threads, smem, st>>>(a);                                      \
+    } while (0)
     if (mesh->dim == 2) {
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(richards_rows_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        richards_rows_kernel<2><<<blocks, threads, smem, st>>>(a);
+        if (mw == 8) WSPM_ASM_LAUNCH(2, 8);
+        else if (mw == 16) WSPM_ASM_LAUNCH(2, 16);
+        else if (mw == 32) WSPM_ASM_LAUNCH(2, 32);
+        else WSPM_ASM_LAUNCH(2, 64);
     } else {
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(richards_rows_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        richards_rows_kernel<3><<<blocks, threads, smem, st>>>(a);
+        if (mw == 8) WSPM_ASM_LAUNCH(3, 8);
+        else if (mw == 16) WSPM_ASM_LAUNCH(3, 16);
+        else if (mw == 32) WSPM_ASM_LAUNCH(3, 32);
+        else WSPM_ASM_LAUNCH(3, 64);
     }
+#undef WSPM_ASM_LAUNCH
     return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }
 
