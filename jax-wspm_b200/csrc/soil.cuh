@@ -2,8 +2,9 @@
 //
 // van Genuchten-Mualem: src/models/van_genuchten.py:24-47 (branch on h < 0).
 // Gardner exponential:  src/models/exponential.py:24-41 (branch on h <= 0).
-// The operation order of the reference's jnp expressions is kept so results
-// agree with the oracle to a few ulps.
+// theta and C follow the reference's expressions; K is the same function
+// evaluated without the reference's cancellation (agrees with it to the
+// conditioning of its form).
 #pragma once
 #include "common.cuh"
 
@@ -19,18 +20,21 @@ __device__ __forceinline__ void soil_eval(const SoilParams &sp, double h,
     if (sp.model == WSPM_SOIL_VAN_GENUCHTEN) {
         const double alpha = sp.p[0], thS = sp.p[1], thR = sp.p[2], n = sp.p[3], m = sp.p[4], Ks = sp.p[5];
         if (h < 0.0) {
-            // (a|h|)^(n-1) by pow (exact enough down to |h| ~ 1e-300, where exp(x log a|h|) loses ~|x| ulps),
-            // (a|h|)^n by one multiply, (1 + (a|h|)^n)^-m through log1p/exp and (1 + (a|h|)^n)^(-m-1) by one
-            // division (the reference evaluates six pow() calls)
+            // Same functions as the reference, with its six pow() calls reduced algebraically:
+            //   a = (alpha|h|)^n, Se = (1 + a)^-m, Se^(1/m) = 1/(1 + a), 1 - Se^(1/m) = a/(1 + a)
+            //   K = Ks sqrt(Se) (1 - (a/(1+a))^m)^2,  (a/(1+a))^m = exp(m log(a/(1+a)))
+            // log(a/(1+a)) is -log1p(1/a) for a >= 1 and log(a/(1+a)) below, and 1 - exp(.) is -expm1(.), so
+            // neither end of the curve loses digits to cancellation (the reference's form does, at both ends).
+            // (alpha|h|)^(n-1) stays a pow: exp((n-1) log(alpha|h|)) loses ~|log| ulps at |h| ~ 1e-300.
             const double ah = alpha * fabs(h);
             const double ahn1 = pow(ah, n - 1.0);
             const double ahn = ahn1 * ah;
             const double onep = 1.0 + ahn;
             const double tm = exp(-m * log1p(ahn));
             theta = (thS - thR) * tm + thR;
-            const double Se = (theta - thR) / (thS - thR);
-            const double t = 1.0 - pow(1.0 - pow(Se, 1.0 / m), m);
-            K = Ks * (sqrt(Se) * (t * t));
+            const double log1mu = ahn >= 1.0 ? -log1p(1.0 / ahn) : log(ahn / onep);
+            const double t = -expm1(m * log1mu);
+            K = Ks * (sqrt(tm) * (t * t));
             C = (thS - thR) * alpha * m * n * ahn1 * (tm / onep);
         } else {
             theta = thS;
