@@ -75,8 +75,12 @@ def make_solver(cfg):
     if cfg.test_case == "Test3D":
         from src.solvers.richards_solver_3D_v2 import RichardsSolver3D
         return RichardsSolver3D(cfg)
-    if cfg.test_case in ("SoluteTest", "NitrogenTest"):
-        raise NotImplementedError(f"{cfg.test_case}: the transport drivers are not part of this build yet")
+    if cfg.test_case == "SoluteTest":
+        from src.solvers.coupled_solver_v2 import CoupledSolver
+        return CoupledSolver(cfg)
+    if cfg.test_case == "NitrogenTest":
+        from src.solvers.nitrogen_solver import NitrogenSolver
+        return NitrogenSolver(cfg)
     from src.solvers.richards_solver_v2 import RichardsSolver
     return RichardsSolver(cfg)
 
@@ -101,6 +105,14 @@ def main(argv=None):
             "memory_usage": 0.0}
     if args.test_case == "Test3D":
         save["elements"] = results["tetrahedra"]
+    elif args.test_case == "SoluteTest":
+        save["solute"] = results.get("solute")
+        save["elements"] = results["triangles"]
+    elif args.test_case == "NitrogenTest":
+        for k in ("NH4_concentration", "NO2_concentration", "NO3_concentration"):
+            save[k] = results[k]
+        save["elements"] = results["triangles"]
+        save["solute"] = None
     else:
         save["solute"] = None
         save["elements"] = results["triangles"]

@@ -126,3 +126,145 @@ def test_coupled_richards_step_with_neumann_and_drainage():
     res = eng.step(1e-3)
     assert res["status"] == 0 and res["iterations"] == it_ref
     np.testing.assert_allclose(host(eng.h_n), h_ref, rtol=1e-9, atol=1e-10)
+
+
+# ---------------------------------------------------------------- transport steps and drivers
+def _config(test_case, mesh_size, mesh_dir, solver="gmres", precond="jacobi", dt=1e-3):
+    from config.settings import SimulationConfig, SolverParameters, TimeSteppingParameters
+    cfg = SimulationConfig(time=TimeSteppingParameters(dt_init=dt, Tmax=1.0),
+                           solver=SolverParameters(solver_type=solver, precond_type=precond), test_case=test_case)
+    cfg.mesh.mesh_size = mesh_size
+    cfg.mesh.mesh_dir = mesh_dir
+    return cfg
+
+
+def _solute_mesh(tmp_path, n=20):
+    """[-0.5, 0.5] x [0, 2] split squares written as the reference's SoluteTest CSV files (1-based elements)."""
+    pts, tri = mesh.structured_triangles(n, 1.0)
+    pts = np.column_stack([pts[:, 0] - 0.5, 2.0 * pts[:, 1]])
+    d = tmp_path / "solute"
+    d.mkdir(parents=True, exist_ok=True)
+    np.savetxt(d / "p_Pinns_t.csv", pts, delimiter=",")
+    np.savetxt(d / "t_Pinns_t.csv", tri + 1, delimiter=",", fmt="%d")
+    return str(tmp_path)
+
+
+def test_solute_step_matches_oracle():
+    from wspm_b200.device import DeviceMesh
+    from wspm_b200.engine import default_rule
+    from wspm_b200.transport import edges_or_none, solute_step
+    pts, tri, h = field(seed=4)
+    top = np.where(pts[:, 1] == 1.0)[0]
+    fx = otr.fluxes_and_dispersion(pts, tri, h, VG_SOLUTE, 0.5, 0.1, 0.0)
+    qx, qz, aq, Dxx, Dxz, Dzz, th = fx
+    c_n = np.linspace(0.1, 0.3, len(pts))
+    want = otr.solute_step(pts, tri, c_n, th, th, qx, qz, Dxx, Dxz, Dzz, 1e-3, top, -0.1, 1.0,
+                           solver="gmres", precond="jacobi")
+    dm = DeviceMesh(pts, tri)
+    got, _ = solute_step(dm, cu(c_n), *[cu(a) for a in (th, qx, qz, Dxx, Dxz, Dzz)], 1e-3, default_rule(2),
+                         edges_or_none(dm, top), -0.1, 1.0, solver="gmres", precond="jacobi")
+    np.testing.assert_allclose(host(got), want, rtol=1e-9, atol=1e-11)
+
+
+def test_nitrogen_species_chain_matches_oracle():
+    from wspm_b200.device import DeviceMesh
+    from wspm_b200.engine import default_rule
+    from wspm_b200.transport import edges_or_none, nitrogen_species_step
+    pts, tri, h = field(seed=5)
+    top = np.where(np.abs(pts[:, 1] - 1.0) < 1e-10)[0]
+    bot = np.where(np.abs(pts[:, 1]) < 1e-10)[0]
+    qx, qz, aq, Dxx, Dxz, Dzz, th = otr.fluxes_and_dispersion(pts, tri, h, VG_SOLUTE, 0.04, 0.0004, 0.288e-4)
+    _, Kn, _ = osoil.van_genuchten_model(h, VG_SOLUTE)
+    rng = np.random.default_rng(6)
+    c1, c2, c3 = (rng.uniform(0, 5, len(pts)) for _ in range(3))
+    dm = DeviceMesh(pts, tri)
+    ce, fe = edges_or_none(dm, top), edges_or_none(dm, bot)
+    kw = dict(solver="gmres", precond="jacobi")
+    species = [(c1, 0.12, 1.6e-6 * 0.34e-6, 0.0, 50.0), (c2, 0.048, 0.0, 0.12, 0.0), (c3, 0.012, 0.0, 0.048, 20.0)]
+    up_ref = up_gpu = None
+    for c_n, mu, sorp, mu_up, c_in in species:
+        want = otr.nitrogen_species_step(pts, tri, c_n, th, qx, qz, Dxx, Dxz, Dzz, Kn, 2e-3, mu, sorp, mu_up, up_ref,
+                                         top, -0.05, c_in, bot, **kw)
+        got, _ = nitrogen_species_step(dm, cu(c_n), *[cu(a) for a in (th, qx, qz, Dxx, Dxz, Dzz, Kn)], 2e-3,
+                                       default_rule(2), mu=mu, sorption=sorp, mu_up=mu_up, c_up=up_gpu,
+                                       cauchy_edges=ce, cauchy_flux=-0.05, c_in=c_in, fd_edges=fe, **kw)
+        np.testing.assert_allclose(host(got), want, rtol=1e-9, atol=1e-9 * max(1.0, np.abs(want).max()))
+        up_ref, up_gpu = want, cu(want)
+
+
+def _oracle_transport_run(pts, tri, cfg, steps, nitrogen):
+    """The drivers' time loop restated on the oracle's step functions."""
+    from src.models.boundary import extract_boundary_nodes
+    phi = cfg.van_genuchten.to_array()
+    bn = extract_boundary_nodes(pts, cfg.test_case)
+    kw = dict(solver=cfg.solver.solver_type, precond=cfg.solver.precond_type, tol=cfg.solver.tol,
+              maxiter=cfg.solver.maxiter, restart=cfg.solver.restart)
+    n = len(pts)
+    h_n = (-1.0 if nitrogen else -1.3) * np.ones(n)
+    if nitrogen:
+        p = cfg.nitrogen
+        cs = [np.full(n, p.c_init_NH4), np.full(n, p.c_init_NO2), np.full(n, p.c_init_NO3)]
+    else:
+        c_n = np.full(n, cfg.solute.c_init)
+    dt = cfg.time.dt_init
+    hist = []
+    for _ in range(steps):
+        _, _, th_n = osoil.van_genuchten_model(h_n, phi)
+        if nitrogen:
+            h, err, it = otr.richards_neumann_step(pts, tri, h_n, th_n, dt, phi, bn.neumann, -0.05,
+                                                   fd_nodes=bn.freedrainage, picard_tol=1e-6, **kw)
+            p = cfg.nitrogen
+            qx, qz, aq, Dxx, Dxz, Dzz, th = otr.fluxes_and_dispersion(pts, tri, h, phi, p.DL, p.DT, p.Dm)
+            _, Kn, _ = osoil.van_genuchten_model(h, phi)
+            up = None
+            new = []
+            for c_n, mu, sorp, mu_up, c_in in ((cs[0], p.mu1, p.rho * p.Kd, 0.0, p.c_inlet_NH4),
+                                               (cs[1], p.mu2, 0.0, p.mu1, p.c_inlet_NO2),
+                                               (cs[2], p.mu3, 0.0, p.mu2, p.c_inlet_NO3)):
+                c = otr.nitrogen_species_step(pts, tri, c_n, th, qx, qz, Dxx, Dxz, Dzz, Kn, dt, mu, sorp, mu_up, up,
+                                              bn.cauchy, -0.05, c_in, bn.freedrainage, **kw)
+                new.append(c)
+                up = c
+            cs = new
+            hist.append((h, it, *cs))
+            dt = min(1.2 * dt, 0.01) if it <= 5 else (dt if it <= 15 else max(0.5 * dt, 1e-6))
+        else:
+            h, err, it = otr.richards_neumann_step(pts, tri, h_n, th_n, dt, phi, bn.neumann, -0.1, picard_tol=1e-4,
+                                                   **kw)
+            s = cfg.solute
+            qx, qz, aq, Dxx, Dxz, Dzz, th = otr.fluxes_and_dispersion(pts, tri, h, phi, s.DL, s.DT, s.Dm)
+            c_n = otr.solute_step(pts, tri, c_n, th, th_n, qx, qz, Dxx, Dxz, Dzz, dt, bn.cauchy, -0.1, s.c_inlet,
+                                  **kw)
+            hist.append((h, it, c_n))
+            t = cfg.time
+            dt = max(t.lambda_amp * dt if it <= t.m_it else (dt if it <= t.M_it else t.lambda_red * dt), 1e-6)
+        h_n = h
+    return hist
+
+
+def test_coupled_solver_matches_oracle_driver(tmp_path):
+    from src.solvers.coupled_solver_v2 import CoupledSolver
+    cfg = _config("SoluteTest", "t", _solute_mesh(tmp_path))
+    solver = CoupledSolver(cfg)
+    assert len(solver.boundary_nodes.cauchy) >= 2
+    res = solver.solve(max_steps=3)
+    want = _oracle_transport_run(solver.points, solver.triangles, cfg, 3, nitrogen=False)
+    for s, (h, it, c) in enumerate(want):
+        assert res["iterations"][s] == it
+        np.testing.assert_allclose(res["pressure_head"][s], h, rtol=1e-9, atol=1e-10)
+        np.testing.assert_allclose(res["solute"][s], c, rtol=1e-8, atol=1e-10)
+    assert set(res) >= {"pressure_head", "theta", "solute", "times", "iterations", "errors", "dt_values",
+                        "final_solute", "triangles"}
+
+
+def test_nitrogen_solver_matches_oracle_driver():
+    from src.solvers.nitrogen_solver import NitrogenSolver
+    cfg = _config("NitrogenTest", "25", None, dt=2e-3)
+    solver = NitrogenSolver(cfg)
+    res = solver.solve(max_steps=3)
+    want = _oracle_transport_run(solver.points, solver.triangles, cfg, 3, nitrogen=True)
+    for s, (h, it, nh4, no2, no3) in enumerate(want):
+        assert res["iterations"][s] == it
+        np.testing.assert_allclose(res["pressure_head"][s], h, rtol=1e-9, atol=1e-10)
+        for key, c in (("NH4_concentration", nh4), ("NO2_concentration", no2), ("NO3_concentration", no3)):
+            np.testing.assert_allclose(res[key][s], c, rtol=1e-8, atol=1e-8 * max(1.0, np.abs(c).max()))
