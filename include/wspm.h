@@ -291,6 +291,52 @@ int wspm_picard_step(void *plan, void *stream);
 int wspm_picard_step_host(void *plan, void *stream);
 int wspm_picard_destroy(void *plan);
 
+/* ---- batched ensemble of independent domains -------------------------------
+ * No single reference function: the reference solves one domain per
+ * RichardsSolver (richards_solver_v2.py:107-168 per step, :272-352 time
+ * loop); an ensemble there is a Python loop over solver instances.  Here the
+ * domains are the diagonal blocks of one mesh (node ranges node_off[d] ..
+ * node_off[d+1], elements never cross domains) and ONE persistent launch
+ * advances every active domain by one implicit step: each CTA takes the next
+ * domain from a device work queue (order[]: largest first), evaluates the VG
+ * soil law with that domain's parameters, assembles its rows, runs Jacobi-CG
+ * with block-level reductions, iterates Picard to the domain's own
+ * tolerance, then adapts that domain's dt (richards_solver_v2.py:91-105) and
+ * advances its time.  Domains with t >= tmax are skipped (the convergence
+ * mask).  Per-domain outcomes are written to its[], kits[], status[], err[]. */
+typedef struct wspm_ensemble {
+    int32_t n_domains;
+    const int64_t *node_off;   /* [n_domains + 1]                              */
+    const int32_t *order;      /* [n_domains] processing order                 */
+    const double  *phi;        /* [n_domains * 6] VG parameters per domain      */
+    const double  *Ks_elem;    /* [n_elems] per-element conductivity factor or NULL */
+    const double  *bc_val;     /* [n_nodes] Dirichlet values, NaN = free, or NULL */
+    double quad_points[16 * 3];
+    double weights[16];
+    int32_t nq;
+    double  krylov_tol;        /* relative residual of each CG solve           */
+    int32_t krylov_maxiter;
+    double  picard_tol;
+    int32_t picard_maxiter;
+    int32_t picard_relative;
+    double  tmax;
+    int32_t m_it, M_it;        /* dt rule: its <= m_it: dt *= lambda_amp ...  */
+    double  lambda_amp, lambda_red;
+    /* state (device) */
+    double *h_n;               /* [n_nodes] in: previous step, out: new step */
+    double *work;              /* wspm_ensemble_workspace_doubles()          */
+    int64_t work_doubles;
+    double *dt, *t;            /* [n_domains] current dt and time            */
+    int32_t *its, *kits, *status;  /* [n_domains] last step's Picard its, Krylov its, status */
+    double *err;               /* [n_domains] last step's Picard error       */
+    uint32_t *queue;           /* device word, zeroed by the call            */
+} wspm_ensemble;
+
+int64_t wspm_ensemble_workspace_doubles(int32_t n_rows, int64_t nnz_padded);
+/* block_threads: CTA size (128, 256 or 512; 0 = 512).                          */
+int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
+                       int32_t block_threads, void *stream);
+
 /* ---- misc ------------------------------------------------------------------ */
 const char *wspm_version(void);
 const char *wspm_status_string(int status);

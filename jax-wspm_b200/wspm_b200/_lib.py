@@ -55,8 +55,23 @@ class WspmPicardDesc(ctypes.Structure):
                 ("result", c_void_p), ("result_f64", c_void_p)]
 
 
+class WspmEnsemble(ctypes.Structure):
+    _fields_ = [("n_domains", c_int32), ("node_off", c_void_p), ("order", c_void_p), ("phi", c_void_p),
+                ("Ks_elem", c_void_p), ("bc_val", c_void_p),
+                ("quad_points", c_double * 48), ("weights", c_double * 16), ("nq", c_int32),
+                ("krylov_tol", c_double), ("krylov_maxiter", c_int32),
+                ("picard_tol", c_double), ("picard_maxiter", c_int32), ("picard_relative", c_int32),
+                ("tmax", c_double), ("m_it", c_int32), ("M_it", c_int32), ("lambda_amp", c_double),
+                ("lambda_red", c_double),
+                ("h_n", c_void_p), ("work", c_void_p), ("work_doubles", c_int64), ("dt", c_void_p), ("t", c_void_p),
+                ("its", c_void_p), ("kits", c_void_p), ("status", c_void_p), ("err", c_void_p),
+                ("queue", c_void_p)]
+
+
 P = ctypes.POINTER
 _SIGS = {
+    "wspm_ensemble_workspace_doubles": (c_int64, [c_int32, c_int64]),
+    "wspm_ensemble_step": (c_int32, [P(WspmMesh), P(WspmPattern), P(WspmEnsemble), c_int32, c_void_p]),
     "wspm_soil_van_genuchten": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_soil_exponential": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_assemble_richards": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p,

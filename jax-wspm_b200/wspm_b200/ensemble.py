@@ -1,0 +1,163 @@
+"""Batched ensemble of independent 2D Richards domains (one persistent launch per step).
+
+The reference runs one ``RichardsSolver`` per domain (richards_solver_v2.py);
+an ensemble there is a Python loop over solver instances.  ``Ensemble`` puts
+the domains on the diagonal of one mesh (node and element ids offset per
+domain, SELL-32 pattern over the union) and ``wspm_ensemble_step`` advances
+every domain still below ``tmax`` by one implicit step in a single launch:
+each CTA takes the next domain (largest first), runs its Picard loop with its
+own soil parameters, Dirichlet values and dt, and adapts that dt.  Domains that
+reached ``tmax`` are masked out of later launches.
+
+``autotune()`` times one step at each CTA size the kernel supports on a copy of
+the state and keeps the fastest.
+"""
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, dptr, lib
+from .device import DeviceMesh
+from .engine import default_rule
+
+BLOCK_SIZES = (128, 256, 512)
+
+
+class Ensemble:
+    """Independent domains d = 0..D-1, each ``(points, triangles, phi[6], bc_val or None, Ks_elem or None)``."""
+
+    def __init__(self, domains, dt0, tmax, krylov_tol=1e-10, krylov_maxiter=1000, picard_tol=1e-6,
+                 picard_maxiter=100, picard_relative=True, time_params=None, quad=None, device=None):
+        dev = torch.device(device or "cuda")
+        D = len(domains)
+        if D == 0:
+            raise ValueError("empty ensemble")
+        sizes = np.array([len(d[0]) for d in domains], dtype=np.int64)
+        node_off = np.zeros(D + 1, dtype=np.int64)
+        np.cumsum(sizes, out=node_off[1:])
+        pts = np.concatenate([np.asarray(d[0], dtype=np.float64) for d in domains])
+        tri = np.concatenate([np.asarray(d[1], dtype=np.int64) + node_off[i] for i, d in enumerate(domains)])
+        phi = np.stack([np.asarray(d[2], dtype=np.float64).reshape(6) for d in domains])
+        N = int(node_off[-1])
+        bc = np.full(N, np.nan)
+        ks = np.ones(len(tri))
+        has_ks = False
+        e0 = 0
+        for i, d in enumerate(domains):
+            ne = len(d[1])
+            if d[3] is not None:
+                bc[node_off[i]:node_off[i + 1]] = np.asarray(d[3], dtype=np.float64)
+            if len(d) > 4 and d[4] is not None:
+                ks[e0:e0 + ne] = np.asarray(d[4], dtype=np.float64)
+                has_ks = True
+            e0 += ne
+        self.n_domains, self.sizes, self.node_off_host = D, sizes, node_off
+        self.dm = DeviceMesh(pts, tri, layout="sell", device=dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.node_off = torch.as_tensor(node_off, device=dev)
+        self.order = torch.as_tensor(np.argsort(-sizes, kind="stable").astype(np.int32), device=dev)
+        self.phi = torch.as_tensor(phi.ravel(), **f64)
+        self.bc_val = torch.as_tensor(bc, **f64)
+        self.Ks_elem = torch.as_tensor(ks, **f64) if has_ks else None
+        self.h_n = torch.empty(N, **f64)
+        wd = int(lib.wspm_ensemble_workspace_doubles(N, self.dm.nnz_padded))
+        self.work = torch.empty(wd, **f64)
+        self.dt = torch.full((D,), float(dt0), **f64)
+        self.t = torch.zeros(D, **f64)
+        self.its, self.kits, self.status = (torch.zeros(D, **i32) for _ in range(3))
+        self.err = torch.zeros(D, **f64)
+        self.queue = torch.zeros(1, **i32)
+        tp = dict(m_it=5, M_it=7, lambda_amp=2.0, lambda_red=0.5)
+        tp.update(time_params or {})
+        Q, W = default_rule(2) if quad is None else quad
+        Q, W = np.ascontiguousarray(Q, dtype=np.float64).ravel(), np.ascontiguousarray(W, dtype=np.float64)
+        e = _lib.WspmEnsemble()
+        e.n_domains = D
+        e.node_off, e.order, e.phi = self.node_off.data_ptr(), self.order.data_ptr(), self.phi.data_ptr()
+        e.Ks_elem = self.Ks_elem.data_ptr() if self.Ks_elem is not None else None
+        e.bc_val = self.bc_val.data_ptr()
+        for j, v in enumerate(Q):
+            e.quad_points[j] = v
+        for j, v in enumerate(W):
+            e.weights[j] = v
+        e.nq = len(W)
+        e.krylov_tol, e.krylov_maxiter = float(krylov_tol), int(krylov_maxiter)
+        e.picard_tol, e.picard_maxiter, e.picard_relative = float(picard_tol), int(picard_maxiter), int(picard_relative)
+        e.tmax = float(tmax)
+        e.m_it, e.M_it = int(tp["m_it"]), int(tp["M_it"])
+        e.lambda_amp, e.lambda_red = float(tp["lambda_amp"]), float(tp["lambda_red"])
+        e.h_n, e.work, e.work_doubles = self.h_n.data_ptr(), self.work.data_ptr(), self.work.numel()
+        e.dt, e.t = self.dt.data_ptr(), self.t.data_ptr()
+        e.its, e.kits, e.status, e.err = (x.data_ptr() for x in (self.its, self.kits, self.status, self.err))
+        e.queue = self.queue.data_ptr()
+        self.c = e
+        self.tmax = float(tmax)
+        self.block_threads = 512
+
+    def set_state(self, h0):
+        """Initial head: one array over all nodes, or a scalar."""
+        if np.isscalar(h0):
+            self.h_n.fill_(float(h0))
+        else:
+            self.h_n.copy_(torch.as_tensor(np.asarray(h0, dtype=np.float64)).to(self.h_n.device))
+
+    def domain(self, d, x=None):
+        x = self.h_n if x is None else x
+        return x[int(self.node_off_host[d]):int(self.node_off_host[d + 1])]
+
+    def launch(self, stream=None):
+        st = stream if stream is not None else torch.cuda.current_stream()
+        check("ensemble_step", lib.wspm_ensemble_step(ctypes.byref(self.dm.c_mesh), ctypes.byref(self.dm.c_pat),
+                                                       ctypes.byref(self.c), int(self.block_threads),
+                                                       ctypes.c_void_p(st.cuda_stream)))
+
+    def active(self):
+        return int((self.t < self.tmax).sum().item())
+
+    def step(self):
+        """One implicit step of every active domain; returns per-domain (its, krylov its, status, err) on the host."""
+        active = (self.t < self.tmax).cpu().numpy()
+        self.launch()
+        return {"active": active, "iterations": self.its.cpu().numpy(), "krylov_iterations": self.kits.cpu().numpy(),
+                "status": self.status.cpu().numpy(), "error": self.err.cpu().numpy()}
+
+    def autotune(self, sizes=BLOCK_SIZES):
+        """Pick the CTA size with the fastest step on a copy of the current state (state restored)."""
+        saved = [x.clone() for x in (self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err)]
+        timing = {}
+        for tb in sizes:
+            for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
+                x.copy_(s)
+            self.block_threads = tb
+            self.launch()                       # warm
+            for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
+                x.copy_(s)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.launch()
+            e1.record()
+            torch.cuda.synchronize()
+            timing[tb] = e0.elapsed_time(e1)
+        for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
+            x.copy_(s)
+        self.block_threads = min(timing, key=timing.get)
+        self.timing = timing
+        return self.block_threads
+
+    def run(self, max_steps=None):
+        """Steps until every domain reached tmax (or max_steps launches); per-launch host records."""
+        out = {"iterations": [], "krylov_iterations": [], "active": [], "status": []}
+        t0 = time.perf_counter()
+        n = 0
+        while self.active() and (max_steps is None or n < max_steps):
+            r = self.step()
+            for k in out:
+                out[k].append(r[k])
+            n += 1
+        out = {k: np.array(v) for k, v in out.items()}
+        out["wall_time"] = time.perf_counter() - t0
+        return out

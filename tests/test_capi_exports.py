@@ -44,3 +44,5 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.wspm_picard_create(None, None) == _lib.WSPM_BAD_ARG
     pat = _lib.WspmPattern()
     assert lib.wspm_jacobi_dinv(ctypes.byref(pat), None, None, None) == _lib.WSPM_BAD_ARG
+    assert lib.wspm_ensemble_step(None, None, None, 0, None) == _lib.WSPM_BAD_ARG
+    assert lib.wspm_ensemble_workspace_doubles(0, 10) == 0

@@ -1,0 +1,70 @@
+"""Batched ensemble (one persistent launch per step) against one single-domain engine per domain.
+
+Each domain of the ensemble must take the same Picard iterations and reach the
+same head as the single-domain Picard engine run with the same soil
+parameters, Dirichlet values, tolerances and dt rule.  The two paths use
+different CG forms (block-level textbook CG vs the single-reduction resident
+kernel), so fields agree to the solve accuracy (rtol 1e-8), not bit for bit.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from wspm_b200 import mesh  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _domains(sizes, seed=0):
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in sizes:
+        pts, tri = mesh.structured_triangles(s, 1.0)
+        alpha = np.exp(rng.uniform(np.log(1.0), np.log(10.0)))
+        n = np.exp(rng.uniform(np.log(1.3), np.log(3.0)))
+        Ks = np.exp(rng.uniform(np.log(0.01), np.log(1.0)))
+        phi = (alpha, 0.40, 0.05, n, 1.0 - 1.0 / n, Ks)
+        bc = np.full(len(pts), np.nan)
+        bc[np.abs(pts[:, 1] - 1.0) < 1e-12] = -0.1
+        out.append((pts, tri, phi, bc, None))
+    return out
+
+
+def test_ensemble_matches_single_domain_engines():
+    from wspm_b200.device import DeviceMesh
+    from wspm_b200.engine import PicardEngine
+    from wspm_b200.ensemble import Ensemble
+    doms = _domains([8, 12, 16, 10, 20, 6])
+    steps = 4
+    ens = Ensemble(doms, dt0=1e-3, tmax=1.0, krylov_tol=1e-10, krylov_maxiter=1000)
+    ens.set_state(-1.0)
+    recs = [ens.step() for _ in range(steps)]
+    for d, (pts, tri, phi, bc, _) in enumerate(doms):
+        eng = PicardEngine(DeviceMesh(pts, tri), "vg", phi, bc_val=bc, solver="cg", precond="jacobi",
+                           krylov_tol=1e-10, krylov_maxiter=1000, picard_tol=1e-6, picard_maxiter=100,
+                           picard_relative=True)
+        ref = eng.run(-1.0 * np.ones(len(pts)), 1e-3, 1.0, max_steps=steps)
+        assert [int(r["iterations"][d]) for r in recs] == list(ref["iterations"]), d
+        assert all(int(r["status"][d]) == 0 for r in recs)
+        np.testing.assert_allclose(ens.domain(d).cpu().numpy(), ref["pressure_head"][-1], rtol=1e-8, atol=1e-10)
+        np.testing.assert_allclose(ens.dt[d].item(), ref["dt_values"][-1], rtol=0, atol=0)
+
+
+def test_ensemble_masks_finished_domains_and_autotunes():
+    from wspm_b200.ensemble import BLOCK_SIZES, Ensemble
+    doms = _domains([6, 14, 9], seed=3)
+    ens = Ensemble(doms, dt0=2e-3, tmax=5e-3, krylov_tol=1e-10, krylov_maxiter=1000)
+    ens.set_state(-1.0)
+    assert ens.autotune() in BLOCK_SIZES
+    assert torch.all(ens.t == 0)                      # autotune restored the state
+    out = ens.run(max_steps=50)
+    assert ens.active() == 0
+    t = ens.t.cpu().numpy()
+    assert np.all(t >= 5e-3)
+    # a finished domain is skipped: one more launch changes nothing
+    h = ens.h_n.clone()
+    ens.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(h, ens.h_n) and np.array_equal(t, ens.t.cpu().numpy())
+    assert out["active"].shape[1] == 3 and out["active"][0].all()
