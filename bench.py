@@ -320,6 +320,98 @@ def cg_probe(args):
     print(f"cg probe {args.cg_probe}: {args.probe_iters} iterations, |x| = {float(torch.linalg.norm(x.double())):.6e}")
 
 
+def ensemble_domains(n_domains, seed, sides=tuple(range(32, 257, 16))):
+    """Config-3 ensemble: side lengths uniform in {32, 48, ..., 256}; VG alpha, n, Ks log-uniform in
+    [1, 10], [1.3, 3], [0.01, 1]; theta_r .05, theta_s .40; h0 -1, top Dirichlet -0.1 (as the unit-square case)."""
+    from wspm_b200 import mesh
+    rng = np.random.default_rng(seed)
+    lu = lambda lo, hi: float(np.exp(rng.uniform(np.log(lo), np.log(hi))))  # noqa: E731
+    cache, doms = {}, []
+    for _ in range(n_domains):
+        s = int(rng.choice(sides))
+        if s not in cache:
+            pts, tri = mesh.structured_triangles(s, 1.0)
+            bc = np.full(len(pts), np.nan)
+            bc[np.abs(pts[:, 1] - 1.0) < 1e-12] = -0.1
+            cache[s] = (pts, tri, bc)
+        pts, tri, bc = cache[s]
+        n = lu(1.3, 3.0)
+        doms.append((pts, tri, (lu(1.0, 10.0), 0.40, 0.05, n, 1.0 - 1.0 / n, lu(0.01, 1.0)), bc, None))
+    return doms
+
+
+def run_ensemble(args):
+    """Batched ensemble (one launch per step for all domains) vs one single-domain engine per domain."""
+    import torch
+    from wspm_b200.device import DeviceMesh
+    from wspm_b200.engine import PicardEngine
+    from wspm_b200.ensemble import Ensemble
+    torch.cuda.set_device(0)
+    doms = ensemble_domains(args.domains, args.seed)
+    sizes = np.array([len(d[0]) for d in doms])
+    dt0, tmax = 1e-4, 1.0
+    kw = dict(krylov_tol=1e-10, krylov_maxiter=2000, picard_tol=1e-6, picard_maxiter=100)
+    ens = Ensemble(doms, dt0=dt0, tmax=tmax, **kw)
+    ens.set_state(-1.0)
+    tuned = ens.autotune()
+    for _ in range(args.warmup):
+        ens.step()
+    its_dev = torch.zeros(len(doms), dtype=torch.int64, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        act = ens.t < tmax                      # device-side mask: no host round trip in the timed loop
+        ens.launch()
+        its_dev += torch.where(act, ens.its, 0)
+    e1.record()
+    torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1) * 1e-3
+    its_b = its_dev.cpu().numpy()
+    dofits = int((sizes * its_b).sum())
+    # sequential: one engine per domain, each advanced by the same steps
+    engines, meshes = [], {}
+    for pts, tri, phi, bc, _ in doms:
+        if len(pts) not in meshes:
+            meshes[len(pts)] = DeviceMesh(pts, tri)
+        eng = PicardEngine(meshes[len(pts)], "vg", phi, bc_val=bc, solver="cg", precond="jacobi",
+                           krylov_maxiter=2000, krylov_tol=1e-10, picard_tol=1e-6, picard_maxiter=100,
+                           picard_relative=True)
+        eng.set_state(-1.0 * np.ones(len(pts)))
+        engines.append(eng)
+    from wspm_b200.engine import adapt_time_step
+    dts = [dt0] * len(doms)
+    for _ in range(args.warmup):
+        for j, eng in enumerate(engines):
+            dts[j] = float(adapt_time_step(dts[j], eng.step(dts[j])["iterations"]))
+    its_s = np.zeros(len(doms), dtype=np.int64)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        for j, eng in enumerate(engines):
+            eng.launch_step(dts[j])
+            r = eng.read_result()           # the dt rule needs the step's iterations on the host
+            its_s[j] += r["iterations"]
+            dts[j] = float(adapt_time_step(dts[j], r["iterations"]))
+    e1.record()
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1) * 1e-3
+    line = {"metric": "ensemble DOF*Picard-iter/s (batched domains, one launch per step)",
+            "value": dofits / t_batch, "unit": "DOF*Picard-iter/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+            "data": f"synthetic (seed {args.seed})",
+            "config": {"workload": f"{len(doms)} independent 2D Richards domains, sides uniform in "
+                                   "{32,...,256}, VG alpha/n/Ks log-uniform, theta_r .05, theta_s .40, "
+                                   "h0 -1, top Dirichlet -0.1, dt0 1e-4 adaptive per domain",
+                       "nodes_total": int(sizes.sum()), "domains": len(doms)},
+            "batched": {"seconds": t_batch, "picard_its": int(its_b.sum()), "block_threads": tuned,
+                        "autotune_ms": getattr(ens, "timing", {})},
+            "sequential": {"seconds": t_seq, "picard_its": int(its_s.sum()),
+                           "value": float((sizes * its_s).sum()) / t_seq},
+            "speedup_vs_sequential": t_seq / t_batch * (dofits / max(1, int((sizes * its_s).sum())))}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -335,6 +427,10 @@ def main():
                     help="profiling target: assemble the workload once and run --probe-iters CG iterations "
                          "through wspm_cg_iterations, then exit (no JSON line)")
     ap.add_argument("--probe-iters", type=int, default=4)
+    ap.add_argument("--ensemble", action="store_true",
+                    help="batched-ensemble workload (independent domains, one launch per step) against one "
+                         "single-domain engine per domain; prints its own JSON line")
+    ap.add_argument("--domains", type=int, default=256)
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Picard/Krylov loops from the host (same kernels; for ncu, which cannot "
                          "profile kernels inside conditional graphs)")
@@ -343,6 +439,8 @@ def main():
         return run_reference(args)
     if args.cg_probe:
         return cg_probe(args)
+    if args.ensemble:
+        return run_ensemble(args)
 
     import torch
     from wspm_b200.device import DeviceMesh, merge_dirichlet
