@@ -337,6 +337,40 @@ int64_t wspm_ensemble_workspace_doubles(int32_t n_rows, int64_t nnz_padded);
 int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
                        int32_t block_threads, void *stream);
 
+/* ---- per-element soil parameters and the discrete adjoint --------------------
+ * No reference counterpart: the reference evaluates one van Genuchten
+ * parameter set per run (van_genuchten.py:9-47) and differentiates with JAX.
+ * Here every element e carries params[3e..3e+2] = (ln Ks, ln alpha, ln n),
+ * m = 1 - 1/n, theta_r / theta_s shared; the soil law is evaluated per element
+ * at its vertices, and the element matrices follow assembly_re_v2.py:13-60
+ * with those element-wise values (2D P1 triangles).
+ *   wspm_elem_assemble_richards: the Picard system A(h_m) h = b(h_m, h_n) with
+ *     Dirichlet rows (bc_val, NaN = free) and Jacobi 1/diag (dinv may be NULL).
+ *   wspm_elem_assemble_jt: J^T, J = dR/dh of the converged-step residual
+ *     R(h) = sum_e Kbar_e detJ G.(grad h + e_z) + Ml (theta(h) - theta(h_old))/dt.
+ *   wspm_elem_adjoint_rhs: rhs = g + lam_next * sum_e Ml C(h_old) / dt_next on free rows.
+ *   wspm_elem_theta_node: theta_node = sum_e Ml theta_e / sum_e Ml, its d/dh, the lumped mass.
+ *   wspm_elem_param_grad: grad[E][3] += -(dR/dp)^T lam + direct theta-sensor term (wl = dL/dtheta_node). */
+int wspm_elem_assemble_richards(const wspm_mesh *mesh, const wspm_pattern *pat, const double *params,
+                                double theta_r, double theta_s, const double *quad_points, const double *weights,
+                                int32_t nq, double dt, const double *bc_val, const double *h_m, const double *h_n,
+                                double *vals, double *rhs, double *dinv, void *stream);
+int wspm_elem_assemble_jt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *params, double theta_r,
+                          double theta_s, const double *quad_points, const double *weights, int32_t nq, double dt,
+                          const double *bc_val, const double *h, const double *h_old, double *vals, double *dinv,
+                          void *stream);
+int wspm_elem_adjoint_rhs(const wspm_mesh *mesh, const wspm_pattern *pat, const double *params, double theta_r,
+                          double theta_s, const double *quad_points, const double *weights, int32_t nq,
+                          double dt_next, const double *bc_val, const double *h_old, const double *lam_next,
+                          const double *g, double *rhs, void *stream);
+int wspm_elem_theta_node(const wspm_mesh *mesh, const wspm_pattern *pat, const double *params, double theta_r,
+                         double theta_s, const double *quad_points, const double *weights, int32_t nq,
+                         const double *h, double *theta_node, double *dtheta_dh, double *mass, void *stream);
+int wspm_elem_param_grad(const wspm_mesh *mesh, const wspm_pattern *pat, const double *params, double theta_r,
+                         double theta_s, const double *quad_points, const double *weights, int32_t nq, double dt,
+                         const double *bc_val, const double *h, const double *h_old, const double *lam,
+                         const double *wl, const double *mass, double *grad, void *stream);
+
 /* ---- misc ------------------------------------------------------------------ */
 const char *wspm_version(void);
 const char *wspm_status_string(int status);

@@ -71,6 +71,20 @@ class WspmEnsemble(ctypes.Structure):
 P = ctypes.POINTER
 _SIGS = {
     "wspm_ensemble_workspace_doubles": (c_int64, [c_int32, c_int64]),
+    "wspm_elem_assemble_richards": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_double, c_double,
+                                              P(c_double), P(c_double), c_int32, c_double, c_void_p, c_void_p,
+                                              c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_elem_assemble_jt": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_double, c_double, P(c_double),
+                                        P(c_double), c_int32, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
+    "wspm_elem_adjoint_rhs": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_double, c_double, P(c_double),
+                                        P(c_double), c_int32, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
+    "wspm_elem_theta_node": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_double, c_double, P(c_double),
+                                       P(c_double), c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wspm_elem_param_grad": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_double, c_double, P(c_double),
+                                       P(c_double), c_int32, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_ensemble_step": (c_int32, [P(WspmMesh), P(WspmPattern), P(WspmEnsemble), c_int32, c_void_p]),
     "wspm_soil_van_genuchten": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_soil_exponential": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
