@@ -412,6 +412,71 @@ def run_ensemble(args):
     print(json.dumps(line))
 
 
+def run_adjoint(args):
+    """Adjoint vs forward time on the per-element-parameter problem, and a finite-difference check."""
+    print(json.dumps(adjoint_measure(args.adjoint_n, args.adjoint_steps, args.seed, args.fd_params)))
+
+
+def adjoint_measure(n, steps, seed, fd_params):
+    import torch
+    from wspm_b200 import mesh
+    from wspm_b200.adjoint import ElementParamRichards
+    from wspm_b200.device import DeviceMesh
+    torch.cuda.set_device(0)
+    pts, tri = mesh.structured_triangles(n, 1.0)
+    bc = np.full(len(pts), np.nan)
+    bc[np.abs(pts[:, 1] - 1.0) < 1e-12] = -0.1
+    dm = DeviceMesh(pts, tri)
+    rng = np.random.default_rng(seed)
+    base = np.log([0.0922, 3.35, 2.0])
+    params = base[None, :] + 0.3 * rng.standard_normal((len(tri), 3))
+    target_params = base[None, :] + 0.3 * rng.standard_normal((len(tri), 3))
+    sensors = rng.choice(np.where(np.isnan(bc))[0], 64, replace=False)
+    h0 = torch.full((len(pts),), -1.0, dtype=torch.float64, device="cuda")
+    tol = dict(picard_tol=1e-12, krylov_tol=1e-13, adjoint_tol=1e-12)
+    prob = ElementParamRichards(dm, 0.102, 0.368, bc, 1e-3, steps, checkpoint_every=10, **tol)
+    p = torch.as_tensor(params, dtype=torch.float64, device="cuda").view(-1)
+    target = prob.simulate_theta(torch.as_tensor(target_params, dtype=torch.float64, device="cuda").view(-1), h0,
+                                 sensors)
+    prob.forward(p, h0, sensors, target)          # warm-up
+    prob.backward()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = prob.forward(p, h0, sensors, target)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    picard_fwd = int(sum(prob.picard_its))
+    t0 = time.perf_counter()
+    grad = prob.backward()
+    torch.cuda.synchronize()
+    t_bwd = time.perf_counter() - t0
+    g = grad.cpu().numpy().ravel()
+    fd = {}
+    if fd_params > 0:
+        idx = rng.choice(g.size, fd_params, replace=False)
+        eps, errs = 1e-6, []
+        scale = np.abs(g).max()
+        for j in idx:
+            pp, pm = p.clone(), p.clone()
+            pp[j] += eps
+            pm[j] -= eps
+            d = (float(prob.forward(pp, h0, sensors, target)) - float(prob.forward(pm, h0, sensors, target))) / (2 * eps)
+            errs.append(abs(g[j] - d) / max(abs(d), 1e-3 * scale))
+        fd = {"params": int(fd_params), "step": eps, "max_rel_err": float(max(errs)),
+              "median_rel_err": float(np.median(errs))}
+    line = {"metric": "adjoint/forward time (discrete adjoint, per-element ln Ks, ln alpha, ln n)",
+            "value": t_bwd / t_fwd, "unit": "ratio", "n_gpus": 1, "higher_is_better": False, "dtype": "f64",
+            "data": f"synthetic (seed {seed})",
+            "config": {"workload": f"{n}^2 P1 triangles, VG means (Ks .0922, alpha 3.35, n 2), ln-parameter "
+                                   f"perturbations sigma 0.3 per element, h0 -1, top Dirichlet -0.1, {steps} steps "
+                                   "at dt 1e-3, 64 theta sensors every step, target from a second draw, "
+                                   "checkpoints every 10 steps", "nodes": len(pts), "elements": len(tri),
+                       "parameters": 3 * len(tri), "picard_tol": 1e-12},
+            "forward_s": t_fwd, "backward_s": t_bwd, "loss": float(loss), "picard_its_forward": picard_fwd,
+            "fd_check": fd}
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -431,6 +496,13 @@ def main():
                     help="batched-ensemble workload (independent domains, one launch per step) against one "
                          "single-domain engine per domain; prints its own JSON line")
     ap.add_argument("--domains", type=int, default=256)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="discrete-adjoint workload: forward and backward time, finite-difference check; prints "
+                         "its own JSON line")
+    ap.add_argument("--adjoint-n", type=int, default=256)
+    ap.add_argument("--adjoint-steps", type=int, default=100)
+    ap.add_argument("--fd-params", type=int, default=32)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement of the main line")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Picard/Krylov loops from the host (same kernels; for ncu, which cannot "
                          "profile kernels inside conditional graphs)")
@@ -441,6 +513,8 @@ def main():
         return cg_probe(args)
     if args.ensemble:
         return run_ensemble(args)
+    if args.adjoint:
+        return run_adjoint(args)
 
     import torch
     from wspm_b200.device import DeviceMesh, merge_dirichlet
@@ -522,6 +596,12 @@ def main():
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(args.n, args.seed)
+    if world == 1 and not args.no_adjoint:
+        # second part of the metric: adjoint / forward time of the per-element-parameter run
+        a = adjoint_measure(args.adjoint_n, args.adjoint_steps, args.seed, 0)
+        line["adjoint"] = {"adjoint_over_forward": a["value"], "forward_s": a["forward_s"],
+                           "backward_s": a["backward_s"], "workload": a["config"]["workload"],
+                           "parameters": a["config"]["parameters"]}
     print(json.dumps(line))
     barrier(world)
     if world > 1:
