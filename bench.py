@@ -123,6 +123,16 @@ def barrier(world):
     torch.cuda.synchronize()
 
 
+def allreduce_sum(v, world):
+    import torch
+    if world == 1:
+        return v
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def allreduce_max(v, world):
     import torch
     if world == 1:
@@ -346,8 +356,13 @@ def run_ensemble(args):
     from wspm_b200.device import DeviceMesh
     from wspm_b200.engine import PicardEngine
     from wspm_b200.ensemble import Ensemble
-    torch.cuda.set_device(0)
-    doms = ensemble_domains(args.domains, args.seed)
+    from wspm_b200.ensemble import gather_domain_results, partition_domains
+    world, rank, _ = dist_setup(args)
+    all_doms = ensemble_domains(args.domains, args.seed)
+    # shard the independent domains over the ranks, balancing nnz (7 per node for these meshes); no collective
+    # on the data path, one gather of the per-domain iteration counts at the end
+    mine = partition_domains([7 * len(d[0]) for d in all_doms], world)[rank]
+    doms = [all_doms[int(i)] for i in mine]
     sizes = np.array([len(d[0]) for d in doms])
     dt0, tmax = 1e-4, 1.0
     kw = dict(krylov_tol=1e-10, krylov_maxiter=2000, picard_tol=1e-6, picard_maxiter=100)
@@ -358,17 +373,18 @@ def run_ensemble(args):
         ens.step()
     its_dev = torch.zeros(len(doms), dtype=torch.int64, device="cuda")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
+    barrier(world)
     e0.record()
     for _ in range(args.steps):
         act = ens.t < tmax                      # device-side mask: no host round trip in the timed loop
         ens.launch()
         its_dev += torch.where(act, ens.its, 0)
     e1.record()
-    torch.cuda.synchronize()
-    t_batch = e0.elapsed_time(e1) * 1e-3
+    barrier(world)
+    t_batch = allreduce_max(e0.elapsed_time(e1) * 1e-3, world)
     its_b = its_dev.cpu().numpy()
-    dofits = int((sizes * its_b).sum())
+    dofits = int(allreduce_sum(float((sizes * its_b).sum()), world))
+    its_all = gather_domain_results(mine, its_b, len(all_doms), world)
     # sequential: one engine per domain, each advanced by the same steps
     engines, meshes = [], {}
     for pts, tri, phi, bc, _ in doms:
@@ -385,7 +401,7 @@ def run_ensemble(args):
         for j, eng in enumerate(engines):
             dts[j] = float(adapt_time_step(dts[j], eng.step(dts[j])["iterations"]))
     its_s = np.zeros(len(doms), dtype=np.int64)
-    torch.cuda.synchronize()
+    barrier(world)
     e0.record()
     for _ in range(args.steps):
         for j, eng in enumerate(engines):
@@ -394,21 +410,30 @@ def run_ensemble(args):
             its_s[j] += r["iterations"]
             dts[j] = float(adapt_time_step(dts[j], r["iterations"]))
     e1.record()
-    torch.cuda.synchronize()
-    t_seq = e0.elapsed_time(e1) * 1e-3
+    barrier(world)
+    t_seq = allreduce_max(e0.elapsed_time(e1) * 1e-3, world)
+    dofits_seq = allreduce_sum(float((sizes * its_s).sum()), world)
+    sizes_all = np.array([len(d[0]) for d in all_doms])
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     line = {"metric": "ensemble DOF*Picard-iter/s (batched domains, one launch per step)",
-            "value": dofits / t_batch, "unit": "DOF*Picard-iter/s", "n_gpus": 1, "steps": args.steps,
+            "value": dofits / t_batch, "unit": "DOF*Picard-iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
             "data": f"synthetic (seed {args.seed})",
             "config": {"workload": f"{len(doms)} independent 2D Richards domains, sides uniform in "
                                    "{32,...,256}, VG alpha/n/Ks log-uniform, theta_r .05, theta_s .40, "
                                    "h0 -1, top Dirichlet -0.1, dt0 1e-4 adaptive per domain",
-                       "nodes_total": int(sizes.sum()), "domains": len(doms)},
-            "batched": {"seconds": t_batch, "picard_its": int(its_b.sum()), "block_threads": tuned,
+                       "nodes_total": int(sizes_all.sum()), "domains": len(all_doms),
+                       "parallelism": f"domains sharded over {world} rank(s), nnz-balanced" if world > 1
+                       else "single GPU"},
+            "scaling": "strong",
+            "batched": {"seconds": t_batch, "picard_its": int(its_all.sum()), "block_threads": tuned,
                         "autotune_ms": getattr(ens, "timing", {})},
-            "sequential": {"seconds": t_seq, "picard_its": int(its_s.sum()),
-                           "value": float((sizes * its_s).sum()) / t_seq},
-            "speedup_vs_sequential": t_seq / t_batch * (dofits / max(1, int((sizes * its_s).sum())))}
+            "sequential": {"seconds": t_seq, "value": dofits_seq / t_seq},
+            "speedup_vs_sequential": (dofits / t_batch) / (dofits_seq / t_seq)}
     print(json.dumps(line))
 
 

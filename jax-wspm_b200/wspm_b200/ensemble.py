@@ -26,6 +26,37 @@ from .engine import default_rule
 BLOCK_SIZES = (128, 256, 512)
 
 
+def partition_domains(work, world):
+    """Split domain ids over `world` ranks, balancing the summed work (e.g. nnz): largest first, each to the
+    least-loaded rank (ties: lowest rank).  Deterministic; every domain goes to exactly one rank."""
+    work = np.asarray(work, dtype=np.float64)
+    load = np.zeros(int(world))
+    parts = [[] for _ in range(int(world))]
+    for d in np.argsort(-work, kind="stable"):
+        r = int(np.argmin(load))
+        parts[r].append(int(d))
+        load[r] += work[d]
+    return [np.array(sorted(p), dtype=np.int64) for p in parts]
+
+
+def gather_domain_results(local_ids, local_values, n_domains, world):
+    """Rank 0 receives every rank's (ids, values) once, at the end of a run (host objects over the process
+    group); returns the values in domain order on rank 0, None elsewhere."""
+    if world == 1:
+        out = np.zeros(n_domains, dtype=np.asarray(local_values).dtype)
+        out[np.asarray(local_ids)] = local_values
+        return out
+    import torch.distributed as dist
+    got = [None] * world
+    dist.all_gather_object(got, (np.asarray(local_ids).tolist(), np.asarray(local_values).tolist()))
+    if dist.get_rank() != 0:
+        return None
+    out = np.zeros(n_domains, dtype=np.asarray(local_values).dtype)
+    for ids, vals in got:
+        out[np.asarray(ids, dtype=np.int64)] = vals
+    return out
+
+
 class Ensemble:
     """Independent domains d = 0..D-1, each ``(points, triangles, phi[6], bc_val or None, Ks_elem or None)``."""
 
