@@ -20,6 +20,19 @@ published algorithms with JAX's documented stopping semantics:
 
 Jacobi: ``Preconditioner.create_jacobi`` (jax_linear_solver.py:11-36):
 ``M x = x / d`` with d = diag(A), zeros replaced by 1.
+
+The reference's other preconditioners, restated from what their code computes
+(``reference_preconditioner``; d = diag(A), L / U = strict lower / upper parts):
+* ``ilu`` (create_ilu0, jax_linear_solver.py:171-252): L scaled by 1/d of its
+  column, U unscaled, no pivot update -- M = (D + L) D^-1 (D' + U) with
+  D' = D with zeros replaced by 1, i.e. symmetric Gauss-Seidel, not a true ILU(0);
+* ``ssor`` (create_ssor, :91-169): forward sweep y = (D/omega + L)^-1 x; the
+  backward sweep reads entries of z that are not computed yet (zeros), so it
+  returns z = omega y;
+* ``block_jacobi`` (create_block_jacobi, :38-89): inverses of the diagonal
+  blocks of size block_size (last block smaller), each + 1e-12 I before inversion.
+The solvers take either a Jacobi diagonal (``dinv`` array) or any such
+callable; with any preconditioner CG tests r.r (JAX's rule for M != identity).
 """
 import numpy as np
 
@@ -30,6 +43,8 @@ def jacobi_inverse_diagonal(A):
 
 
 def _precond(dinv):
+    if callable(dinv):
+        return dinv
     if dinv is None:
         return lambda v: v
     return lambda v: dinv * v
@@ -159,22 +174,62 @@ def gmres(A, b, x0, tol=1e-10, atol=0.0, restart=30, maxiter=100, dinv=None):
     return x, k
 
 
+def reference_preconditioner(A, precond_type, omega=1.0, block_size=2):
+    """Callable M(v) of the reference's preconditioner of A (see the module docstring)."""
+    import scipy.sparse as sp
+    from scipy.sparse.linalg import spsolve_triangular
+    A = sp.csr_matrix(A)
+    n = A.shape[0]
+    d = A.diagonal().astype(np.float64)
+    if precond_type == "jacobi":
+        dinv = jacobi_inverse_diagonal(A)
+        return lambda v: dinv * v
+    if precond_type == "ilu":
+        dz = np.where(d == 0, 1.0, d)
+        L = sp.tril(A, -1).tocsr() @ sp.diags(1.0 / dz)
+        Lw = (L + sp.identity(n)).tocsr()
+        Uw = (sp.triu(A, 1) + sp.diags(dz)).tocsr()
+        return lambda v: spsolve_triangular(Uw, spsolve_triangular(Lw, v, lower=True, unit_diagonal=True),
+                                            lower=False)
+    if precond_type == "ssor":
+        Lw = (sp.tril(A, -1) + sp.diags(d / omega)).tocsr()
+        return lambda v: omega * spsolve_triangular(Lw, v, lower=True)
+    if precond_type == "block_jacobi":
+        Ad = A.toarray() if n <= 4096 else None
+        invs = []
+        for s0 in range(0, n, block_size):
+            s1 = min(s0 + block_size, n)
+            blk = (Ad[s0:s1, s0:s1] if Ad is not None else A[s0:s1, s0:s1].toarray()) + 1e-12 * np.eye(s1 - s0)
+            invs.append((s0, s1, np.linalg.inv(blk)))
+
+        def apply(v):
+            out = np.empty_like(v)
+            for s0, s1, inv in invs:
+                out[s0:s1] = inv @ v[s0:s1]
+            return out
+        return apply
+    raise ValueError(f"unknown preconditioner {precond_type!r}")
+
+
 def solve_system(A, b, x0, solver_type="gmres", precond_type="none", tol=1e-10,
-                 maxiter=100, restart=30):
-    """Dispatch of src/solvers/solver_types.py:7-67 (Jacobi or no preconditioner).
+                 maxiter=100, restart=30, omega=1.0, block_size=2):
+    """Dispatch of src/solvers/solver_types.py:7-67 with the reference's preconditioners.
 
     Returns (x, iterations).  ``direct`` solves exactly (the reference densifies
     and calls jnp.linalg.solve; a sparse LU gives the same solution).
     """
-    if precond_type not in ("none", None, "jacobi"):
-        raise NotImplementedError(f"oracle preconditioner {precond_type!r}")
-    dinv = jacobi_inverse_diagonal(A) if precond_type == "jacobi" else None
+    if precond_type in ("none", None):
+        M = None
+    elif precond_type == "jacobi":
+        M = jacobi_inverse_diagonal(A)
+    else:
+        M = reference_preconditioner(A, precond_type, omega=omega, block_size=block_size)
     if solver_type == "cg":
-        return cg(A, b, x0, tol=tol, maxiter=maxiter, dinv=dinv)
+        return cg(A, b, x0, tol=tol, maxiter=maxiter, dinv=M)
     if solver_type == "bicgstab":
-        return bicgstab(A, b, x0, tol=tol, maxiter=maxiter, dinv=dinv)
+        return bicgstab(A, b, x0, tol=tol, maxiter=maxiter, dinv=M)
     if solver_type == "gmres":
-        return gmres(A, b, x0, tol=tol, restart=restart, maxiter=maxiter, dinv=dinv)
+        return gmres(A, b, x0, tol=tol, restart=restart, maxiter=maxiter, dinv=M)
     if solver_type == "direct":
         import scipy.sparse.linalg as spla
         return spla.spsolve(A.tocsc(), b), 0

@@ -20,7 +20,7 @@ ROWS = json.load(open(os.path.join(GOLD, "re2d_metrics.json")))
 UNPINNED = {("Test1", 50, "bicgstab", "none")}
 
 
-def golden_rows(meshes, solvers=("cg", "bicgstab", "gmres", "direct"), preconds=("none", "jacobi")):
+def golden_rows(meshes, solvers=("cg", "bicgstab", "gmres", "direct"), preconds=("none", "jacobi", "ilu")):
     seen, out = set(), []
     for r in ROWS:
         key = (r["test_case"], r["mesh"], r["solver"], r["precond"])
