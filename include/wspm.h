@@ -47,6 +47,9 @@ extern "C" {
 #define WSPM_SOLVER_GMRES     2
 #define WSPM_PRECOND_NONE     0
 #define WSPM_PRECOND_JACOBI   1
+#define WSPM_PRECOND_ILU      2   /* the reference's create_ilu0 (symmetric Gauss-Seidel form) */
+#define WSPM_PRECOND_SSOR     3   /* the reference's create_ssor: omega (D/omega + L)^-1        */
+#define WSPM_PRECOND_BLOCK_JACOBI 4
 #define WSPM_SOIL_VAN_GENUCHTEN 0
 #define WSPM_SOIL_EXPONENTIAL   1
 
@@ -370,6 +373,27 @@ int wspm_elem_param_grad(const wspm_mesh *mesh, const wspm_pattern *pat, const d
                          double theta_s, const double *quad_points, const double *weights, int32_t nq, double dt,
                          const double *bc_val, const double *h, const double *h_old, const double *lam,
                          const double *wl, const double *mass, double *grad, void *stream);
+
+/* ---- the reference's other preconditioners ---------------------------------
+ * Preconditioner.create_ilu0 / create_ssor / create_block_jacobi,
+ * src/solvers/jax_linear_solver.py:38-252, as their code computes them
+ * (d = diag(A), L / U = strict lower / upper parts of A):
+ *   WSPM_PRECOND_ILU:  y = (D' + U)^-1 (I + L D'^-1)^-1 x, D' = D with zeros -> 1;
+ *   WSPM_PRECOND_SSOR: y = omega (D/omega + L)^-1 x;
+ *   WSPM_PRECOND_BLOCK_JACOBI: y = blockdiag((A_bb + 1e-12 I)^-1) x, blocks of block_size (1 or 2).
+ * The triangular sweeps run level by level: rows of one level depend only on
+ * rows of earlier levels (lower: columns j < i, upper: j > i), listed by
+ * wspm_levels (built on the host from the pattern).  One CTA walks the levels,
+ * so a sweep costs one block barrier per level.  tmp: n_rows doubles.        */
+typedef struct wspm_levels {
+    int32_t n_levels;
+    const int32_t *level_ptr;  /* [n_levels + 1] offsets into rows           */
+    const int32_t *rows;       /* [n_rows] row ids grouped by level          */
+} wspm_levels;
+
+int wspm_precond_apply(const wspm_pattern *pat, const double *vals, int32_t kind, double omega,
+                       int32_t block_size, const wspm_levels *lower, const wspm_levels *upper, const double *x,
+                       double *y, double *tmp, void *stream);
 
 /* ---- misc ------------------------------------------------------------------ */
 const char *wspm_version(void);

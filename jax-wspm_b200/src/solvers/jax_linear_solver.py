@@ -1,17 +1,20 @@
 """Preconditioners and Krylov solvers (drop-in for src/solvers/jax_linear_solver.py:8-329).
 
-Same class and method names.  The solves run as CUDA graphs in libwspm.so
-(``wspm_krylov_solve``): the whole Krylov loop, including its convergence
-test, stays on the device.  Jacobi is the only preconditioner of the hot
-path; ``block_jacobi``, ``ssor`` and ``ilu`` raise NotImplementedError (the
-reference builds them with sequential scans over the nonzeros, see
-jax_linear_solver.py:38-252; they are the next items to port).
+Same class and method names.  With no preconditioner or Jacobi the solves
+run as CUDA graphs in libwspm.so (``wspm_krylov_solve``): the whole Krylov
+loop, including its convergence test, stays on the device.  ``ilu``, ``ssor``
+and ``block_jacobi`` are the reference's own operators as its code computes
+them (jax_linear_solver.py:38-252: ilu is the symmetric Gauss-Seidel form,
+ssor a scaled forward sweep), applied on the device with level-scheduled
+triangular sweeps (``wspm_b200.precond``); their Krylov loops are driven from
+the host.
 """
 from typing import Optional, Tuple
 
 import torch
 
 from wspm_b200 import context
+from wspm_b200 import precond as _pre
 from wspm_b200.device import KrylovWorkspace, SparseMatrix, jacobi_dinv, krylov_solve
 
 
@@ -27,21 +30,19 @@ class Preconditioner:
         return fn
 
     @staticmethod
-    def _unsupported(name):
-        raise NotImplementedError(f"preconditioner {name!r} is not implemented on the GPU path "
-                                  "(supported: 'none', 'jacobi')")
-
-    @staticmethod
     def create_block_jacobi(A, block_size: int = 2):
-        Preconditioner._unsupported("block_jacobi")
+        """Inverses of the diagonal blocks (+ 1e-12 I), jax_linear_solver.py:38-89."""
+        return _pre.ReferencePreconditioner(A.dmesh, A.vals, "block_jacobi", block_size=block_size)
 
     @staticmethod
     def create_ssor(A, omega: float = 1.0):
-        Preconditioner._unsupported("ssor")
+        """omega (D/omega + L)^-1, what jax_linear_solver.py:91-169 computes."""
+        return _pre.ReferencePreconditioner(A.dmesh, A.vals, "ssor", omega=omega)
 
     @staticmethod
     def create_ilu0(A):
-        Preconditioner._unsupported("ilu")
+        """(D' + U)^-1 (I + L D'^-1)^-1, what jax_linear_solver.py:171-252 computes."""
+        return _pre.ReferencePreconditioner(A.dmesh, A.vals, "ilu")
 
 
 def _workspace(A):
@@ -65,12 +66,6 @@ class JAXSparseSolver:
             return None
         if precond_type == "jacobi":
             return Preconditioner.create_jacobi(self.A).dinv
-        if precond_type == "block_jacobi":
-            return Preconditioner.create_block_jacobi(self.A, kw.get("block_size", 2))
-        if precond_type == "ssor":
-            return Preconditioner.create_ssor(self.A, kw.get("omega", 1.0))
-        if precond_type == "ilu":
-            return Preconditioner.create_ilu0(self.A)
         raise ValueError(f"Unsupported preconditioner: {precond_type}")
 
     def _solve(self, solver, b, x0, tol, atol, maxiter, restart, precond_type, **kw):
@@ -78,6 +73,12 @@ class JAXSparseSolver:
         x0 = b.new_zeros(b.shape) if x0 is None else context.as_cuda_f64(x0)
         if maxiter is None:
             maxiter = 10 * b.numel()
+        if precond_type in ("ilu", "ssor", "block_jacobi"):
+            x, k = _pre.solve(self.A.dmesh, self.A.vals, b, x0, solver, precond_type, tol=tol, atol=atol,
+                              maxiter=maxiter, restart=restart, omega=kw.get("omega", 1.0),
+                              block_size=kw.get("block_size", 2))
+            status = 3 if k < 0 else (1 if k >= maxiter else 0)
+            return x, torch.tensor([status, max(k, 0), 0, 0], dtype=torch.int32, device=b.device)
         x, res = krylov_solve(self.A.dmesh, self.A.vals, b, x0, solver=solver, dinv=self._dinv(precond_type, **kw),
                               tol=tol, atol=atol, maxiter=maxiter, restart=restart, workspace=_workspace(self.A))
         return x, res

@@ -68,8 +68,15 @@ class WspmEnsemble(ctypes.Structure):
                 ("queue", c_void_p)]
 
 
+class WspmLevels(ctypes.Structure):
+    _fields_ = [("n_levels", c_int32), ("level_ptr", c_void_p), ("rows", c_void_p)]
+
+
+PRECOND_KIND = {"ilu": 2, "ssor": 3, "block_jacobi": 4}
 P = ctypes.POINTER
 _SIGS = {
+    "wspm_precond_apply": (c_int32, [P(WspmPattern), c_void_p, c_int32, c_double, c_int32, P(WspmLevels),
+                                     P(WspmLevels), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_ensemble_workspace_doubles": (c_int64, [c_int32, c_int64]),
     "wspm_elem_assemble_richards": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_double, c_double,
                                               P(c_double), P(c_double), c_int32, c_double, c_void_p, c_void_p,

@@ -134,6 +134,27 @@ class Pattern:
         inc_s[islot] = packed
         self.inc_elem, self.inc_slots = inc_e, inc_s
 
+    def tri_levels(self, lower=True):
+        """Level schedule of a triangular sweep over this pattern: (level_ptr, rows), rows grouped so that row i
+        only depends on rows of earlier levels (lower: columns j < i, swept upwards; upper: j > i, downwards)."""
+        cache = self.__dict__.setdefault("_levels", {})
+        if lower in cache:
+            return cache[lower]
+        n, ptr, idx = self.n_rows, self.csr_indptr, self.csr_indices
+        level = np.zeros(n, dtype=np.int64)
+        order = range(n) if lower else range(n - 1, -1, -1)
+        for i in order:
+            c = idx[ptr[i]:ptr[i + 1]]
+            dep = c[c < i] if lower else c[c > i]
+            if dep.size:
+                level[i] = level[dep].max() + 1
+        rows = np.argsort(level, kind="stable").astype(np.int32)
+        counts = np.bincount(level, minlength=int(level.max()) + 1 if n else 0)
+        level_ptr = np.zeros(counts.size + 1, dtype=np.int32)
+        np.cumsum(counts, out=level_ptr[1:])
+        cache[lower] = (level_ptr, rows)
+        return cache[lower]
+
     def slot(self, i, j):
         """Row position k of column j in row i (i, j arrays)."""
         return np.asarray(self._slot(np.asarray(i, dtype=np.int64), np.asarray(j, dtype=np.int64)))
