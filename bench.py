@@ -502,6 +502,71 @@ def adjoint_measure(n, steps, seed, fd_params):
     return line
 
 
+def run_config2(args):
+    """3D Richards (Kuhn tetrahedra, BiCGSTAB + Jacobi) and a three-species transport chain on a 2D grid."""
+    import torch
+    from wspm_b200 import mesh
+    from wspm_b200.device import (DeviceMesh, apply_dirichlet, assemble_adr, flux_dispersion, jacobi_dinv,
+                                  krylov_solve, merge_dirichlet)
+    from wspm_b200.engine import PicardEngine, default_rule
+    torch.cuda.set_device(0)
+    # ---- 3D Richards: unit cube, n^3 hexahedra split in 6 tets, VG c0 soil, h0 -1, top face Dirichlet -0.1
+    n = args.n3d
+    pts, tets = mesh.kuhn_tetrahedra(n, 1.0)
+    top = np.where(np.abs(pts[:, 2] - 1.0) < 1e-12)[0]
+    dm3 = DeviceMesh(pts, tets)
+    eng = PicardEngine(dm3, "vg", VG_PHI_UNIT_KS, bc_val=merge_dirichlet(len(pts), [(top, -0.1)]),
+                       solver="bicgstab", precond="jacobi", krylov_tol=1e-8, krylov_maxiter=1000)
+    h0 = -np.ones(len(pts))
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    t3 = time_path(eng, h0, 1e-4, args.steps3d, args.warmup, 1, lambda: flush_buf.fill_(1.0))
+    # ---- transport chain on an m x m grid: species 1 -> 2 -> 3, first-order rates k1, k2, sorption on species 2,
+    # dispersivities 0.5 / 0.1, Dirichlet 1.0 for species 1 on the top edge, GMRES(30) + Jacobi
+    m = args.n_transport
+    p2, tri = mesh.structured_triangles(m, 1.0)
+    dm2 = DeviceMesh(p2, tri)
+    top2 = np.where(np.abs(p2[:, 1] - 1.0) < 1e-12)[0]
+    hh = torch.as_tensor(-0.5 - 0.5 * p2[:, 1], dtype=torch.float64, device="cuda")
+    Q, W = default_rule(2)
+    c = [torch.zeros(len(p2), dtype=torch.float64, device="cuda") for _ in range(3)]
+    k1, k2, sorption = 0.36, 0.2, 1.5 * 3.5
+
+    def transport_step():
+        qx, qz, aq, Dxx, Dxz, Dzz, th = flux_dispersion(dm2, hh, VG_PHI_UNIT_KS, 0.5, 0.1, 0.0)
+        up = None
+        for s_, (mu, sorp, mu_up) in enumerate(((k1, 0.0, 0.0), (k2, sorption, k1), (0.0, 0.0, k2))):
+            vals, rhs, dinv = assemble_adr(dm2, th, qx, qz, Dxx, Dxz, Dzz, c[s_], 1e-3, Q, W, mu=mu, sorption=sorp,
+                                           mu_up=mu_up, c_up=up, lumped=True)
+            if s_ == 0:
+                apply_dirichlet(dm2, top2, np.ones(top2.size), vals, rhs)
+            c[s_], _ = krylov_solve(dm2, vals, rhs, c[s_], "gmres", dinv=jacobi_dinv(dm2, vals), tol=1e-10,
+                                    maxiter=100, restart=30)
+            up = c[s_]
+    for _ in range(args.warmup):
+        transport_step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps3d):
+        transport_step()
+    e1.record()
+    torch.cuda.synchronize()
+    t_tr = e0.elapsed_time(e1) / args.steps3d
+    line = {"metric": "3D Richards DOF*Picard-iter/s (FP64, BiCGSTAB + Jacobi) and transport-chain step time",
+            "value": len(pts) * t3["picard_its"] / (t3["ms"] * 1e-3), "unit": "DOF*Picard-iter/s", "n_gpus": 1,
+            "steps": args.steps3d, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": f"{n}^3 unit cube, Kuhn split (6 tets per hexahedron), VG "
+                                                        "c0 soil, h0 -1, top face Dirichlet -0.1, dt 1e-4 fixed",
+                                            "nodes": len(pts), "elements": len(tets), "nnz": int(dm3.pattern.nnz)},
+            "richards3d": {"ms_per_step": t3["ms"] / args.steps3d, "picard_its": t3["picard_its"],
+                           "krylov_its": t3["krylov_its"]},
+            "transport": {"workload": f"{m}^2 triangles, 3 species first-order chain (0.36, 0.2 /day), sorption "
+                                      "rho_b Kd = 5.25 on species 2, dispersivity 0.5 / 0.1, Dirichlet 1.0 inflow of "
+                                      "species 1 on the top edge, lumped mass, GMRES(30) + Jacobi, dt 1e-3",
+                          "nodes": len(p2), "ms_per_step": t_tr}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -528,6 +593,11 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--fd-params", type=int, default=32)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement of the main line")
+    ap.add_argument("--config2", action="store_true",
+                    help="3D Richards on Kuhn tetrahedra and a three-species transport chain; own JSON line")
+    ap.add_argument("--n3d", type=int, default=96)
+    ap.add_argument("--steps3d", type=int, default=5)
+    ap.add_argument("--n-transport", type=int, default=512)
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Picard/Krylov loops from the host (same kernels; for ncu, which cannot "
                          "profile kernels inside conditional graphs)")
@@ -540,6 +610,8 @@ def main():
         return run_ensemble(args)
     if args.adjoint:
         return run_adjoint(args)
+    if args.config2:
+        return run_config2(args)
 
     import torch
     from wspm_b200.device import DeviceMesh, merge_dirichlet

@@ -395,6 +395,17 @@ int wspm_precond_apply(const wspm_pattern *pat, const double *vals, int32_t kind
                        int32_t block_size, const wspm_levels *lower, const wspm_levels *upper, const double *x,
                        double *y, double *tmp, void *stream);
 
+/* ---- mass balance and transport stability numbers (2D) ---------------------
+ * integrate_2d_domain, src/solvers/.ipynb_checkpoints/richards_mass_balance-checkpoint.py:25-69
+ * (3-point rule, weights 1/3 times |det J|: twice the integral, as the
+ * reference); calculate_peclet_courant, src/models/transport_utilities.py:193-242.
+ * Results land in device memory (out: 1 double; out2: Pe, Cr); work holds
+ * wspm_balance_workspace_doubles() doubles.  Fixed-order reductions.           */
+int64_t wspm_balance_workspace_doubles(void);
+int wspm_integrate_2d(const wspm_mesh *mesh, const double *f, double *out, double *work, void *stream);
+int wspm_peclet_courant(const wspm_mesh *mesh, const double *qx, const double *qz, const double *theta,
+                        const double *Dxx, const double *Dzz, double dt, double *out2, double *work, void *stream);
+
 /* ---- misc ------------------------------------------------------------------ */
 const char *wspm_version(void);
 const char *wspm_status_string(int status);

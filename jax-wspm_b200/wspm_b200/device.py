@@ -310,3 +310,23 @@ def assemble_adr(dm, theta, qx, qz, Dxx, Dxz, Dzz, c_n, dt, quad_points, weights
         dptr(Dzz), dptr(c_n), dptr(c_up), float(mu), float(sorption), float(mu_up), int(bool(lumped)),
         _lib.dbl_array(q), _lib.dbl_array(w), len(w), float(dt), dptr(vals), dptr(rhs), dptr(dinv), _stream()))
     return vals, rhs, dinv
+
+
+# ---------------------------------------------------------------- mass balance, Peclet / Courant
+def integrate_2d(dm, f):
+    """The reference's integrate_2d_domain of a nodal field (device scalar tensor)."""
+    _require_cuda(f, torch.float64, "f", dm.n_nodes)
+    work = torch.empty(int(lib.wspm_balance_workspace_doubles()), dtype=torch.float64, device=dm.device)
+    out = torch.empty(1, dtype=torch.float64, device=dm.device)
+    check("integrate_2d", lib.wspm_integrate_2d(ctypes.byref(dm.c_mesh), dptr(f), dptr(out), dptr(work), _stream()))
+    return out[0]
+
+
+def peclet_courant(dm, qx, qz, theta, Dxx, Dzz, dt):
+    """(Pe, Cr) maxima over the mesh (transport_utilities.py:193-242), device tensor [2]."""
+    work = torch.empty(int(lib.wspm_balance_workspace_doubles()), dtype=torch.float64, device=dm.device)
+    out = torch.empty(2, dtype=torch.float64, device=dm.device)
+    check("peclet_courant", lib.wspm_peclet_courant(ctypes.byref(dm.c_mesh), dptr(qx), dptr(qz), dptr(theta),
+                                                    dptr(Dxx), dptr(Dzz), float(dt), dptr(out), dptr(work),
+                                                    _stream()))
+    return out

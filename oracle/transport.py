@@ -240,3 +240,37 @@ def nitrogen_species_step(points, tri, c_n, theta, qx, qz, Dxx, Dxz, Dzz, K_node
     A = ((1.0 / dt) * Ml + K).tocsr()
     c, _ = solve_system(A, b, c_n, solver, precond, tol=tol, maxiter=maxiter, restart=restart)
     return c
+
+
+# ------------------------------------------------------------------ mass balance, Peclet / Courant
+def integrate_2d_domain(f, points, triangles):
+    """richards_mass_balance-checkpoint.py:25-69: sum_e |det J| sum_q (1/3) f(x_q) (twice the integral)."""
+    t = np.asarray(triangles)
+    P = np.asarray(points)
+    J00 = P[t[:, 1], 0] - P[t[:, 0], 0]
+    J01 = P[t[:, 2], 0] - P[t[:, 0], 0]
+    J10 = P[t[:, 1], 1] - P[t[:, 0], 1]
+    J11 = P[t[:, 2], 1] - P[t[:, 0], 1]
+    det = np.abs(J00 * J11 - J01 * J10)
+    fl = np.asarray(f)[t]
+    total = np.zeros(len(t))
+    for a, b in ((1 / 6, 1 / 6), (2 / 3, 1 / 6), (1 / 6, 2 / 3)):
+        total += (1 / 3) * (fl[:, 0] * (1 - a - b) + fl[:, 1] * a + fl[:, 2] * b)
+    return float(np.sum(total * det))
+
+
+def element_size(points, triangles):
+    """transport_utilities.py:196-203: shortest edge per triangle."""
+    v = np.asarray(points)[np.asarray(triangles)]
+    e = v - np.roll(v, 1, axis=1)
+    return np.min(np.sqrt(np.sum(e ** 2, axis=2)), axis=1)
+
+
+def peclet_courant(points, triangles, qx, qz, theta, Dxx, Dzz, dt):
+    """transport_utilities.py:205-242: max over elements and nodes of |v| h / (2D) and |v| dt / h."""
+    t = np.asarray(triangles)
+    h = element_size(points, triangles)[:, None]
+    vx, vz = np.abs(qx[t] / theta[t]), np.abs(qz[t] / theta[t])
+    pe = np.maximum(vx * h / (2 * Dxx[t]), vz * h / (2 * Dzz[t])).max()
+    cr = np.maximum(vx * dt / h, vz * dt / h).max()
+    return float(pe), float(cr)

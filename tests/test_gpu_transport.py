@@ -268,3 +268,16 @@ def test_nitrogen_solver_matches_oracle_driver():
         np.testing.assert_allclose(res["pressure_head"][s], h, rtol=1e-9, atol=1e-10)
         for key, c in (("NH4_concentration", nh4), ("NO2_concentration", no2), ("NO3_concentration", no3)):
             np.testing.assert_allclose(res[key][s], c, rtol=1e-8, atol=1e-8 * max(1.0, np.abs(c).max()))
+
+
+def test_mass_integral_and_peclet_courant_match_oracle():
+    from src.models.transport_utilities import calculate_peclet_courant
+    from src.utils.mass_balance import integrate_2d_domain
+    pts, tri, h = field(seed=8)
+    th = osoil.van_genuchten_model(h, VG_SOLUTE)[2]
+    assert abs(integrate_2d_domain(th, pts, tri) - otr.integrate_2d_domain(th, pts, tri)) <= 1e-13 * abs(
+        otr.integrate_2d_domain(th, pts, tri))
+    qx, qz, aq, Dxx, Dxz, Dzz, th = otr.fluxes_and_dispersion(pts, tri, h, VG_SOLUTE, 0.5, 0.1, 0.0288)
+    got = calculate_peclet_courant(pts, tri, qx, qz, th, Dxx, Dzz, 1e-3)
+    want = otr.peclet_courant(pts, tri, qx, qz, th, Dxx, Dzz, 1e-3)
+    np.testing.assert_allclose(got, want, rtol=1e-13)
