@@ -19,11 +19,23 @@ constexpr int kSlice = 32;          // SELL slice height == warp size
 constexpr int kBlock = 256;         // threads per block for vector kernels
 constexpr int kMaxPartials = 16384; // partial-sum slots: one block per 256 rows up to 4M rows
 
-// One thread per row (or element) up to kMaxPartials blocks, grid-stride beyond.
+// Grid of a reducing kernel: one thread per row (or element) up to 8 blocks
+// per SM, grid-stride beyond.  Every block publishes one partial through an
+// atomic ticket on a single word, so the cap bounds that serialised tail
+// (4,000+ blocks at 10^6 rows would queue 4,000+ atomics); the grid stays a
+// fixed function of n, so the summation order is fixed.
 inline int reduction_blocks(int64_t n) {
+    static int cap = 0;
+    if (cap == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cap = sms > 0 ? 8 * sms : 1024;
+        if (cap > kMaxPartials) cap = kMaxPartials;
+    }
     int64_t b = (n + kBlock - 1) / kBlock;
     if (b < 1) b = 1;
-    if (b > kMaxPartials) b = kMaxPartials;
+    if (b > cap) b = cap;
     return (int)b;
 }
 
