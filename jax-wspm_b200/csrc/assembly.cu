@@ -45,6 +45,7 @@ struct RichardsAsmArgs {
     const int32_t *conn;
     const double *coords;
     const double *theta_m, *theta_n, *h_m, *K, *C, *Ks_elem, *bc_val;
+    const double *Ks_inc;    // per-element factor in incidence order (pad marker on padding slots)
     double s[4];       // K-average weights per vertex
     double mcoef[4];   // lumped-mass coefficients per vertex
     double inv_dt;
@@ -151,26 +152,59 @@ __device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM],
     }
 }
 
-// Row kernel.  Every vertex of an element incident to node i is a column of row
-// i, and the incidence word records, per element vertex, its position in the
-// row.  So the kernel first gathers the coordinates and K of the row's columns
-// (all loads in flight together, into shared memory), and the element loop
-// then reads each vertex from there: two dependent memory round trips per row
-// (incidence words; column data and per-element Ks) instead of walking
-// element id -> connectivity -> vertex data per element.  Vertex order inside
-// each element and the element order are unchanged, so every value and the
-// accumulation order are those of the element-walking form.
-template <int DIM, int MW>
-__global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
-    constexpr int NV = DIM + 1;
-    const int TB = blockDim.x;
-    extern __shared__ double acc_sm[];   // [MW][TB] accumulators, then [MW][NV][TB] column data
-    __shared__ int s_off[MW];
+// Incidence-ordered per-element values: slot o of the incidence layout gets
+// elem[inc_elem[o]]; padding slots get kIncPad, a NaN bit pattern that the
+// row kernel tests for (so it needs no element id per slot).
+constexpr long long kIncPad = (long long)0xFFF0DEAD00000000ULL;
+
+__global__ void incidence_gather_kernel(int n_slices, const int64_t *__restrict__ inc_ptr,
+                                        const int32_t *__restrict__ inc_width, const int32_t *__restrict__ inc_elem,
+                                        const double *__restrict__ elem, double *out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = i >> 5, lane = i & 31;
+    if (s >= n_slices) return;
+    const int64_t ib = inc_ptr[s] + lane;
+    const int w = inc_width[s];
+    for (int k = 0; k < w; ++k) {
+        const int64_t o = ib + (int64_t)kSlice * k;
+        const int e = inc_elem[o];
+        out[o] = e >= 0 ? elem[e] : __longlong_as_double(kIncPad);
+    }
+}
+
+// Row kernel.  Every vertex of an element incident to node i is a column of
+// row i, and the incidence word records, per element vertex, its position in
+// the row.  Thread i walks the incident elements in ascending id, computes
+// row "local vertex of i" of each element matrix in registers and accumulates
+// into the row's slots in shared memory; vertex order inside each element and
+// the element order are those of the element-walking form, so every value and
+// every accumulation order are unchanged.
+//
+// Column data (coordinates, K) come either from a shared-memory stage filled
+// once per row with all loads in flight (STAGE; two dependent memory round
+// trips per row), or, for DIA patterns, straight from global memory per
+// element at column i + off[position] (L1-resident: the row's columns are the
+// neighbouring rows' columns too).  2D takes the stage; 3D (15 columns x 4
+// values would hold occupancy to two blocks per SM) takes the direct reads.
+//
+// KSM selects the per-element conductivity factor: 0 none, 1 gathered by
+// element id, 2 read in incidence order (Ks_inc, built once per time step by
+// incidence_gather_kernel: one coalesced load per slot, no dependent gather,
+// and its pad marker replaces the element-id read).
+//
+// The element-local row index li selects a column of G by selects: an indexed
+// register array would live in local memory.
+template <int DIM, int MW, int KSM, bool STAGE, int TB, int MINB>
+__global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs a) {
+    constexpr int NV = DIM + 1;
+    constexpr int CH = STAGE ? 4 : 1;   // incidences whose loads are issued together
+    extern __shared__ double acc_sm[];  // [MW][TB] accumulators, then [MW][NV][TB] column data (STAGE)
+    __shared__ int s_off[MW];
+    const int i = blockIdx.x * TB + threadIdx.x;
     const int s = i >> 5, lane = i & 31;
     const bool dia = a.n_diags > 0;
     if (dia)
-        for (int k = threadIdx.x; k < a.n_diags; k += blockDim.x) s_off[k] = a.diag_off[k];
+        for (int k = threadIdx.x; k < a.n_diags; k += TB) s_off[k] = a.diag_off[k];
     __syncthreads();
     if (s >= ((a.n_rows + kSlice - 1) >> 5)) return;
     const int width = dia ? a.n_diags : a.slice_width[s];
@@ -203,77 +237,96 @@ __global__ void __launch_bounds__(128) richards_rows_kernel(RichardsAsmArgs a) {
         const double storage = tm - tn - Ci * hi;
         const int deg = a.inc_width[s];
         const int64_t ib = a.inc_ptr[s] + lane;
-        // column data of the row: coordinates and K, CG columns per batch of loads in flight
-        constexpr int CG = DIM == 2 ? 8 : 4;
-        const int last = a.n_rows - 1;
+        if constexpr (STAGE) {
+            // column data of the row: coordinates and K, CG columns per batch of loads in flight
+            constexpr int CG = DIM == 2 ? 8 : 4;
+            const int last = a.n_rows - 1;
 #pragma unroll
-        for (int k0 = 0; k0 < MW; k0 += CG) {
-            if (k0 >= width) break;
-            double xv[CG][DIM], kv[CG];
+            for (int k0 = 0; k0 < MW; k0 += CG) {
+                if (k0 >= width) break;
+                double xv[CG][DIM], kv[CG];
 #pragma unroll
-            for (int g = 0; g < CG; ++g) {
-                const int k = k0 + g;
-                if (k < width) {
-                    int c = dia ? i + s_off[k] : __ldg(a.cols + vb + kstride * k);
-                    c = c < 0 ? 0 : (c > last ? last : c);
+                for (int g = 0; g < CG; ++g) {
+                    const int k = k0 + g;
+                    if (k < width) {
+                        int c = dia ? i + s_off[k] : __ldg(a.cols + vb + kstride * k);
+                        c = c < 0 ? 0 : (c > last ? last : c);
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) xv[g][d] = __ldg(a.coords + (int64_t)DIM * c + d);
-                    kv[g] = __ldg(a.K + c);
+                        for (int d = 0; d < DIM; ++d) xv[g][d] = __ldg(a.coords + (int64_t)DIM * c + d);
+                        kv[g] = __ldg(a.K + c);
+                    }
                 }
-            }
 #pragma unroll
-            for (int g = 0; g < CG; ++g) {
-                const int k = k0 + g;
-                if (k < width) {
+                for (int g = 0; g < CG; ++g) {
+                    const int k = k0 + g;
+                    if (k < width) {
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) colv[(k * NV + d) * TB] = xv[g][d];
-                    colv[(k * NV + DIM) * TB] = kv[g];
+                        for (int d = 0; d < DIM; ++d) colv[(k * NV + d) * TB] = xv[g][d];
+                        colv[(k * NV + DIM) * TB] = kv[g];
+                    }
                 }
             }
         }
         double bsum = 0.0;
-        // incidences in chunks of CH: ids and slot words, then the per-element Ks, then the math
-        constexpr int CH = 4;
 #pragma unroll 1
         for (int k0 = 0; k0 < deg; k0 += CH) {
             uint32_t pk[CH];
-            int ev[CH];
+            bool ok[CH];
             double kse[CH];
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
                 pk[c] = 0u;
-                ev[c] = -1;
+                ok[c] = false;
+                kse[c] = 1.0;
                 if (k0 + c < deg) {
-                    pk[c] = __ldg(a.inc_slots + ib + (int64_t)kSlice * (k0 + c));
-                    ev[c] = __ldg(a.inc_elem + ib + (int64_t)kSlice * (k0 + c));   // -1: padding of the slice
+                    const int64_t o = ib + (int64_t)kSlice * (k0 + c);
+                    pk[c] = __ldg(a.inc_slots + o);
+                    if constexpr (KSM == 2) {
+                        kse[c] = __ldg(a.Ks_inc + o);
+                        ok[c] = __double_as_longlong(kse[c]) != kIncPad;
+                    } else {
+                        const int ev = __ldg(a.inc_elem + o);   // -1: padding of the slice
+                        ok[c] = ev >= 0;
+                        if (KSM == 1 && ev >= 0) kse[c] = __ldg(a.Ks_elem + ev);
+                    }
                 }
             }
 #pragma unroll
-            for (int c = 0; c < CH; ++c) kse[c] = (a.Ks_elem && ev[c] >= 0) ? __ldg(a.Ks_elem + ev[c]) : 1.0;
-#pragma unroll
             for (int c = 0; c < CH; ++c) {
-                if (ev[c] < 0) continue;
+                if (!ok[c]) continue;
                 const uint32_t packed = pk[c];
                 const int li = packed & 3;
                 double X[NV][DIM], Kv[NV];
 #pragma unroll
                 for (int j = 0; j < NV; ++j) {
                     const int kp = (packed >> (2 + 6 * j)) & 63;
+                    if constexpr (STAGE) {
 #pragma unroll
-                    for (int d = 0; d < DIM; ++d) X[j][d] = colv[(kp * NV + d) * TB];
-                    Kv[j] = colv[(kp * NV + DIM) * TB];
+                        for (int d = 0; d < DIM; ++d) X[j][d] = colv[(kp * NV + d) * TB];
+                        Kv[j] = colv[(kp * NV + DIM) * TB];
+                    } else {
+                        const int col = i + s_off[kp];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) X[j][d] = __ldg(a.coords + (int64_t)DIM * col + d);
+                        Kv[j] = __ldg(a.K + col);
+                    }
                 }
                 double G[DIM][NV], detJ;
                 p1_geometry_xyz<DIM>(X, G, detJ);
                 double Kbar = 0.0;
 #pragma unroll
                 for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], Kv[j], Kbar);
-                if (a.Ks_elem) Kbar *= kse[c];
+                if constexpr (KSM != 0) Kbar *= kse[c];
                 const double kd = Kbar * detJ;
                 const double Ml = a.mcoef[li] * detJ;
                 double gli[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) gli[d] = G[d][li];
+                for (int d = 0; d < DIM; ++d) {
+                    double g = G[d][0];
+#pragma unroll
+                    for (int j = 1; j < NV; ++j) g = li == j ? G[d][j] : g;
+                    gli[d] = g;
+                }
 #pragma unroll
                 for (int j = 0; j < NV; ++j) {
                     double gg = 0.0;
@@ -321,18 +374,32 @@ void quadrature_constants(int dim, const double *Q, const double *W, int nq, dou
     }
 }
 
+template <int DIM, int MW, bool STAGE, int TB, int MINB>
+static void launch_rows(const RichardsAsmArgs &a, int ksm, int n_slices, cudaStream_t st) {
+    const int blocks = (n_slices * kSlice + TB - 1) / TB;
+    const size_t smem = (size_t)MW * TB * sizeof(double) * (STAGE ? 1 + (DIM + 1) : 1);
+    auto run = [&](auto kfn) {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kfn<<<blocks, TB, smem, st>>>(a);
+    };
+    if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB>);
+    else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB>);
+    else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB>);
+}
+
 static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_pattern *pat,
                                          const double *theta_m, const double *theta_n, const double *h_m,
                                          const double *K, const double *C, const double *Ks_elem,
-                                         const double s[4], const double mc[4], double dt, const double *dt_dev,
-                                         const double *bc_val, double *vals, float *vals32, double *rhs,
-                                         double *dinv, cudaStream_t st) {
+                                         const double *Ks_inc, const double s[4], const double mc[4], double dt,
+                                         const double *dt_dev, const double *bc_val, double *vals, float *vals32,
+                                         double *rhs, double *dinv, cudaStream_t st) {
     RichardsAsmArgs a;
     a.n_rows = pat->n_rows;
     a.slice_ptr = pat->slice_ptr; a.slice_width = pat->slice_width; a.diag_pos = pat->diag_pos;
     a.inc_ptr = pat->inc_ptr; a.inc_width = pat->inc_width; a.inc_elem = pat->inc_elem; a.inc_slots = pat->inc_slots;
     a.conn = mesh->conn; a.coords = mesh->coords;
     a.theta_m = theta_m; a.theta_n = theta_n; a.h_m = h_m; a.K = K; a.C = C; a.Ks_elem = Ks_elem; a.bc_val = bc_val;
+    a.Ks_inc = Ks_inc;
     for (int j = 0; j < 4; ++j) { a.s[j] = s[j]; a.mcoef[j] = mc[j]; }
     a.inv_dt = 1.0 / dt;
     a.dt_dev = dt_dev;
@@ -341,30 +408,23 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     a.vals = vals; a.vals32 = vals32; a.rhs = rhs; a.dinv = dinv;
     a.diag_off = pat->diag_offsets;
     a.cols = pat->cols;
-    const int mw = pat->max_width <= 8 ? 8 : (pat->max_width <= 16 ? 16 : (pat->max_width <= 32 ? 32 : 64));
     if (pat->max_width > 63) return WSPM_UNSUPPORTED;      // the incidence word holds 6-bit row positions
-    const int threads = mw <= 16 ? 128 : (mw == 32 ? 64 : 32);
-    const int blocks = (pat->n_slices * kSlice + threads - 1) / threads;
-    const size_t smem = (size_t)mw * threads * sizeof(double) * (1 + (mesh->dim + 1));
-#define WSPM_ASM_LAUNCH(D, M)                                                                              \
-    do {                                                                                                   \
-        if (smem > 48 * 1024)                                                                              \
-            cudaFuncSetAttribute(richards_rows_kernel<D, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                 (int)smem);                                                               \
-        richards_rows_kernel<D, M><<<blocks, threads, smem, st>>>(a);                                      \
-    } while (0)
+    const int ksm = Ks_inc ? 2 : (Ks_elem ? 1 : 0);
+    const int ns = pat->n_slices;
+    const int mw = pat->max_width;
+    // launch shapes measured on the 1024^2 triangle and 96^3 Kuhn-tetrahedron grids (B200)
     if (mesh->dim == 2) {
-        if (mw == 8) WSPM_ASM_LAUNCH(2, 8);
-        else if (mw == 16) WSPM_ASM_LAUNCH(2, 16);
-        else if (mw == 32) WSPM_ASM_LAUNCH(2, 32);
-        else WSPM_ASM_LAUNCH(2, 64);
+        if (mw <= 8) launch_rows<2, 8, true, 256, 3>(a, ksm, ns, st);
+        else if (mw <= 16) launch_rows<2, 16, true, 128, 1>(a, ksm, ns, st);
+        else if (mw <= 32) launch_rows<2, 32, true, 64, 1>(a, ksm, ns, st);
+        else launch_rows<2, 64, true, 32, 1>(a, ksm, ns, st);
     } else {
-        if (mw == 8) WSPM_ASM_LAUNCH(3, 8);
-        else if (mw == 16) WSPM_ASM_LAUNCH(3, 16);
-        else if (mw == 32) WSPM_ASM_LAUNCH(3, 32);
-        else WSPM_ASM_LAUNCH(3, 64);
+        if (pat->n_diags > 0 && mw <= 16) launch_rows<3, 16, false, 128, 8>(a, ksm, ns, st);
+        else if (mw <= 8) launch_rows<3, 8, true, 128, 1>(a, ksm, ns, st);
+        else if (mw <= 16) launch_rows<3, 16, true, 128, 1>(a, ksm, ns, st);
+        else if (mw <= 32) launch_rows<3, 32, true, 64, 1>(a, ksm, ns, st);
+        else launch_rows<3, 64, true, 32, 1>(a, ksm, ns, st);
     }
-#undef WSPM_ASM_LAUNCH
     return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }
 
@@ -373,17 +433,24 @@ int launch_richards_assembly(const wspm_mesh *mesh, const wspm_pattern *pat, con
                              const double *Ks_elem, const double s[4], const double mc[4], double dt,
                              const double *bc_val, double *vals, float *vals32, double *rhs, double *dinv,
                              cudaStream_t st) {
-    return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, s, mc, dt, nullptr,
-                                         bc_val, vals, vals32, rhs, dinv, st);
+    return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, nullptr, s, mc, dt,
+                                         nullptr, bc_val, vals, vals32, rhs, dinv, st);
 }
 
 int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
                                     const double *theta_n, const double *h_m, const double *K, const double *C,
-                                    const double *Ks_elem, const double s[4], const double mc[4],
-                                    const double *dt_dev, const double *bc_val, double *vals, float *vals32,
-                                    double *rhs, double *dinv, cudaStream_t st) {
-    return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, s, mc, 1.0, dt_dev,
-                                         bc_val, vals, vals32, rhs, dinv, st);
+                                    const double *Ks_elem, const double *Ks_inc, const double s[4],
+                                    const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
+                                    float *vals32, double *rhs, double *dinv, cudaStream_t st) {
+    return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, Ks_inc, s, mc, 1.0,
+                                         dt_dev, bc_val, vals, vals32, rhs, dinv, st);
+}
+
+int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st) {
+    const int ns = pat->n_slices;
+    incidence_gather_kernel<<<(ns * kSlice + 255) / 256, 256, 0, st>>>(ns, pat->inc_ptr, pat->inc_width,
+                                                                      pat->inc_elem, elem, out);
+    return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }
 
 int launch_soil(const SoilParams &sp, const double *h, int64_t n, double *C, double *K, double *theta,

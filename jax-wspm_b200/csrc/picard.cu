@@ -27,9 +27,10 @@ int launch_edge_terms(const wspm_pattern *pat, const wspm_edges *e, int mode, do
                       const double *K, const double *theta, double *vals, double *rhs, cudaStream_t st);
 int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
                                     const double *theta_n, const double *h_m, const double *K, const double *C,
-                                    const double *Ks_elem, const double s[4], const double mc[4],
-                                    const double *dt_dev, const double *bc_val, double *vals, float *vals32,
-                                    double *rhs, double *dinv, cudaStream_t st);
+                                    const double *Ks_elem, const double *Ks_inc, const double s[4],
+                                    const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
+                                    float *vals32, double *rhs, double *dinv, cudaStream_t st);
+int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st);
 
 struct PicardState {
     double err, tol;
@@ -202,6 +203,7 @@ struct PicardPlan {
     KrylovState *irs = nullptr;
     double *r64 = nullptr;
     float *x32 = nullptr, *dinv32 = nullptr;
+    double *Ks_inc = nullptr;   // Ks_elem in incidence order (owned by the plan), refreshed at every step start
 };
 
 int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
@@ -242,13 +244,14 @@ static int build_picard_graph(PicardPlan *P) {
             if (k) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
         if (P->irs) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)P->irs, (int)(sizeof(KrylovState) / 4));
     }
+    if (P->Ks_inc) launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, cs);
     step_init_kernel<<<nb, kBlock, 0, cs>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
                                             d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, hp, 1);
     if (e == cudaSuccess) e = capture_while(cs, hp, [&](cudaStream_t bs) {
         launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, bs);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
-                                        P->s, P->mc, d.dt_dev, d.bc_val, d.vals, d.mixed ? d.vals32 : nullptr,
-                                        d.rhs, d.dinv, bs);
+                                        P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
+                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, bs);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           bs);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
@@ -341,13 +344,14 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
     KrylovState *sts[5] = {P->cg64.st, P->cg32.st, P->bicg.st, P->gm.st, P->irs};
     for (KrylovState *k : sts)
         if (k) state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
+    if (P->Ks_inc) launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, st);
     step_init_kernel<<<nb, kBlock, 0, st>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
                                             d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, none, 0);
     for (int it = 0; it < d.picard_maxiter && rc == WSPM_OK; ++it) {
         launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, st);
-        launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem, P->s,
-                                        P->mc, d.dt_dev, d.bc_val, d.vals, d.mixed ? d.vals32 : nullptr, d.rhs,
-                                        d.dinv, st);
+        launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
+                                        P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
+                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, st);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           st);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
@@ -480,8 +484,21 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     } else {
         P->cg64 = carve_cg<double>(p, n, &used); p += used;
     }
+    if (d.Ks_elem) {
+        // incidence slots: at most n_slices * 32 * max_inc
+        const size_t slots = (size_t)P->pat.n_slices * kSlice * (size_t)(P->pat.max_inc > 0 ? P->pat.max_inc : 1);
+        if (cudaMalloc(&P->Ks_inc, slots * sizeof(double)) != cudaSuccess) {
+            P->Ks_inc = nullptr;
+            delete P;
+            return WSPM_CUDA_ERROR;
+        }
+    }
     int rc = build_picard_graph(P);
-    if (rc != WSPM_OK) { delete P; return rc; }
+    if (rc != WSPM_OK) {
+        if (P->Ks_inc) cudaFree(P->Ks_inc);
+        delete P;
+        return rc;
+    }
     *plan_out = P;
     return WSPM_OK;
 }
@@ -498,6 +515,7 @@ extern "C" int wspm_picard_destroy(void *plan) {
     PicardPlan *P = (PicardPlan *)plan;
     if (P->exec) cudaGraphExecDestroy(P->exec);
     if (P->graph) cudaGraphDestroy(P->graph);
+    if (P->Ks_inc) cudaFree(P->Ks_inc);
     delete P;
     return WSPM_OK;
 }
