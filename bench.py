@@ -195,8 +195,9 @@ def time_e2e(eng, h0, dt, steps, world, flush):
     return {"ms": ms, "picard_its": its, "h2d": N * 8, "d2h": N * 8 + 32}
 
 
-def roofline_probe(dm, eng, fp32, reps=200):
-    """Average duration of one Jacobi-CG iteration of the persistent CG kernel on the assembled system.
+def roofline_probe(dm, eng, fp32, reps=200, pipelined=False):
+    """Average duration of one Jacobi-CG iteration of the persistent CG kernel on the assembled system
+    (pipelined: the kernel of the mixed path's FP32 inner solve).
 
     The solve starts from x = 0 (so the residual cannot reach zero within `reps` iterations) and the kernel
     reports how many iterations it ran; a short run raises instead of being timed."""
@@ -210,6 +211,7 @@ def roofline_probe(dm, eng, fp32, reps=200):
     else:
         vals, dinv, b = eng.vals, eng.dinv, eng.rhs.clone()
     x = torch.zeros_like(b)
+    mode = (1 if fp32 else 0) | (2 if pipelined else 0)
     done = torch.zeros(1, dtype=torch.int32, device="cuda")
     work = torch.empty(int(lib.wspm_krylov_workspace_doubles(N, 0, 0)), dtype=torch.float64, device="cuda")
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -218,7 +220,7 @@ def roofline_probe(dm, eng, fp32, reps=200):
         x.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        check("cg_iterations", lib.wspm_cg_iterations(ctypes.byref(dm.c_pat), int(fp32), _lib.dptr(vals),
+        check("cg_iterations", lib.wspm_cg_iterations(ctypes.byref(dm.c_pat), mode, _lib.dptr(vals),
                                                        _lib.dptr(b), _lib.dptr(x), _lib.dptr(dinv), iters,
                                                        _lib.dptr(work), work.numel(), _lib.dptr(done), st))
         e1.record()
@@ -319,12 +321,13 @@ def cg_probe(args):
     Q, W = default_rule(2)
     vals, rhs, dinv, vals32 = assemble_richards(dm, th, th, h, K, C, Q, W, 1e-4, bc_val=bc,
                                                 Ks_elem=torch.as_tensor(Ks, device="cuda"), want_f32=True)
-    fp32 = args.cg_probe == "fp32"
+    fp32 = args.cg_probe in ("fp32", "fp32p")
+    mode = (1 if fp32 else 0) | (2 if args.cg_probe == "fp32p" else 0)
     v, b, x, d = (vals32, rhs.float(), h.float(), dinv.float()) if fp32 else (vals, rhs, h.clone(), dinv)
     work = torch.empty(int(_lib.lib.wspm_krylov_workspace_doubles(N, 0, 0)), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     _lib.check("cg_iterations", _lib.lib.wspm_cg_iterations(
-        ctypes.byref(dm.c_pat), int(fp32), _lib.dptr(v), _lib.dptr(b), _lib.dptr(x), _lib.dptr(d), args.probe_iters,
+        ctypes.byref(dm.c_pat), mode, _lib.dptr(v), _lib.dptr(b), _lib.dptr(x), _lib.dptr(d), args.probe_iters,
         _lib.dptr(work), work.numel(), None, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
     torch.cuda.synchronize()
     print(f"cg probe {args.cg_probe}: {args.probe_iters} iterations, |x| = {float(torch.linalg.norm(x.double())):.6e}")
@@ -578,7 +581,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--inner-tol", type=float, default=1e-5,
                     help="floor of the relative tolerance of each FP32 solve in the refinement loop")
-    ap.add_argument("--cg-probe", choices=["fp64", "fp32"], default=None,
+    ap.add_argument("--cg-probe", choices=["fp64", "fp32", "fp32p"], default=None,
                     help="profiling target: assemble the workload once and run --probe-iters CG iterations "
                          "through wspm_cg_iterations, then exit (no JSON line)")
     ap.add_argument("--probe-iters", type=int, default=4)
@@ -645,7 +648,7 @@ def main():
         res_true[name] = float(torch.linalg.norm(r) / torch.linalg.norm(eng.rhs))
     rel_diff = float(torch.linalg.norm(hmx - h64) / torch.linalg.norm(h64))
     # roofline of the dominant kernels (one Jacobi-CG iteration = fused K1 + K2)
-    t_it32 = roofline_probe(dm, engmx, fp32=True)
+    t_it32 = roofline_probe(dm, engmx, fp32=True, pipelined=True)
     t_it64 = roofline_probe(dm, eng64, fp32=False)
     nnz = dm.pattern.nnz
     peak, peak_kind = load_peaks()
@@ -683,7 +686,7 @@ def main():
         "status": {"fp64": r64["status"], "mixed": rmx["status"]},
         "e2e": {"value": ve2e, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
         "gpu_launches": rmx["launches"] + r64["launches"],
-        "roofline": {"bound": "hbm", "kernel": "one FP32 Jacobi-CG iteration (fused SpMV kernel + update kernel)",
+        "roofline": {"bound": "hbm", "kernel": "one FP32 Jacobi-CG iteration of the resident pipelined CG kernel (mixed path inner solve)",
                      "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak, "peak_kind": peak_kind,
                      "traffic": load_traffic("cg_iteration_f32"), "algorithmic_bytes": b32,
                      "seconds_per_iteration": t_it32,

@@ -203,14 +203,21 @@ int wspm_krylov_solve(const wspm_pattern *pat, const double *vals,
                       int32_t *result, void *stream);
 
 /* Measurement hook (no reference counterpart): runs up to `iters` Jacobi-CG
- * iterations of the persistent CG kernel with tolerance 0 from x on the given
+ * iterations of a persistent CG kernel with tolerance 0 from x on the given
  * system, as plain launches on `stream`, so the per-iteration time of the
  * dominant kernel can be taken with CUDA events.  The kernel still stops early
  * on an exactly zero residual or a non-finite value; `iters_done` (device
  * int32, may be NULL) receives the iterations actually run, so a timing can be
- * rejected when it is short.  fp32 != 0 selects the FP32 kernel (vals, b, x,
- * dinv are then float arrays).  `work` as for CG.                            */
-int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const void *vals, const void *b, void *x,
+ * rejected when it is short.  `mode` is a bit set: WSPM_CGIT_FP32 selects the
+ * FP32 kernel (vals, b, x, dinv are then float arrays); WSPM_CGIT_PIPELINED
+ * the pipelined form used by the mixed path's inner solve (DIA patterns whose
+ * per-block vectors fit on chip; WSPM_UNSUPPORTED otherwise), whose
+ * reduction is waited for by one dedicated warp per block unless
+ * WSPM_CGIT_NO_WARP_SPECIALIZATION is set.  `work` as for CG.              */
+#define WSPM_CGIT_FP32 1
+#define WSPM_CGIT_PIPELINED 2
+#define WSPM_CGIT_NO_WARP_SPECIALIZATION 4
+int wspm_cg_iterations(const wspm_pattern *pat, int32_t mode, const void *vals, const void *b, void *x,
                        const void *dinv, int32_t iters, double *work, int64_t work_doubles,
                        int32_t *iters_done, void *stream);
 

@@ -301,10 +301,13 @@ extern "C" int wspm_krylov_solve(const wspm_pattern *pat, const double *vals, co
 
 __global__ void copy_k_kernel(const KrylovState *st, int32_t *out) { *out = st->k; }
 
-extern "C" int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const void *vals, const void *b, void *x,
+extern "C" int wspm_cg_iterations(const wspm_pattern *pat, int32_t mode, const void *vals, const void *b, void *x,
                                   const void *dinv, int32_t iters, double *work, int64_t work_doubles,
                                   int32_t *iters_done, void *stream) {
-    if (!pattern_ok(pat) || !vals || !b || !x || !work || iters < 0) return WSPM_BAD_ARG;
+    if (!pattern_ok(pat) || !vals || !b || !x || !work || iters < 0 || mode < 0 || mode > 7) return WSPM_BAD_ARG;
+    const bool fp32 = (mode & WSPM_CGIT_FP32) != 0;
+    const bool pipelined = (mode & WSPM_CGIT_PIPELINED) != 0;
+    const bool ws = (mode & WSPM_CGIT_NO_WARP_SPECIALIZATION) == 0;
     if (work_doubles < cg_workspace_doubles(pat->n_rows, fp32 ? 4 : 8)) return WSPM_BAD_ARG;
     const Sell A = make_sell(pat);
     cudaStream_t st = (cudaStream_t)stream;
@@ -316,14 +319,22 @@ extern "C" int wspm_cg_iterations(const wspm_pattern *pat, int32_t fp32, const v
         CgBuffers<float> w = carve_cg<float>(work, pat->n_rows, &used);
         state = w.st;
         state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
-        rc = cg_persistent_enqueue<float>(A, (const float *)vals, (const float *)b, nullptr, (float *)x,
-                                          (const float *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
+        if (pipelined)
+            rc = pcg_persistent_enqueue<float>(A, (const float *)vals, (const float *)b, nullptr, (float *)x,
+                                               (const float *)dinv, w, 0.0, 0.0, iters, false, nullptr, st, ws);
+        else
+            rc = cg_persistent_enqueue<float>(A, (const float *)vals, (const float *)b, nullptr, (float *)x,
+                                              (const float *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
     } else {
         CgBuffers<double> w = carve_cg<double>(work, pat->n_rows, &used);
         state = w.st;
         state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
-        rc = cg_persistent_enqueue<double>(A, (const double *)vals, (const double *)b, nullptr, (double *)x,
-                                           (const double *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
+        if (pipelined)
+            rc = pcg_persistent_enqueue<double>(A, (const double *)vals, (const double *)b, nullptr, (double *)x,
+                                                (const double *)dinv, w, 0.0, 0.0, iters, false, nullptr, st, ws);
+        else
+            rc = cg_persistent_enqueue<double>(A, (const double *)vals, (const double *)b, nullptr, (double *)x,
+                                               (const double *)dinv, w, 0.0, 0.0, iters, false, nullptr, st);
     }
     if (rc == WSPM_OK && iters_done) copy_k_kernel<<<1, 1, 0, st>>>(state, iters_done);
     return rc;

@@ -849,6 +849,482 @@ template int cg_persistent_enqueue<float>(const Sell &, const float *, const flo
                                           const float *, const CgBuffers<float> &, double, double, int, bool,
                                           const double *, cudaStream_t);
 
+// ---------------------------------------------------------------- pipelined CG
+// Pipelined Jacobi-CG (Ghysels & Vanroose, Parallel Computing 40 (2014)
+// 224-238, Alg. 4) as one resident cooperative launch.  With M diagonal the
+// recurrences of u = M r, q = M s and m = M w collapse into products with
+// 1/diag taken on the fly, leaving
+//   gamma = (r, u), delta = (w, u), rho = (r, r)     (reduction i, in flight)
+//   n = A m,  m = M w                                (SpMV i, overlapping it)
+//   beta = gamma/gamma_old, alpha = gamma/(delta - beta gamma/alpha_old)
+//   z = n + beta z ; s = w + beta s ; p = M r + beta p
+//   x += alpha p ; r -= alpha s ; w -= alpha z
+// so the grid-wide reduction of iteration i travels while the block computes
+// its SpMV: the scalars are read after the SpMV, not before it.  The iterates
+// equal those of CG in exact arithmetic; the recurrence for w (w = A M r is
+// never recomputed) lets the recursive residual drift from the true one by
+// rounding, which is why this form serves the FP32 inner solve of the mixed
+// path, where the outer FP64 refinement measures the true residual.
+//
+// Block b owns rows [b*chunk, (b+1)*chunk); r, w, s, p, z, n (and x when it
+// fits) stay in shared memory.  m crosses blocks through two alternating
+// global vectors: m_{i+1} is written into the vector that held m_{i-1}, which
+// every block finished reading before it arrived at reduction i (a block
+// writes only after passing that reduction).  Partial sums alternate between
+// two buffers for the same reason.  One warp of each block waits for the
+// reduction and sums the partials while the other warps run the SpMV (named
+// barrier 1 among them), so the reduction latency leaves the critical path.
+// Every wait is bounded like the other resident kernels.
+enum PcgVec { kPR = 0, kPW, kPS, kPP, kPZ, kPN, kPX, kNumPcgVec };
+
+template <typename T>
+struct PcgArgs {
+    Sell A;
+    const T *vals;
+    const T *b;
+    const double *b64;
+    T *x;
+    const T *dinv;
+    T *ex[2];              // exchange vectors: u0 in ex[0], then m_i in ex[(i + 1) & 1]
+    int chunk;
+    T *part;               // [2 parities][3][grid], then [1][grid] for the init
+    unsigned int *flag;    // [grid] per-block exchange epoch
+    KrylovState *st;
+    GridBarrier *bar;
+    double tol, atol;
+    const double *tol_dev;
+    int maxiter, zero_x0;
+};
+
+// OR of `pred` over the nthreads threads that use named barrier `id`.
+__device__ __forceinline__ int bar_red_or(int id, int nthreads, int pred) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.s32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(pred), "r"(id), "r"(nthreads)
+        : "memory");
+    return r;
+}
+
+// wait_zflags for a group of threads [0, nthr) of the block: the block-wide
+// barrier (named = false) or named barrier 1 (named = true).
+__device__ __forceinline__ bool wait_flags_group(const unsigned int *flag, int lo, int hi, unsigned int epoch,
+                                                 GridBarrier *gb, int tid, int nthr, bool named) {
+    int fail = 0;
+    for (int c = lo + tid; c <= hi && !fail; c += nthr) {
+        if (c == (int)blockIdx.x) continue;
+        long long spins = 0;
+        while (ld_acquire_u32(flag + c) < epoch) {
+            if (++spins > kBarrierSpinLimit) { atomicExch(&gb->error, 1); fail = 1; break; }
+            if ((spins & 1023) == 0 && *(volatile int *)&gb->error) { fail = 1; break; }
+            __nanosleep(20);
+        }
+    }
+    if (named) return bar_red_or(1, nthr, fail) == 0;
+    return __syncthreads_or(fail) == 0;
+}
+
+// Bounded wait until the counting barrier has seen `target` arrivals (one thread).
+__device__ __forceinline__ bool count_wait(GridBarrier *gb, unsigned int target) {
+    long long spins = 0;
+    while (ld_acquire_u32(&gb->mono) < target) {
+        if (++spins > kBarrierSpinLimit) { atomicExch(&gb->error, 1); return false; }
+        if ((spins & 1023) == 0 && *(volatile int *)&gb->error) return false;
+        __nanosleep(20);
+    }
+    return (*(volatile int *)&gb->error) == 0;
+}
+
+// reduce_partials_rows done by a single warp (rows one after the other, the
+// same per-row arithmetic, so every block gets bitwise identical sums).
+template <typename T, int NV>
+__device__ __forceinline__ void warp_partials(const T *partials, int nb, T (&out)[NV]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const T *pj = partials + (int64_t)j * nb;
+        T acc = T(0);
+        for (int b0 = 0; b0 < nb; b0 += 256) {
+            T x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int b = b0 + lane + 32 * u;
+                x[u] = b < nb ? __ldcg(pj + b) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc += x[u];
+        }
+        out[j] = warp_sum(acc);
+    }
+}
+
+// dst[l] = (A src)[r0 + l] over the block's rows, 16-byte groups, threads
+// [0, nthr) of the block (round-robin like rcg_spmv_dia: interior groups
+// first, the wait for the neighbours' flags before the first round with a
+// halo group).  Returns false when that wait gave up.
+template <typename T, int MW>
+__device__ __forceinline__ bool pcg_spmv_dia(int nl, int lo_i, int hi_i, const T *__restrict__ vals, int64_t ld,
+                                             int r0, int last, int nd, const int *s_off, const T *src, T *dst,
+                                             const unsigned int *flag, int nbr_lo, int nbr_hi, unsigned int epoch,
+                                             bool poll, GridBarrier *bar, int tid, int nthr, bool named) {
+    using VT = Vec16<T>;
+    constexpr int N = VT::N;
+    const int ng = (nl + N - 1) / N;
+    const int gi0 = lo_i / N, gi1 = hi_i / N;
+    const int nint = gi1 - gi0, nlow = gi0;
+    const int rounds = (ng + nthr - 1) / nthr;
+    const int m_wait = poll ? nint / nthr : rounds;
+    for (int m = 0; m < rounds; ++m) {
+        if (m == m_wait && !wait_flags_group(flag, nbr_lo, nbr_hi, epoch, bar, tid, nthr, named)) return false;
+        const int j = tid + m * nthr;
+        if (j >= ng) continue;
+        int g;
+        if (j < nint) g = gi0 + j;
+        else {
+            const int h = j - nint;
+            g = h < nlow ? h : gi1 + (h - nlow);
+        }
+        const int l = g * N, i = r0 + l;
+        if (l + N <= nl) {
+            T w[N];
+            dia_group_z<T, MW>(vals, ld, i, last, nd, s_off, src, w);
+            *reinterpret_cast<typename VT::V *>(dst + l) = VT::join(w);
+        } else {
+            for (int q = 0; l + q < nl; ++q) dst[l + q] = dia_row_z<T, MW>(vals, ld, i + q, last, nd, s_off, src);
+        }
+    }
+    if (m_wait >= rounds && poll && !wait_flags_group(flag, nbr_lo, nbr_hi, epoch, bar, tid, nthr, named))
+        return false;
+    return true;
+}
+
+template <typename T, int MW, bool XS, bool WS>
+__global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a) {
+    using VT = Vec16<T>;
+    using V = typename VT::V;
+    constexpr int N = VT::N;
+    extern __shared__ __align__(16) unsigned char rcg_smem[];
+    __shared__ int s_off[MW];
+    __shared__ T s_scal[3];
+    __shared__ int s_ok;
+    T *const sm = reinterpret_cast<T *>(rcg_smem);
+    const int n = a.A.n_rows;
+    const int nb = gridDim.x;
+    const int chunk = a.chunk;
+    const int r0 = blockIdx.x * chunk;
+    const int r1 = min(n, r0 + chunk);
+    const int nl = max(0, r1 - r0);
+    const int TB = blockDim.x;
+    const int tid = threadIdx.x;
+    unsigned int gen = tid == 0 ? ld_acquire_u32(&a.bar->gen) : 0u;
+    if (tid == 0) {
+        a.flag[blockIdx.x] = 0u;
+        if (blockIdx.x == 0) a.bar->mono = 0u;
+    }
+    const T *const vals = a.vals;
+    const T *const dg = a.dinv;
+    T *const xg = a.x;
+    T *const ex0 = a.ex[0];
+    T *const ex1 = a.ex[1];
+    T *const part = a.part;
+    unsigned int *const flag = a.flag;
+    GridBarrier *const bar = a.bar;
+    T *const vR = sm + kPR * chunk, *const vW = sm + kPW * chunk, *const vS = sm + kPS * chunk;
+    T *const vP = sm + kPP * chunk, *const vZ = sm + kPZ * chunk, *const vN = sm + kPN * chunk;
+    T *const vX = XS ? sm + kPX * chunk : xg + r0;   // x: on chip when it fits, else the caller's array
+    const int nd = a.A.n_diags;
+    const int64_t ld = a.A.ld;
+    const int last = n - 1;
+    int mn = 0, mx = 0;
+    for (int k = 0; k < nd; ++k) {
+        const int o = __ldg(a.A.diag_off + k);
+        if (tid == 0) s_off[k] = o;
+        mn = min(mn, o);
+        mx = max(mx, o);
+    }
+    const int lo_i = min(nl, (-mn + N - 1) / N * N);
+    const int hi_i = max(lo_i, (nl - mx) / N * N);
+    int nbr_lo = min(nb - 1, max(0, r0 + mn) / chunk);
+    int nbr_hi = min(nb - 1, min(n - 1, r1 - 1 + mx) / chunk);
+    if (nl == 0) { nbr_lo = 1; nbr_hi = 0; }
+    __syncthreads();
+    // ---- init: r = b - A x0, p = s = z = 0, u0 = M r -> ex0
+    {
+        T v[1] = {T(0)};
+        for (int l = tid; l < nl; l += TB) {
+            const int i = r0 + l;
+            const T bi = a.b64 ? (T)a.b64[i] : a.b[i];
+            T ri;
+            if (a.zero_x0) {
+                xg[i] = T(0);
+                if (XS) vX[l] = T(0);
+                ri = bi;
+            } else {
+                if (XS) vX[l] = xg[i];
+                ri = bi - dia_row_z<T, MW>(vals, ld, i, last, nd, s_off, xg);
+            }
+            const T di = dg ? dg[i] : T(1);
+            vR[l] = ri;
+            vS[l] = T(0);
+            vP[l] = T(0);
+            vZ[l] = T(0);
+            ex0[i] = di * ri;
+            v[0] += bi * bi;
+        }
+        block_sum<T, 1>(v);
+        if (tid == 0) part[6 * (int64_t)nb + blockIdx.x] = v[0];
+    }
+    bool ok = grid_barrier(bar, nb, gen);     // u0 complete everywhere; flags and mono reset
+    T binit[1];
+    reduce_partials_rows<T, 1>(part + 6 * (int64_t)nb, nb, binit);
+    const double bs = (double)binit[0];
+    const double tl = a.tol_dev ? *a.tol_dev : a.tol;
+    const double atol2 = fmax(tl * tl * bs, a.atol * a.atol);
+    // publish the partials (r, Mr), (w, Mr), (r, r) of the block's rows, arrive, raise the exchange flag
+    auto publish = [&](T *pp, unsigned int epoch, T (&v)[3]) {
+        block_sum<T, 3>(v);        // ends with a block barrier: every m store of this block is done
+        if (tid == 0) {
+            pp[blockIdx.x] = v[0];
+            pp[nb + blockIdx.x] = v[1];
+            pp[2 * nb + blockIdx.x] = v[2];
+            __threadfence();
+            atomicAdd(&bar->mono, 1u);
+            st_release_u32(flag + blockIdx.x, epoch);
+        }
+    };
+    // w0 = A u0 (the grid barrier published u0), then m0 = M w0 and reduction 0
+    if (ok) {
+        ok = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, ld, r0, last, nd, s_off, ex0, vW, flag, nbr_lo, nbr_hi, 0u,
+                                 false, bar, tid, TB, false);
+        __syncthreads();
+        T v[3] = {T(0), T(0), T(0)};
+        for (int l = tid; l < nl; l += TB) {
+            const int i = r0 + l;
+            const T di = dg ? dg[i] : T(1);
+            const T ri = vR[l], wi = vW[l];
+            const T ui = di * ri;
+            ex1[i] = di * wi;
+            v[0] += ri * ui;
+            v[1] += wi * ui;
+            v[2] += ri * ri;
+        }
+        publish(part, 2u, v);
+    }
+    double gamma = 0.0, delta = 0.0, rho = 0.0, gamma_old = 1.0, alpha = 0.0, beta = 0.0;
+    int k = 0, status = WSPM_OK;
+    const int nthr = WS ? TB - 32 : TB;
+    const bool red_warp = WS && tid >= TB - 32;
+    while (ok) {
+        // ---- SpMV n_k = A m_k (m_k in ex[(k + 1) & 1]) while reduction k travels
+        const T *msrc = (k & 1) ? ex0 : ex1;
+        const T *pp = part + (int64_t)(k & 1) * 3 * nb;
+        const unsigned int target = (unsigned)(k + 1) * (unsigned)nb;
+        if (WS) {
+            if (!red_warp) {
+                const bool o = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, ld, r0, last, nd, s_off, msrc, vN, flag,
+                                                   nbr_lo, nbr_hi, (unsigned)(k + 2), true, bar, tid, nthr, true);
+                if (tid == 0) s_ok = o ? 1 : 0;
+            } else {
+                int w_ok = 1;
+                if ((tid & 31) == 0) w_ok = count_wait(bar, target) ? 1 : 0;
+                w_ok = __shfl_sync(0xffffffffu, w_ok, 0);
+                __syncwarp();
+                T t3[3];
+                warp_partials<T, 3>(pp, nb, t3);
+                if ((tid & 31) == 0) {
+                    s_scal[0] = t3[0];
+                    s_scal[1] = t3[1];
+                    s_scal[2] = t3[2];
+                    if (!w_ok) atomicExch(&bar->error, 1);
+                }
+            }
+            __syncthreads();
+            ok = s_ok != 0 && (*(volatile int *)&bar->error) == 0;
+            __syncthreads();       // every thread has read s_ok before it is written again
+        } else {
+            ok = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, ld, r0, last, nd, s_off, msrc, vN, flag, nbr_lo, nbr_hi,
+                                     (unsigned)(k + 2), true, bar, tid, TB, false);
+            if (tid == 0) s_ok = count_wait(bar, target) ? 1 : 0;
+            __syncthreads();
+            ok = ok && s_ok != 0;
+            T t3[3];
+            reduce_partials_rows<T, 3>(pp, nb, t3);
+            if (tid == 0) {
+                s_scal[0] = t3[0];
+                s_scal[1] = t3[1];
+                s_scal[2] = t3[2];
+            }
+            __syncthreads();
+        }
+        if (!ok) break;
+        gamma = (double)s_scal[0];
+        delta = (double)s_scal[1];
+        rho = (double)s_scal[2];
+        const double rs = dg ? rho : gamma;
+        if (!isfinite(rs)) { status = WSPM_NAN; break; }
+        if (!(rs > atol2)) break;
+        if (k >= a.maxiter) { status = WSPM_MAXITER; break; }
+        if (k == 0) {
+            beta = 0.0;
+            alpha = (double)((T)gamma / (T)delta);
+        } else {
+            beta = (double)((T)gamma / (T)gamma_old);
+            alpha = (double)((T)gamma / ((T)delta - (T)beta * (T)gamma / (T)alpha));
+        }
+        if (!isfinite(alpha)) { status = WSPM_NAN; break; }
+        // ---- update: x_{k+1}, r, w, s, p, z; m_{k+1} = M w_{k+1} -> ex[k & 1]; reduction k + 1
+        T *mdst = (k & 1) ? ex1 : ex0;
+        T *pn = part + (int64_t)((k + 1) & 1) * 3 * nb;
+        {
+            const T al = (T)alpha, bt = (T)beta;
+            T v[3] = {T(0), T(0), T(0)};
+            for (int l = N * tid; l < nl; l += N * TB) {
+                if (l + N <= nl) {
+                    T nv[N], zv[N], sv[N], pv[N], xv[N], rv[N], wv[N], dv[N];
+                    VT::split(*reinterpret_cast<const V *>(vN + l), nv);
+                    VT::split(*reinterpret_cast<const V *>(vZ + l), zv);
+                    VT::split(*reinterpret_cast<const V *>(vS + l), sv);
+                    VT::split(*reinterpret_cast<const V *>(vP + l), pv);
+                    VT::split(*reinterpret_cast<const V *>(vX + l), xv);
+                    VT::split(*reinterpret_cast<const V *>(vR + l), rv);
+                    VT::split(*reinterpret_cast<const V *>(vW + l), wv);
+                    if (dg) VT::split(__ldg(reinterpret_cast<const V *>(dg + r0 + l)), dv);
+                    else {
+#pragma unroll
+                        for (int q = 0; q < N; ++q) dv[q] = T(1);
+                    }
+                    T mv[N];
+#pragma unroll
+                    for (int q = 0; q < N; ++q) {
+                        zv[q] = fma(bt, zv[q], nv[q]);
+                        sv[q] = fma(bt, sv[q], wv[q]);
+                        pv[q] = fma(bt, pv[q], dv[q] * rv[q]);
+                        xv[q] = fma(al, pv[q], xv[q]);
+                        rv[q] = fma(-al, sv[q], rv[q]);
+                        wv[q] = fma(-al, zv[q], wv[q]);
+                        const T u = dv[q] * rv[q];
+                        mv[q] = dv[q] * wv[q];
+                        v[0] += rv[q] * u;
+                        v[1] += wv[q] * u;
+                        v[2] += rv[q] * rv[q];
+                    }
+                    *reinterpret_cast<V *>(vZ + l) = VT::join(zv);
+                    *reinterpret_cast<V *>(vS + l) = VT::join(sv);
+                    *reinterpret_cast<V *>(vP + l) = VT::join(pv);
+                    *reinterpret_cast<V *>(vX + l) = VT::join(xv);
+                    *reinterpret_cast<V *>(vR + l) = VT::join(rv);
+                    *reinterpret_cast<V *>(vW + l) = VT::join(wv);
+                    *reinterpret_cast<V *>(mdst + r0 + l) = VT::join(mv);
+                } else {
+                    for (int q = 0; l + q < nl; ++q) {
+                        const int lq = l + q;
+                        const T di = dg ? dg[r0 + lq] : T(1);
+                        const T zi = fma(bt, vZ[lq], vN[lq]);
+                        const T si = fma(bt, vS[lq], vW[lq]);
+                        const T pi = fma(bt, vP[lq], di * vR[lq]);
+                        const T xi = fma(al, pi, vX[lq]);
+                        const T ri = fma(-al, si, vR[lq]);
+                        const T wi = fma(-al, zi, vW[lq]);
+                        const T u = di * ri;
+                        vZ[lq] = zi; vS[lq] = si; vP[lq] = pi; vX[lq] = xi; vR[lq] = ri; vW[lq] = wi;
+                        mdst[r0 + lq] = di * wi;
+                        v[0] += ri * u;
+                        v[1] += wi * u;
+                        v[2] += ri * ri;
+                    }
+                }
+            }
+            publish(pn, (unsigned)(k + 3), v);
+        }
+        gamma_old = gamma;
+        ++k;
+    }
+    if (XS) {
+        __syncthreads();
+        for (int l = tid; l < nl; l += TB) xg[r0 + l] = vX[l];
+    }
+    if (blockIdx.x == 0 && tid == 0) {
+        KrylovState *st = a.st;
+        st->gamma = gamma; st->rr = rho; st->bs = bs; st->atol2 = atol2;
+        st->alpha = alpha; st->beta = beta;
+        st->k = k;
+        st->status = ok ? status : WSPM_CUDA_ERROR;
+        st->done = 1;
+    }
+}
+
+template <typename T, int MW, bool XS, bool WS>
+static cudaError_t pcg_launch(int grid, size_t smem, const PcgArgs<T> &a, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(pcg_resident_kernel<T, MW, XS, WS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kRcgBlock);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, pcg_resident_kernel<T, MW, XS, WS>, a);
+}
+
+template <typename T>
+int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
+                           const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
+                           const double *tol_dev, cudaStream_t st, bool warp_specialized) {
+    if (A.n_diags <= 0 || A.n_diags > 16) return WSPM_UNSUPPORTED;       // DIA patterns only
+    const uintptr_t al = (uintptr_t)vals | (uintptr_t)x | (uintptr_t)w.z | (uintptr_t)w.q |
+                         (uintptr_t)(dinv ? dinv : vals);
+    if (al % 16) return WSPM_BAD_ARG;
+    const RcgPlan pl = rcg_plan<T>(A.n_rows);
+    static int optin = 0;
+    if (optin == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    }
+    const int64_t per_vec = (int64_t)pl.chunk * sizeof(T);
+    const int64_t room = (int64_t)optin - 4096;
+    int nsv;
+    if (room >= kNumPcgVec * per_vec) nsv = kNumPcgVec;
+    else if (room >= (kNumPcgVec - 1) * per_vec) nsv = kNumPcgVec - 1;
+    else return WSPM_UNSUPPORTED;                                        // too many rows per block
+    PcgArgs<T> a;
+    a.A = A; a.vals = vals; a.b = b; a.b64 = b64; a.x = x; a.dinv = dinv;
+    a.ex[0] = w.z; a.ex[1] = w.q;
+    a.chunk = pl.chunk;
+    a.part = w.partials; a.st = w.st;
+    a.bar = (GridBarrier *)&w.st->ticket[0];
+    a.flag = reinterpret_cast<unsigned int *>(w.partials + 16 * 1024);   // after 7 * grid <= 7168 slots
+    a.tol = tol; a.atol = atol; a.tol_dev = tol_dev; a.maxiter = maxiter; a.zero_x0 = zero_x0 ? 1 : 0;
+    const size_t smem = (size_t)(nsv * per_vec);
+    cudaError_t e = cudaSuccess;
+    const bool xs = nsv == kNumPcgVec;
+#define WSPM_PCG(MW_)                                                                              \
+    do {                                                                                           \
+        if (xs) e = warp_specialized ? pcg_launch<T, MW_, true, true>(pl.grid, smem, a, st)        \
+                                     : pcg_launch<T, MW_, true, false>(pl.grid, smem, a, st);      \
+        else e = warp_specialized ? pcg_launch<T, MW_, false, true>(pl.grid, smem, a, st)          \
+                                  : pcg_launch<T, MW_, false, false>(pl.grid, smem, a, st);        \
+    } while (0)
+    if (A.n_diags <= 8) WSPM_PCG(8);
+    else WSPM_PCG(16);
+#undef WSPM_PCG
+    return e == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+}
+
+template int pcg_persistent_enqueue<double>(const Sell &, const double *, const double *, const double *, double *,
+                                            const double *, const CgBuffers<double> &, double, double, int, bool,
+                                            const double *, cudaStream_t, bool);
+template int pcg_persistent_enqueue<float>(const Sell &, const float *, const float *, const double *, float *,
+                                           const float *, const CgBuffers<float> &, double, double, int, bool,
+                                           const double *, cudaStream_t, bool);
+
 // ---------------------------------------------------------------- BiCGSTAB (FP64)
 template <int MW>
 __global__ void __launch_bounds__(kBlock) bicg_init_kernel(Sell A, const double *__restrict__ vals,

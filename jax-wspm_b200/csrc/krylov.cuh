@@ -67,6 +67,15 @@ int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double
                           const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
                           const double *tol_dev, cudaStream_t st);
 
+// Pipelined Jacobi-CG (one reduction per iteration, overlapped with the SpMV)
+// in one cooperative launch, same buffers and state as cg_persistent_enqueue.
+// DIA patterns whose per-block vectors fit in shared memory only; returns
+// WSPM_UNSUPPORTED (nothing launched) otherwise.
+template <typename T>
+int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
+                           const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
+                           const double *tol_dev, cudaStream_t st, bool warp_specialized = true);
+
 struct BicgBuffers {
     double *r, *rhat, *p, *phat, *q, *t;
     double *partials;

@@ -222,6 +222,19 @@ int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
     return t;
 }
 
+// FP32 inner solve of the refinement loop (correction d of A d = r64, from 0):
+// the pipelined CG where the pattern and the per-block vectors allow it (the
+// outer loop measures the true FP64 residual, so the pipelined recurrences
+// cannot hide an inaccurate inner solve), else the single-reduction form.
+static void inner_cg_enqueue(const Sell &A, const wspm_picard_desc &d, PicardPlan *P, const float *dv32,
+                             cudaStream_t s) {
+    const int rc = pcg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol,
+                                                 0.0, d.inner_maxiter, true, &P->irs->inner_tol, s);
+    if (rc == WSPM_UNSUPPORTED)
+        cg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
+                                     d.inner_maxiter, true, &P->irs->inner_tol, s);
+}
+
 static int build_picard_graph(PicardPlan *P) {
     const wspm_picard_desc &d = P->d;
     const int n = P->mesh.n_nodes;
@@ -269,8 +282,7 @@ static int build_picard_graph(PicardPlan *P) {
                                                                               d.refine_maxiter, hir, 1));
             capture_while(bs, hir, [&](cudaStream_t ibs) {
                 const float *dv32 = dinv ? P->dinv32 : nullptr;
-                cg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
-                                             d.inner_maxiter, true, &P->irs->inner_tol, ibs);
+                inner_cg_enqueue(A, d, P, dv32, ibs);
                 ir_correct_kernel<<<nb, kBlock, 0, ibs>>>(n, d.x, P->x32);
                 WSPM_WIDTH_DISPATCH(A.max_width,
                                     ir_residual_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, d.rhs, d.x, P->r64,
@@ -367,8 +379,7 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
             const float *dv32 = dinv ? P->dinv32 : nullptr;
             for (int r = 0; r <= d.refine_maxiter && rc == WSPM_OK; ++r) {
                 if ((rc = read_flag(&P->irs->done, st, &flag, pinned)) != WSPM_OK || flag) break;
-                cg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
-                                             d.inner_maxiter, true, &P->irs->inner_tol, st);
+                inner_cg_enqueue(A, d, P, dv32, st);
                 ir_correct_kernel<<<nb, kBlock, 0, st>>>(n, d.x, P->x32);
                 WSPM_WIDTH_DISPATCH(A.max_width,
                                     ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.x, P->r64,

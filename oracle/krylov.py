@@ -79,6 +79,49 @@ def cg(A, b, x0, tol=1e-10, atol=0.0, maxiter=100, dinv=None):
     return x, k
 
 
+
+def pipelined_cg(A, b, x0, tol=1e-10, atol=0.0, maxiter=100, dinv=None, dtype=np.float64):
+    """Pipelined Jacobi-CG as the device's inner solver computes it (not a reference function: the mixed
+    path's FP32 inner solve).  Ghysels & Vanroose, Parallel Computing 40 (2014) 224-238, Alg. 4, with the
+    recurrences of u = M r, q = M s, m = M w collapsed into products with the diagonal d (M = diag(d)):
+    gamma = (r, u), delta = (w, u), rho = (r, r) are read after n = A M w; the stopping rule tests rho
+    (gamma without a preconditioner) before the update.  Equals CG in exact arithmetic; the recurrence for
+    w = A M r drifts by rounding.  Returns (x, iterations)."""
+    d = np.ones(len(b)) if dinv is None else np.asarray(dinv)
+    A = A.astype(dtype)
+    d = d.astype(dtype)
+    b = np.asarray(b).astype(dtype)
+    x = np.array(x0, dtype=dtype, copy=True)
+    r = b - A @ x
+    u = d * r
+    w = A @ u
+    z, s, p = (np.zeros_like(r) for _ in range(3))
+    bs = float(b @ b)
+    atol2 = max(tol * tol * bs, atol * atol)
+    gamma_old = alpha = 0.0
+    k = 0
+    while True:
+        gamma, delta, rho = float(r @ u), float(w @ u), float(r @ r)
+        n_ = A @ (d * w)
+        rs = gamma if dinv is None else rho
+        if not (rs > atol2) or k >= maxiter:
+            break
+        if k == 0:
+            beta, alpha = 0.0, gamma / delta
+        else:
+            beta = gamma / gamma_old
+            alpha = gamma / (delta - beta * gamma / alpha)
+        z = n_ + dtype(beta) * z
+        s = w + dtype(beta) * s
+        p = u + dtype(beta) * p
+        x = x + dtype(alpha) * p
+        r = r - dtype(alpha) * s
+        w = w - dtype(alpha) * z
+        u = d * r
+        gamma_old = gamma
+        k += 1
+    return x, k
+
 def bicgstab(A, b, x0, tol=1e-10, atol=0.0, maxiter=100, dinv=None):
     """Returns (x, iterations); iterations < 0 flags a breakdown exit."""
     M = _precond(dinv)

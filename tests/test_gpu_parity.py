@@ -213,6 +213,74 @@ def test_zero_rhs_gmres_returns_x0():
     assert host(res)[1] == 0
 
 
+def _cg_iterations(dm, vals, b, x0, dinv, iters, mode):
+    """`iters` iterations of a persistent CG kernel (tolerance 0) through wspm_cg_iterations."""
+    import ctypes
+    from wspm_b200 import _lib
+    work = torch.empty(int(_lib.lib.wspm_krylov_workspace_doubles(dm.n_nodes, 0, 0)), dtype=torch.float64,
+                       device="cuda")
+    done = torch.zeros(1, dtype=torch.int32, device="cuda")
+    x = x0.clone()
+    _lib.check("cg_iterations", _lib.lib.wspm_cg_iterations(
+        ctypes.byref(dm.c_pat), mode, _lib.dptr(vals), _lib.dptr(b), _lib.dptr(x), _lib.dptr(dinv), iters,
+        _lib.dptr(work), work.numel(), _lib.dptr(done), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    return x, int(done.item())
+
+
+@pytest.mark.parametrize("n", [30, 256])
+@pytest.mark.parametrize("warp_specialized", [True, False])
+def test_pipelined_cg_iterates_match_cg(n, warp_specialized):
+    """The pipelined CG kernel (the mixed path's inner solver) against the oracle's restatement of the same
+    algorithm: after k iterations from a nonzero x0, x agrees to FP64 rounding (1e-9 norm-wise) and, in FP32, to
+    FP32 rounding (1e-4).  Against textbook CG it agrees only up to the recurrence drift of the pipelined form
+    (1.3e-5 relative after 25 iterations at n = 256, the same in the oracle restatement and for the
+    single-reduction kernel), so that comparison is loose.  n = 256 has 148 blocks of 448 rows."""
+    pts, el, A, b, h = _linear_system(n=n)
+    D = dev()
+    dm = D.DeviceMesh(pts, el, layout="dia")
+    assert dm.pattern.n_diags > 0
+    vals = cu(dm.pattern.sell_from_csr_values(A.data))
+    dinv = D.jacobi_dinv(dm, vals)
+    dj = okry.jacobi_inverse_diagonal(A)
+    k = 25
+    pipe = 2 | (0 if warp_specialized else 4)
+    x_pref, kp = okry.pipelined_cg(A, b, h, tol=0.0, maxiter=k, dinv=dj)
+    x_ref, k_ref = okry.cg(A, b, h, tol=0.0, maxiter=k, dinv=dj)
+    assert kp == k_ref == k
+    nrm = np.linalg.norm(x_ref)
+    x_cg, k1 = _cg_iterations(dm, vals, cu(b), cu(h), dinv, k, 0)
+    x_p, k2 = _cg_iterations(dm, vals, cu(b), cu(h), dinv, k, pipe)
+    assert (k1, k2) == (k, k)
+    assert np.linalg.norm(host(x_p) - x_pref) <= 1e-9 * nrm
+    # the single-reduction kernel's recurrences drift from textbook CG alike (1.3e-5 at n = 256)
+    assert np.linalg.norm(host(x_cg) - x_ref) <= 1e-4 * nrm
+    assert np.linalg.norm(host(x_p) - x_ref) <= 1e-4 * nrm
+    # FP32: fewer iterations, before the iterates reach FP32 rounding (where the scalar recurrences of either
+    # form may produce a non-finite step and stop the run)
+    k32 = 10
+    x_pref, _ = okry.pipelined_cg(A, b, h, tol=0.0, maxiter=k32, dinv=dj)
+    x_ref, _ = okry.cg(A, b, h, tol=0.0, maxiter=k32, dinv=dj)
+    v32, b32, h32, d32 = vals.float(), cu(b, torch.float32), cu(h, torch.float32), dinv.float()
+    x_cg32, k3 = _cg_iterations(dm, v32, b32, h32, d32, k32, 1)
+    x_p32, k4 = _cg_iterations(dm, v32, b32, h32, d32, k32, 1 | pipe)
+    assert (k3, k4) == (k32, k32)
+    assert np.linalg.norm(host(x_p32).astype(np.float64) - x_pref) <= 1e-4 * nrm
+    # the single-reduction FP32 kernel against textbook FP64 CG: FP32 rounding plus the recurrence drift
+    assert np.linalg.norm(host(x_cg32).astype(np.float64) - x_ref) <= 1e-2 * nrm
+
+
+def test_pipelined_cg_rejects_sell_patterns():
+    from wspm_b200._lib import WSPM_UNSUPPORTED, WspmError
+    pts, el, A, b, h = _linear_system(n=8)
+    D = dev()
+    dm = D.DeviceMesh(pts, el, layout="sell")
+    vals = cu(dm.pattern.sell_from_csr_values(A.data))
+    with pytest.raises(WspmError) as e:
+        _cg_iterations(dm, vals, cu(b), cu(h), D.jacobi_dinv(dm, vals), 5, 2)
+    assert e.value.code == WSPM_UNSUPPORTED
+
+
 def _engine_test_case(case, n, solver, precond, layout="auto", **kw):
     from wspm_b200.device import DeviceMesh, merge_dirichlet
     from wspm_b200.engine import PicardEngine

@@ -72,3 +72,24 @@ def test_oracle_reproduces_test3d_npz(solver):
         np.testing.assert_allclose(res["pressure_head"][s], g["pressure_head"][k], rtol=1e-12, atol=1e-12)
         np.testing.assert_allclose(res["theta"][s], g["theta"][k], rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(res["errors"], g["errors"], rtol=1e-6)
+
+
+def test_oracle_pipelined_cg_converges_like_cg():
+    """The oracle's restatement of the device's pipelined inner CG: same solution as CG to the tolerance, the
+    iteration count within a few of CG's (the pipelined recurrences drift by rounding only)."""
+    from scipy.sparse import diags
+    from oracle import krylov
+    n = 400
+    rng = np.random.default_rng(3)
+    main = 2.0 + rng.uniform(0.0, 1.0, n)
+    A = diags([-np.ones(n - 1), main, -np.ones(n - 1)], [-1, 0, 1], format="csr")
+    b = rng.standard_normal(n)
+    d = krylov.jacobi_inverse_diagonal(A)
+    x1, k1 = krylov.cg(A, b, np.zeros(n), tol=1e-10, maxiter=1000, dinv=d)
+    x2, k2 = krylov.pipelined_cg(A, b, np.zeros(n), tol=1e-10, maxiter=1000, dinv=d)
+    assert abs(k1 - k2) <= 2
+    assert np.linalg.norm(b - A @ x2) <= 2e-10 * np.linalg.norm(b)
+    np.testing.assert_allclose(x2, x1, rtol=1e-8, atol=1e-8)
+    # a cap stops the run with exactly maxiter updates
+    _, k3 = krylov.pipelined_cg(A, b, np.zeros(n), tol=0.0, maxiter=7, dinv=d)
+    assert k3 == 7
