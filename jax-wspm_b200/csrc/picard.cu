@@ -133,55 +133,134 @@ __global__ void step_finish_kernel(int n, const double *__restrict__ h_m, double
 // ---- mixed precision: FP32 CG corrections inside FP64 refinement ----------
 // ir state (KrylovState): bs, atol2, rr, k (refinement iterations), steps (inner
 // iterations summed), status.
+//
+// (A y) for rows i and i + 1 (i even).  DIA with 16-byte aligned values: one
+// 16-byte load per diagonal for both rows; otherwise two row dots.  Each row
+// accumulates in diagonal order with fma, like sell_row_dot, so both paths
+// give the same bits.
+template <int MW, typename Y>
+__device__ __forceinline__ void ir_rows2(const Sell &A, const double *__restrict__ vals, bool vec, int i,
+                                         const Y *__restrict__ y, double (&acc)[2]) {
+    if (vec) {
+        const int nd = A.n_diags, last = A.n_rows - 1;
+        acc[0] = acc[1] = 0.0;
+#pragma unroll
+        for (int k = 0; k < MW; ++k) {
+            if (k < nd) {
+                const double2 v = __ldg(reinterpret_cast<const double2 *>(vals + (int64_t)k * A.ld + i));
+                const int o = __ldg(A.diag_off + k);
+                int c0 = i + o, c1 = i + 1 + o;
+                c0 = c0 < 0 ? 0 : (c0 > last ? last : c0);
+                c1 = c1 < 0 ? 0 : (c1 > last ? last : c1);
+                acc[0] = fma(v.x, (double)y[c0], acc[0]);
+                acc[1] = fma(v.y, (double)y[c1], acc[1]);
+            }
+        }
+    } else {
+        acc[0] = sell_row_dot<double, MW>(A, vals, i, [&](int c) { return (double)y[c]; });
+        acc[1] = i + 1 < A.n_rows ? sell_row_dot<double, MW>(A, vals, i + 1, [&](int c) { return (double)y[c]; })
+                                  : 0.0;
+    }
+}
+
+// Reduction tail shared by the two refinement kernels: tot = (r.r, b.b); sets
+// the next inner tolerance, the continue flag and the graph condition.
+__device__ __forceinline__ void ir_decide(const double (&tot)[2], KrylovState *irs, const KrylovState *inner,
+                                          int is_init, double tol, double inner_floor, int maxit,
+                                          cudaGraphConditionalHandle cond, int use_cond) {
+    if (is_init) {
+        irs->bs = tot[1];
+        irs->atol2 = tol * tol * tot[1];
+        irs->k = 0;
+        irs->steps = 0;
+        irs->pad0 = 0;
+        irs->status = WSPM_OK;
+    } else {
+        irs->k += 1;
+        irs->steps += inner->k;
+        irs->pad0 += 1;
+    }
+    irs->rr = tot[0];
+    // the next FP32 solve aims at the reduction the FP64 residual still needs
+    // (half of it, for margin), never tighter than the floor FP32 can reach
+    const double need = 0.5 * sqrt(irs->atol2 / fmax(tot[0], 1e-300));
+    irs->inner_tol = fmin(0.5, fmax(inner_floor, need));
+    int cont = tot[0] > irs->atol2 && irs->k < maxit;
+    if (!cont && tot[0] > irs->atol2) irs->status = WSPM_MAXITER;
+    if (!isfinite(tot[0])) { cont = 0; irs->status = WSPM_NAN; }
+    irs->done = !cont;
+    if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+}
+
+// Start of the refinement loop: x = x0, r = b - A x0 (FP64), the FP32 copy of
+// 1/diag, and the loop state.
 template <int MW>
-__global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const double *__restrict__ vals,
-                                                             const double *__restrict__ b, const double *x,
-                                                             double *r, const double *__restrict__ dinv,
-                                                             float *dinv32, double *partials, KrylovState *irs,
-                                                             const KrylovState *inner, int is_init, double tol,
+__global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const double *__restrict__ vals, bool vec,
+                                                             const double *__restrict__ b,
+                                                             const double *__restrict__ x0, double *x, double *r,
+                                                             const double *__restrict__ dinv, float *dinv32,
+                                                             double *partials, KrylovState *irs, double tol,
                                                              double inner_floor, int maxit,
                                                              cudaGraphConditionalHandle cond, int use_cond) {
     double v[2] = {0.0, 0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
-        const double acc = sell_row_dot<double, MW>(A, vals, i, [&](int c) { return x[c]; });
-        const double ri = b[i] - acc;
-        r[i] = ri;
-        if (is_init && dinv32) dinv32[i] = (float)dinv[i];
-        v[0] += ri * ri;
-        v[1] += b[i] * b[i];
+    const int n = A.n_rows;
+    for (int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 2 * gridDim.x * blockDim.x) {
+        double acc[2];
+        ir_rows2<MW, double>(A, vals, vec, i, x0, acc);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int iq = i + q;
+            if (iq < n) {
+                const double ri = b[iq] - acc[q];
+                r[iq] = ri;
+                x[iq] = x0[iq];
+                if (dinv32) dinv32[iq] = (float)dinv[iq];
+                v[0] += ri * ri;
+                v[1] += b[iq] * b[iq];
+            }
+        }
     }
     if (publish_partials<double, 2>(v, partials, &irs->ticket[0])) {
         double tot[2];
         final_sum<double, 2>(partials, tot, &irs->ticket[0]);
-        if (threadIdx.x == 0) {
-            if (is_init) {
-                irs->bs = tot[1];
-                irs->atol2 = tol * tol * tot[1];
-                irs->k = 0;
-                irs->steps = 0;
-                irs->pad0 = 0;
-                irs->status = WSPM_OK;
-            } else {
-                irs->k += 1;
-                irs->steps += inner->k;
-                irs->pad0 += 1;
-            }
-            irs->rr = tot[0];
-            // the next FP32 solve aims at the reduction the FP64 residual still needs
-            // (half of it, for margin), never tighter than the floor FP32 can reach
-            const double need = 0.5 * sqrt(irs->atol2 / fmax(tot[0], 1e-300));
-            irs->inner_tol = fmin(0.5, fmax(inner_floor, need));
-            int cont = tot[0] > irs->atol2 && irs->k < maxit;
-            if (!cont && tot[0] > irs->atol2) irs->status = WSPM_MAXITER;
-            if (!isfinite(tot[0])) { cont = 0; irs->status = WSPM_NAN; }
-            irs->done = !cont;
-            if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
-        }
+        if (threadIdx.x == 0) ir_decide(tot, irs, nullptr, 1, tol, inner_floor, maxit, cond, use_cond);
     }
 }
 
-__global__ void ir_correct_kernel(int n, double *x, const float *__restrict__ d) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += (double)d[i];
+// After an FP32 correction d: x += d and r -= A d (FP64; equal to b - A x up to
+// FP64 rounding, without re-reading b and the previous x).
+template <int MW>
+__global__ void __launch_bounds__(kBlock) ir_update_kernel(Sell A, const double *__restrict__ vals, bool vec,
+                                                           const float *__restrict__ d, double *x, double *r,
+                                                           double *partials, KrylovState *irs,
+                                                           const KrylovState *inner, double tol, double inner_floor,
+                                                           int maxit, cudaGraphConditionalHandle cond, int use_cond) {
+    double v[2] = {0.0, 0.0};
+    const int n = A.n_rows;
+    for (int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 2 * gridDim.x * blockDim.x) {
+        double acc[2];
+        ir_rows2<MW, float>(A, vals, vec, i, d, acc);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int iq = i + q;
+            if (iq < n) {
+                const double ri = r[iq] - acc[q];
+                r[iq] = ri;
+                x[iq] += (double)d[iq];
+                v[0] += ri * ri;
+            }
+        }
+    }
+    if (publish_partials<double, 2>(v, partials, &irs->ticket[0])) {
+        double tot[2];
+        final_sum<double, 2>(partials, tot, &irs->ticket[0]);
+        if (threadIdx.x == 0) ir_decide(tot, irs, inner, 0, tol, inner_floor, maxit, cond, use_cond);
+    }
+}
+
+// 16-byte aligned DIA values take the paired-row path of the refinement kernels
+static bool ir_vec(const Sell &A, const double *vals) {
+    return A.n_diags > 0 && ((uintptr_t)vals % 16) == 0 && (A.ld % 2) == 0;
 }
 
 struct PicardPlan {
@@ -274,22 +353,20 @@ static int build_picard_graph(PicardPlan *P) {
         if (d.mixed) {
             cudaGraphConditionalHandle hir;
             make_cond_handle(bs, &hir);
-            copy_kernel_d(d.h_m, d.x, n, bs);
+            const bool vec = ir_vec(A, d.vals);
             WSPM_WIDTH_DISPATCH(A.max_width,
-                                ir_residual_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, d.rhs, d.x, P->r64, d.dinv,
-                                                                              P->dinv32, P->partials, P->irs, P->cg32.st,
-                                                                              1, d.krylov_tol, d.inner_tol,
+                                ir_residual_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, vec, d.rhs, d.h_m, d.x, P->r64,
+                                                                              d.dinv, P->dinv32, P->partials, P->irs,
+                                                                              d.krylov_tol, d.inner_tol,
                                                                               d.refine_maxiter, hir, 1));
             capture_while(bs, hir, [&](cudaStream_t ibs) {
                 const float *dv32 = dinv ? P->dinv32 : nullptr;
                 inner_cg_enqueue(A, d, P, dv32, ibs);
-                ir_correct_kernel<<<nb, kBlock, 0, ibs>>>(n, d.x, P->x32);
                 WSPM_WIDTH_DISPATCH(A.max_width,
-                                    ir_residual_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, d.rhs, d.x, P->r64,
-                                                                                   d.dinv, nullptr, P->partials,
-                                                                                   P->irs, P->cg32.st, 0,
-                                                                                   d.krylov_tol, d.inner_tol,
-                                                                                   d.refine_maxiter, hir, 1));
+                                    ir_update_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, vec, P->x32, d.x, P->r64,
+                                                                                 P->partials, P->irs, P->cg32.st,
+                                                                                 d.krylov_tol, d.inner_tol,
+                                                                                 d.refine_maxiter, hir, 1));
             });
             irs = P->irs;
         } else if (d.solver == WSPM_SOLVER_BICGSTAB) {
@@ -370,23 +447,21 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                           st);
         const KrylovState *ks = nullptr, *irs = nullptr;
         if (d.mixed) {
-            copy_kernel_d(d.h_m, d.x, n, st);
+            const bool vec = ir_vec(A, d.vals);
             WSPM_WIDTH_DISPATCH(A.max_width,
-                                ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.x, P->r64, d.dinv,
-                                                                              P->dinv32, P->partials, P->irs,
-                                                                              P->cg32.st, 1, d.krylov_tol, d.inner_tol,
+                                ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, vec, d.rhs, d.h_m, d.x, P->r64,
+                                                                              d.dinv, P->dinv32, P->partials, P->irs,
+                                                                              d.krylov_tol, d.inner_tol,
                                                                               d.refine_maxiter, none, 0));
             const float *dv32 = dinv ? P->dinv32 : nullptr;
             for (int r = 0; r <= d.refine_maxiter && rc == WSPM_OK; ++r) {
                 if ((rc = read_flag(&P->irs->done, st, &flag, pinned)) != WSPM_OK || flag) break;
                 inner_cg_enqueue(A, d, P, dv32, st);
-                ir_correct_kernel<<<nb, kBlock, 0, st>>>(n, d.x, P->x32);
                 WSPM_WIDTH_DISPATCH(A.max_width,
-                                    ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.x, P->r64,
-                                                                                  d.dinv, nullptr, P->partials, P->irs,
-                                                                                  P->cg32.st, 0, d.krylov_tol,
-                                                                                  d.inner_tol, d.refine_maxiter, none,
-                                                                                  0));
+                                    ir_update_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, vec, P->x32, d.x, P->r64,
+                                                                                P->partials, P->irs, P->cg32.st,
+                                                                                d.krylov_tol, d.inner_tol,
+                                                                                d.refine_maxiter, none, 0));
             }
             irs = P->irs;
         } else {
