@@ -342,7 +342,10 @@ def test_picard_engine_test3d_golden(solver):
         np.testing.assert_allclose(res["pressure_head"][s], g["pressure_head"][k], rtol=1e-8, atol=1e-8)
 
 
-def test_mixed_precision_refinement_reaches_fp64_residual():
+@pytest.mark.parametrize("layout", ["auto", "sell"])
+def test_mixed_precision_refinement_reaches_fp64_residual(layout):
+    """DIA (auto): the inner FP32 solves use the pipelined CG kernel; SELL: the single-reduction kernel.  Both
+    reach the FP64 residual and the FP64 path's Picard iterations."""
     from wspm_b200.device import DeviceMesh, merge_dirichlet, spmv
     from wspm_b200.engine import PicardEngine
     pts, tri = mesh.structured_triangles(96, 1.0)
@@ -351,7 +354,8 @@ def test_mixed_precision_refinement_reaches_fp64_residual():
     top = np.where(pts[:, 1] == 1.0)[0]
     bc = merge_dirichlet(len(pts), [(top, -0.1)])
     phi = opic.VG_UNIT_PHI[:5] + (1.0,)
-    dm = DeviceMesh(pts, tri)
+    dm = DeviceMesh(pts, tri, layout=layout)
+    assert (dm.pattern.n_diags > 0) == (layout == "auto")
     out = {}
     for mixed in (False, True):
         eng = PicardEngine(dm, "vg", phi, Ks_elem=Ks, bc_val=bc, solver="cg", precond="jacobi", krylov_tol=1e-8,
