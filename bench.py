@@ -434,6 +434,7 @@ def run_ensemble(args):
                        else "single GPU"},
             "scaling": "strong",
             "batched": {"seconds": t_batch, "picard_its": int(its_all.sum()), "block_threads": tuned,
+                        "cluster_size": ens.cluster_size,
                         "autotune_ms": getattr(ens, "timing", {})},
             "sequential": {"seconds": t_seq, "value": dofits_seq / t_seq},
             "speedup_vs_sequential": (dofits / t_batch) / (dofits_seq / t_seq)}

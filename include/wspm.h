@@ -340,10 +340,12 @@ typedef struct wspm_ensemble {
     int32_t *its, *kits, *status;  /* [n_domains] last step's Picard its, Krylov its, status */
     double *err;               /* [n_domains] last step's Picard error       */
     uint32_t *queue;           /* device word, zeroed by the call            */
+    int32_t cluster_size;      /* CTAs per domain (thread-block cluster): 0 or 1, 2, 4, 8 */
 } wspm_ensemble;
 
 int64_t wspm_ensemble_workspace_doubles(int32_t n_rows, int64_t nnz_padded);
-/* block_threads: CTA size (128, 256 or 512; 0 = 512).                          */
+/* block_threads: CTA size (128, 256 or 512; 0 = 512); ens->cluster_size CTAs
+ * (one thread-block cluster) share each domain.                                */
 int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
                        int32_t block_threads, void *stream);
 

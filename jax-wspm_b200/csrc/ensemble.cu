@@ -13,6 +13,16 @@
 // cap.  The assembly walks each row's incident elements in ascending element
 // id, as the single-domain row kernel does, so a domain's matrix is bitwise
 // the matrix the single-domain path assembles for it.
+//
+// With a cluster size CS > 1 a domain is taken by a thread-block cluster of CS
+// CTAs (one per SM): CTA rank c owns the c-th slice of the domain's rows, the
+// phases that read other slices (soil -> assembly, p -> SpMV, h_m -> residual)
+// are separated by hardware cluster barriers, and every reduction sums the
+// CTAs' partials through distributed shared memory in rank order, so all CTAs
+// of the cluster hold bitwise identical scalars and take the same branches.
+// This spreads the largest domains, which bound the step, over CS SMs.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "soil.cuh"
 #include "krylov.cuh"
@@ -44,14 +54,42 @@ struct EnsArgs {
     unsigned int *queue;
 };
 
-// Block-wide sums of NV values, broadcast to every thread (two block barriers).
-template <int NV>
-__device__ __forceinline__ void block_allsum(double (&v)[NV]) {
+// Barrier over the CTAs that share a domain (the block, or the cluster).
+template <int CS>
+__device__ __forceinline__ void domain_sync() {
+    if constexpr (CS == 1) __syncthreads();
+    else cooperative_groups::this_cluster().sync();
+}
+
+// Sums of NV values over the domain's CTAs, broadcast to every thread.  CS > 1:
+// each CTA publishes its block sum in shared memory, one cluster barrier, then
+// thread j of every CTA adds component j over the ranks in rank order.  The
+// published slots alternate between two buffers: a CTA rewrites a buffer only
+// two sums later, after a cluster barrier that every CTA reaches once it has
+// read that buffer.
+template <int CS, int NV>
+__device__ __forceinline__ void domain_allsum(double (&v)[NV], int &parity) {
     __shared__ double bc[NV];
+    __shared__ double cpart[2][NV];
     block_sum<double, NV>(v);
-    if (threadIdx.x == 0) {
+    if constexpr (CS == 1) {
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int j = 0; j < NV; ++j) bc[j] = v[j];
+            for (int j = 0; j < NV; ++j) bc[j] = v[j];
+        }
+    } else {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) cpart[parity][j] = v[j];
+        }
+        cl.sync();
+        if (threadIdx.x < NV) {
+            double t = 0.0;
+            for (int r = 0; r < CS; ++r) t += *cl.map_shared_rank(&cpart[parity][threadIdx.x], r);
+            bc[threadIdx.x] = t;
+        }
+        parity ^= 1;
     }
     __syncthreads();
 #pragma unroll
@@ -103,7 +141,9 @@ __device__ __forceinline__ void ens_assemble_row(const EnsArgs &a, const Sell &A
             if (a.Ks_elem) Kbar *= a.Ks_elem[e];
             const double kd = Kbar * detJ;
             const double Ml = a.mc[li] * detJ;
-            const double g0 = G[0][li], g1 = G[1][li];
+            // column li of G by selects (an indexed register array would live in local memory)
+            const double g0 = li == 0 ? G[0][0] : (li == 1 ? G[0][1] : G[0][2]);
+            const double g1 = li == 0 ? G[1][0] : (li == 1 ? G[1][1] : G[1][2]);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 double gg = fma(g0, G[0][j], 0.0);
@@ -142,10 +182,12 @@ __device__ __forceinline__ double ens_row_dot(const Sell &A, const double *vals,
     return acc;
 }
 
-template <int MW>
+template <int MW, int CS>
 __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
     extern __shared__ double acc_sm[];   // [MW][blockDim.x]
     __shared__ int s_j;
+    int par = 0;                         // buffer parity of domain_allsum
+    const int rank = CS == 1 ? 0 : (int)cooperative_groups::this_cluster().block_rank();
     const int TB = blockDim.x;
     const Sell A = a.A;
     double *acc = acc_sm + threadIdx.x;
@@ -153,14 +195,19 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
     double *const p = a.p, *const q = a.q;
     const double *const vals = a.vals, *const dinv = a.dinv, *const rhs = a.rhs;
     for (;;) {
-        if (threadIdx.x == 0) s_j = (int)atomicAdd(a.queue, 1u);
-        __syncthreads();
-        const int j = s_j;
-        __syncthreads();
+        if (rank == 0 && threadIdx.x == 0) s_j = (int)atomicAdd(a.queue, 1u);
+        domain_sync<CS>();
+        int j;
+        if constexpr (CS == 1) j = s_j;
+        else j = *cooperative_groups::this_cluster().map_shared_rank(&s_j, 0);
+        domain_sync<CS>();                                // rank 0 rewrites s_j only after every rank read it
         if (j >= a.n_domains) break;
         const int d = a.order[j];
         if (!(a.t[d] < a.tmax)) continue;                 // finished domain: masked out
-        const int n0 = (int)a.node_off[d], n1 = (int)a.node_off[d + 1];
+        // this CTA's slice [n0, n1) of the domain's rows
+        const int d0 = (int)a.node_off[d], d1 = (int)a.node_off[d + 1];
+        const int slice = (d1 - d0 + CS - 1) / CS;
+        const int n0 = min(d1, d0 + rank * slice), n1 = min(d1, n0 + slice);
         SoilParams sp;
         sp.model = WSPM_SOIL_VAN_GENUCHTEN;
         for (int k = 0; k < 6; ++k) sp.p[k] = a.phi[6 * d + k];
@@ -172,7 +219,7 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
             a.theta_n[i] = th;
             hm[i] = hn[i];
         }
-        __syncthreads();
+        domain_sync<CS>();
         int it = 0, kits = 0, status = WSPM_OK;
         double err = __longlong_as_double(0x7ff0000000000000LL);   // +inf
         while (it < a.picard_maxiter && !(err < a.picard_tol)) {
@@ -183,7 +230,7 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
                 a.K[i] = k;
                 a.theta_m[i] = th;
             }
-            __syncthreads();
+            domain_sync<CS>();                            // K of the slice's neighbours
             for (int i = n0 + threadIdx.x; i < n1; i += TB) ens_assemble_row<MW>(a, A, i, inv_dt, acc, TB);
             __syncthreads();
             // ---- Jacobi-CG from x0 = h_m (textbook recurrences, stop on ||r|| <= tol ||b||)
@@ -199,7 +246,7 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
                 v3[1] += ri * ri;
                 v3[2] += rhs[i] * rhs[i];
             }
-            block_allsum<3>(v3);
+            domain_allsum<CS, 3>(v3, par);
             double gamma = v3[0], rr = v3[1];
             const double atol2 = a.krylov_tol * a.krylov_tol * v3[2];
             int k = 0;
@@ -210,7 +257,7 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
                     q[i] = qi;
                     v1[0] += p[i] * qi;
                 }
-                block_allsum<1>(v1);
+                domain_allsum<CS, 1>(v1, par);
                 const double alpha = gamma / v1[0];
                 double v2[2] = {0.0, 0.0};
                 for (int i = n0 + threadIdx.x; i < n1; i += TB) {
@@ -222,12 +269,12 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
                     v2[0] += ri * zi;
                     v2[1] += ri * ri;
                 }
-                block_allsum<2>(v2);
+                domain_allsum<CS, 2>(v2, par);
                 const double beta = v2[0] / gamma;
                 gamma = v2[0];
                 rr = v2[1];
                 for (int i = n0 + threadIdx.x; i < n1; i += TB) p[i] = fma(beta, p[i], z[i]);
-                __syncthreads();
+                domain_sync<CS>();                        // p of the neighbouring slices for the next SpMV
                 ++k;
                 if (!isfinite(rr) || !isfinite(alpha)) break;
             }
@@ -239,16 +286,16 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
                 ve[0] += dx * dx;
                 ve[1] += x[i] * x[i];
             }
-            block_allsum<2>(ve);
+            domain_allsum<CS, 2>(ve, par);
             err = a.picard_relative ? sqrt(ve[0]) / sqrt(ve[1]) : sqrt(ve[0]);
             for (int i = n0 + threadIdx.x; i < n1; i += TB) hm[i] = x[i];
-            __syncthreads();
+            domain_sync<CS>();
             ++it;
             if (!isfinite(err)) { status = WSPM_NAN; break; }
         }
         if (status == WSPM_OK && !(err < a.picard_tol)) status = WSPM_MAXITER;
         for (int i = n0 + threadIdx.x; i < n1; i += TB) hn[i] = hm[i];
-        if (threadIdx.x == 0) {
+        if (rank == 0 && threadIdx.x == 0) {
             a.its[d] = it;
             a.kits[d] = kits;
             a.status[d] = status;
@@ -260,6 +307,36 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
         }
         __syncthreads();
     }
+}
+
+// One CTA (CS = 1) or one cluster of CS CTAs per domain at a time, as many
+// CTAs as fit on the GPU (a whole number of clusters), at most one domain each.
+template <int MW, int CS>
+static cudaError_t ensemble_launch(const EnsArgs &a, int TB, int sms, int n_domains, cudaStream_t st) {
+    const int mw = MW > 0 ? MW : 64;
+    const size_t smem = (size_t)mw * TB * sizeof(double);
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024)
+        e = cudaFuncSetAttribute(ensemble_step_kernel<MW, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ensemble_step_kernel<MW, CS>, TB, smem);
+    if (e != cudaSuccess) return e;
+    int clusters = sms * (per > 0 ? per : 1) / CS;
+    if (clusters > n_domains) clusters = n_domains;
+    if (clusters < 1) clusters = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(clusters * CS);
+    cfg.blockDim = dim3(TB);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, ensemble_step_kernel<MW, CS>, a);
 }
 
 }  // namespace wspm
@@ -282,6 +359,9 @@ extern "C" int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat
     if (ens->work_doubles < wspm_ensemble_workspace_doubles(pat->n_rows, pat->nnz_padded)) return WSPM_BAD_ARG;
     const int TB = block_threads == 0 ? 512 : block_threads;
     if (TB != 128 && TB != 256 && TB != 512) return WSPM_BAD_ARG;
+    if (ens->cluster_size != 0 && ens->cluster_size != 1 && ens->cluster_size != 2 && ens->cluster_size != 4 &&
+        ens->cluster_size != 8)
+        return WSPM_BAD_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     EnsArgs a;
     a.A = make_sell(pat);
@@ -310,22 +390,13 @@ extern "C" int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int cs = ens->cluster_size == 0 ? 1 : ens->cluster_size;
     cudaError_t e = cudaSuccess;
     WSPM_WIDTH_DISPATCH(pat->max_width, {
-        const int mw = MW > 0 ? MW : 64;
-        const size_t smem = (size_t)mw * TB * sizeof(double);
-        if (smem > 48 * 1024)
-            e = cudaFuncSetAttribute(ensemble_step_kernel<MW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem);
-        int per = 0;
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ensemble_step_kernel<MW>, TB, smem);
-        if (e == cudaSuccess) {
-            int grid = sms * (per > 0 ? per : 1);
-            if (grid > ens->n_domains) grid = ens->n_domains;
-            ensemble_step_kernel<MW><<<grid, TB, smem, st>>>(a);
-            e = cudaGetLastError();
-        }
+        if (cs == 1) e = ensemble_launch<MW, 1>(a, TB, sms, ens->n_domains, st);
+        else if (cs == 2) e = ensemble_launch<MW, 2>(a, TB, sms, ens->n_domains, st);
+        else if (cs == 4) e = ensemble_launch<MW, 4>(a, TB, sms, ens->n_domains, st);
+        else e = ensemble_launch<MW, 8>(a, TB, sms, ens->n_domains, st);
     });
     return e == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }

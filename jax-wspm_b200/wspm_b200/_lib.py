@@ -65,7 +65,7 @@ class WspmEnsemble(ctypes.Structure):
                 ("lambda_red", c_double),
                 ("h_n", c_void_p), ("work", c_void_p), ("work_doubles", c_int64), ("dt", c_void_p), ("t", c_void_p),
                 ("its", c_void_p), ("kits", c_void_p), ("status", c_void_p), ("err", c_void_p),
-                ("queue", c_void_p)]
+                ("queue", c_void_p), ("cluster_size", c_int32)]
 
 
 class WspmLevels(ctypes.Structure):

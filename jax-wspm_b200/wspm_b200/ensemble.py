@@ -5,12 +5,13 @@ an ensemble there is a Python loop over solver instances.  ``Ensemble`` puts
 the domains on the diagonal of one mesh (node and element ids offset per
 domain, SELL-32 pattern over the union) and ``wspm_ensemble_step`` advances
 every domain still below ``tmax`` by one implicit step in a single launch:
-each CTA takes the next domain (largest first), runs its Picard loop with its
-own soil parameters, Dirichlet values and dt, and adapts that dt.  Domains that
-reached ``tmax`` are masked out of later launches.
+each CTA -- or each thread-block cluster of ``cluster_size`` CTAs, which spreads
+a domain over that many SMs -- takes the next domain (largest first), runs its
+Picard loop with its own soil parameters, Dirichlet values and dt, and adapts
+that dt.  Domains that reached ``tmax`` are masked out of later launches.
 
-``autotune()`` times one step at each CTA size the kernel supports on a copy of
-the state and keeps the fastest.
+``autotune()`` times one step at each (CTA size, cluster size) the kernel
+supports on a copy of the state and keeps the fastest.
 """
 import ctypes
 import time
@@ -24,6 +25,8 @@ from .device import DeviceMesh
 from .engine import default_rule
 
 BLOCK_SIZES = (128, 256, 512)
+CLUSTER_SIZES = (1, 2, 4, 8)
+LAUNCH_SHAPES = tuple((tb, cs) for cs in CLUSTER_SIZES for tb in ((128, 256, 512) if cs == 1 else (512,)))
 
 
 def partition_domains(work, world):
@@ -128,6 +131,7 @@ class Ensemble:
         self.c = e
         self.tmax = float(tmax)
         self.block_threads = 512
+        self.cluster_size = 1
 
     def set_state(self, h0):
         """Initial head: one array over all nodes, or a scalar."""
@@ -142,6 +146,7 @@ class Ensemble:
 
     def launch(self, stream=None):
         st = stream if stream is not None else torch.cuda.current_stream()
+        self.c.cluster_size = int(self.cluster_size)
         check("ensemble_step", lib.wspm_ensemble_step(ctypes.byref(self.dm.c_mesh), ctypes.byref(self.dm.c_pat),
                                                        ctypes.byref(self.c), int(self.block_threads),
                                                        ctypes.c_void_p(st.cuda_stream)))
@@ -156,14 +161,15 @@ class Ensemble:
         return {"active": active, "iterations": self.its.cpu().numpy(), "krylov_iterations": self.kits.cpu().numpy(),
                 "status": self.status.cpu().numpy(), "error": self.err.cpu().numpy()}
 
-    def autotune(self, sizes=BLOCK_SIZES):
-        """Pick the CTA size with the fastest step on a copy of the current state (state restored)."""
+    def autotune(self, shapes=LAUNCH_SHAPES):
+        """Pick the (CTA size, cluster size) with the fastest step on a copy of the current state (state
+        restored); returns the CTA size and sets ``block_threads`` and ``cluster_size``."""
         saved = [x.clone() for x in (self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err)]
         timing = {}
-        for tb in sizes:
+        for tb, cs in shapes:
             for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
                 x.copy_(s)
-            self.block_threads = tb
+            self.block_threads, self.cluster_size = tb, cs
             self.launch()                       # warm
             for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
                 x.copy_(s)
@@ -172,11 +178,11 @@ class Ensemble:
             self.launch()
             e1.record()
             torch.cuda.synchronize()
-            timing[tb] = e0.elapsed_time(e1)
+            timing[(tb, cs)] = e0.elapsed_time(e1)
         for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
             x.copy_(s)
-        self.block_threads = min(timing, key=timing.get)
-        self.timing = timing
+        self.block_threads, self.cluster_size = min(timing, key=timing.get)
+        self.timing = {f"{tb}x{cs}": t for (tb, cs), t in timing.items()}
         return self.block_threads
 
     def run(self, max_steps=None):

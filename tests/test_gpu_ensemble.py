@@ -31,13 +31,17 @@ def _domains(sizes, seed=0):
     return out
 
 
-def test_ensemble_matches_single_domain_engines():
+@pytest.mark.parametrize("cluster_size", [1, 2, 4])
+def test_ensemble_matches_single_domain_engines(cluster_size):
+    """Each domain, whether one CTA or a cluster of 2 / 4 CTAs runs it, takes exactly the Picard iterations and the
+    dt sequence of its own single-domain engine; heads agree to 1e-8."""
     from wspm_b200.device import DeviceMesh
     from wspm_b200.engine import PicardEngine
     from wspm_b200.ensemble import Ensemble
     doms = _domains([8, 12, 16, 10, 20, 6])
     steps = 4
     ens = Ensemble(doms, dt0=1e-3, tmax=1.0, krylov_tol=1e-10, krylov_maxiter=1000)
+    ens.cluster_size = cluster_size
     ens.set_state(-1.0)
     recs = [ens.step() for _ in range(steps)]
     for d, (pts, tri, phi, bc, _) in enumerate(doms):
