@@ -133,35 +133,6 @@ __global__ void step_finish_kernel(int n, const double *__restrict__ h_m, double
 // ---- mixed precision: FP32 CG corrections inside FP64 refinement ----------
 // ir state (KrylovState): bs, atol2, rr, k (refinement iterations), steps (inner
 // iterations summed), status.
-//
-// (A y) for rows i and i + 1 (i even).  DIA with 16-byte aligned values: one
-// 16-byte load per diagonal for both rows; otherwise two row dots.  Each row
-// accumulates in diagonal order with fma, like sell_row_dot, so both paths
-// give the same bits.
-template <int MW, typename Y>
-__device__ __forceinline__ void ir_rows2(const Sell &A, const double *__restrict__ vals, bool vec, int i,
-                                         const Y *__restrict__ y, double (&acc)[2]) {
-    if (vec) {
-        const int nd = A.n_diags, last = A.n_rows - 1;
-        acc[0] = acc[1] = 0.0;
-#pragma unroll
-        for (int k = 0; k < MW; ++k) {
-            if (k < nd) {
-                const double2 v = __ldg(reinterpret_cast<const double2 *>(vals + (int64_t)k * A.ld + i));
-                const int o = __ldg(A.diag_off + k);
-                int c0 = i + o, c1 = i + 1 + o;
-                c0 = c0 < 0 ? 0 : (c0 > last ? last : c0);
-                c1 = c1 < 0 ? 0 : (c1 > last ? last : c1);
-                acc[0] = fma(v.x, (double)y[c0], acc[0]);
-                acc[1] = fma(v.y, (double)y[c1], acc[1]);
-            }
-        }
-    } else {
-        acc[0] = sell_row_dot<double, MW>(A, vals, i, [&](int c) { return (double)y[c]; });
-        acc[1] = i + 1 < A.n_rows ? sell_row_dot<double, MW>(A, vals, i + 1, [&](int c) { return (double)y[c]; })
-                                  : 0.0;
-    }
-}
 
 // Reduction tail shared by the two refinement kernels: tot = (r.r, b.b); sets
 // the next inner tolerance, the continue flag and the graph condition.
@@ -195,7 +166,7 @@ __device__ __forceinline__ void ir_decide(const double (&tot)[2], KrylovState *i
 // Start of the refinement loop: x = x0, r = b - A x0 (FP64), the FP32 copy of
 // 1/diag, and the loop state.
 template <int MW>
-__global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const double *__restrict__ vals, bool vec,
+__global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const double *__restrict__ vals,
                                                              const double *__restrict__ b,
                                                              const double *__restrict__ x0, double *x, double *r,
                                                              const double *__restrict__ dinv, float *dinv32,
@@ -203,22 +174,13 @@ __global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const doubl
                                                              double inner_floor, int maxit,
                                                              cudaGraphConditionalHandle cond, int use_cond) {
     double v[2] = {0.0, 0.0};
-    const int n = A.n_rows;
-    for (int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 2 * gridDim.x * blockDim.x) {
-        double acc[2];
-        ir_rows2<MW, double>(A, vals, vec, i, x0, acc);
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int iq = i + q;
-            if (iq < n) {
-                const double ri = b[iq] - acc[q];
-                r[iq] = ri;
-                x[iq] = x0[iq];
-                if (dinv32) dinv32[iq] = (float)dinv[iq];
-                v[0] += ri * ri;
-                v[1] += b[iq] * b[iq];
-            }
-        }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
+        const double ri = b[i] - sell_row_dot<double, MW>(A, vals, i, [&](int c) { return x0[c]; });
+        r[i] = ri;
+        x[i] = x0[i];
+        if (dinv32) dinv32[i] = (float)dinv[i];
+        v[0] += ri * ri;
+        v[1] += b[i] * b[i];
     }
     if (publish_partials<double, 2>(v, partials, &irs->ticket[0])) {
         double tot[2];
@@ -230,37 +192,23 @@ __global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const doubl
 // After an FP32 correction d: x += d and r -= A d (FP64; equal to b - A x up to
 // FP64 rounding, without re-reading b and the previous x).
 template <int MW>
-__global__ void __launch_bounds__(kBlock) ir_update_kernel(Sell A, const double *__restrict__ vals, bool vec,
+__global__ void __launch_bounds__(kBlock) ir_update_kernel(Sell A, const double *__restrict__ vals,
                                                            const float *__restrict__ d, double *x, double *r,
                                                            double *partials, KrylovState *irs,
                                                            const KrylovState *inner, double tol, double inner_floor,
                                                            int maxit, cudaGraphConditionalHandle cond, int use_cond) {
     double v[2] = {0.0, 0.0};
-    const int n = A.n_rows;
-    for (int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x); i < n; i += 2 * gridDim.x * blockDim.x) {
-        double acc[2];
-        ir_rows2<MW, float>(A, vals, vec, i, d, acc);
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int iq = i + q;
-            if (iq < n) {
-                const double ri = r[iq] - acc[q];
-                r[iq] = ri;
-                x[iq] += (double)d[iq];
-                v[0] += ri * ri;
-            }
-        }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
+        const double ri = r[i] - sell_row_dot<double, MW>(A, vals, i, [&](int c) { return (double)d[c]; });
+        r[i] = ri;
+        x[i] += (double)d[i];
+        v[0] += ri * ri;
     }
     if (publish_partials<double, 2>(v, partials, &irs->ticket[0])) {
         double tot[2];
         final_sum<double, 2>(partials, tot, &irs->ticket[0]);
         if (threadIdx.x == 0) ir_decide(tot, irs, inner, 0, tol, inner_floor, maxit, cond, use_cond);
     }
-}
-
-// 16-byte aligned DIA values take the paired-row path of the refinement kernels
-static bool ir_vec(const Sell &A, const double *vals) {
-    return A.n_diags > 0 && ((uintptr_t)vals % 16) == 0 && (A.ld % 2) == 0;
 }
 
 struct PicardPlan {
@@ -353,9 +301,8 @@ static int build_picard_graph(PicardPlan *P) {
         if (d.mixed) {
             cudaGraphConditionalHandle hir;
             make_cond_handle(bs, &hir);
-            const bool vec = ir_vec(A, d.vals);
             WSPM_WIDTH_DISPATCH(A.max_width,
-                                ir_residual_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, vec, d.rhs, d.h_m, d.x, P->r64,
+                                ir_residual_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, d.rhs, d.h_m, d.x, P->r64,
                                                                               d.dinv, P->dinv32, P->partials, P->irs,
                                                                               d.krylov_tol, d.inner_tol,
                                                                               d.refine_maxiter, hir, 1));
@@ -363,7 +310,7 @@ static int build_picard_graph(PicardPlan *P) {
                 const float *dv32 = dinv ? P->dinv32 : nullptr;
                 inner_cg_enqueue(A, d, P, dv32, ibs);
                 WSPM_WIDTH_DISPATCH(A.max_width,
-                                    ir_update_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, vec, P->x32, d.x, P->r64,
+                                    ir_update_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, P->x32, d.x, P->r64,
                                                                                  P->partials, P->irs, P->cg32.st,
                                                                                  d.krylov_tol, d.inner_tol,
                                                                                  d.refine_maxiter, hir, 1));
@@ -447,9 +394,8 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                           st);
         const KrylovState *ks = nullptr, *irs = nullptr;
         if (d.mixed) {
-            const bool vec = ir_vec(A, d.vals);
             WSPM_WIDTH_DISPATCH(A.max_width,
-                                ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, vec, d.rhs, d.h_m, d.x, P->r64,
+                                ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.h_m, d.x, P->r64,
                                                                               d.dinv, P->dinv32, P->partials, P->irs,
                                                                               d.krylov_tol, d.inner_tol,
                                                                               d.refine_maxiter, none, 0));
@@ -458,7 +404,7 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                 if ((rc = read_flag(&P->irs->done, st, &flag, pinned)) != WSPM_OK || flag) break;
                 inner_cg_enqueue(A, d, P, dv32, st);
                 WSPM_WIDTH_DISPATCH(A.max_width,
-                                    ir_update_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, vec, P->x32, d.x, P->r64,
+                                    ir_update_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, P->x32, d.x, P->r64,
                                                                                 P->partials, P->irs, P->cg32.st,
                                                                                 d.krylov_tol, d.inner_tol,
                                                                                 d.refine_maxiter, none, 0));

@@ -31,9 +31,9 @@ def _domains(sizes, seed=0):
     return out
 
 
-@pytest.mark.parametrize("cluster_size", [1, 2, 4])
+@pytest.mark.parametrize("cluster_size", [1, 2, 4, 8])
 def test_ensemble_matches_single_domain_engines(cluster_size):
-    """Each domain, whether one CTA or a cluster of 2 / 4 CTAs runs it, takes exactly the Picard iterations and the
+    """Each domain, whether one CTA or a cluster of 2, 4 or 8 CTAs runs it, takes exactly the Picard iterations and the
     dt sequence of its own single-domain engine; heads agree to 1e-8."""
     from wspm_b200.device import DeviceMesh
     from wspm_b200.engine import PicardEngine
