@@ -90,6 +90,44 @@ typedef struct wspm_pattern {
     const int32_t *diag_offsets;
 } wspm_pattern;
 
+/* Host-side pattern builder (replaces the reference's per-assembly COO fill +
+ * BCOO.sum_duplicates, src/numerics/assembly_re_v2.py:114-152 and
+ * assembly_re_3D.py:118-151, by a pattern built once per mesh).
+ * elements: [n_elems * nv] 0-based vertex ids (nv = 3 triangles, 4 tetrahedra);
+ * extra_pairs: [n_extra * 2] node pairs that need matrix slots although no
+ * element holds both (boundary edges), added in both directions, or NULL.
+ * layout: WSPM_LAYOUT_AUTO (DIA when every row's column offsets belong to one
+ * set of at most 16, else SELL-32), _SELL or _DIA.  On success *out holds host
+ * arrays (free with wspm_pattern_free) from which a wspm_pattern is made by
+ * uploading them to the device.  WSPM_BAD_ARG for ids out of range or a node
+ * in no element; WSPM_UNSUPPORTED for more than 63 diagonals (DIA) or rows
+ * longer than 63 (SELL).  Single-threaded, O(E nv^2 log).                  */
+#define WSPM_LAYOUT_AUTO 0
+#define WSPM_LAYOUT_SELL 1
+#define WSPM_LAYOUT_DIA  2
+typedef struct wspm_pattern_host {
+    int32_t n_rows, n_slices, max_width, max_inc, n_diags, layout;
+    int64_t nnz;              /* unique (row, col) pairs                     */
+    int64_t nnz_padded;       /* storage slots                               */
+    int64_t n_inc;            /* incidence slots (inc_ptr[n_slices])         */
+    int64_t ld;               /* DIA: 32 * n_slices; SELL: 0                 */
+    int64_t *csr_indptr;      /* [n_rows + 1]                                */
+    int32_t *csr_indices;     /* [nnz], ascending per row                    */
+    int64_t *sell_index;      /* [nnz] CSR entry -> storage slot             */
+    int64_t *slice_ptr;       /* [n_slices + 1]                              */
+    int32_t *slice_width;     /* [n_slices]                                  */
+    int32_t *cols;            /* [nnz_padded]                                */
+    int32_t *diag_pos;        /* [n_rows]                                    */
+    int32_t *diag_offsets;    /* [n_diags]                                   */
+    int64_t *inc_ptr;         /* [n_slices + 1]                              */
+    int32_t *inc_width;       /* [n_slices]                                  */
+    int32_t *inc_elem;        /* [n_inc], -1 = padding                       */
+    uint32_t *inc_slots;      /* [n_inc], packed as in wspm_pattern          */
+} wspm_pattern_host;
+int wspm_pattern_build(const int64_t *elements, int64_t n_elems, int32_t nv, int32_t n_nodes,
+                       const int64_t *extra_pairs, int64_t n_extra, int32_t layout, wspm_pattern_host **out);
+void wspm_pattern_free(wspm_pattern_host *p);
+
 /* ---- soil models -------------------------------------------------------- */
 /* van_genuchten_model, src/models/van_genuchten.py:9-47 (vmapped over nodes).
  * phi = {alpha, theta_s, theta_r, n, m, Ks} (host array, 6 doubles).

@@ -68,6 +68,20 @@ class WspmEnsemble(ctypes.Structure):
                 ("queue", c_void_p), ("cluster_size", c_int32)]
 
 
+def _ptr(t):
+    return ctypes.POINTER(t)
+
+
+class WspmPatternHost(ctypes.Structure):
+    _fields_ = [("n_rows", c_int32), ("n_slices", c_int32), ("max_width", c_int32), ("max_inc", c_int32),
+                ("n_diags", c_int32), ("layout", c_int32), ("nnz", c_int64), ("nnz_padded", c_int64),
+                ("n_inc", c_int64), ("ld", c_int64),
+                ("csr_indptr", _ptr(c_int64)), ("csr_indices", _ptr(c_int32)), ("sell_index", _ptr(c_int64)),
+                ("slice_ptr", _ptr(c_int64)), ("slice_width", _ptr(c_int32)), ("cols", _ptr(c_int32)),
+                ("diag_pos", _ptr(c_int32)), ("diag_offsets", _ptr(c_int32)), ("inc_ptr", _ptr(c_int64)),
+                ("inc_width", _ptr(c_int32)), ("inc_elem", _ptr(c_int32)), ("inc_slots", _ptr(ctypes.c_uint32))]
+
+
 class WspmLevels(ctypes.Structure):
     _fields_ = [("n_levels", c_int32), ("level_ptr", c_void_p), ("rows", c_void_p)]
 
@@ -127,6 +141,9 @@ _SIGS = {
     "wspm_picard_step": (c_int32, [c_void_p, c_void_p]),
     "wspm_picard_step_host": (c_int32, [c_void_p, c_void_p]),
     "wspm_picard_destroy": (c_int32, [c_void_p]),
+    "wspm_pattern_build": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_int64, c_int32,
+                                     P(P(WspmPatternHost))]),
+    "wspm_pattern_free": (None, [P(WspmPatternHost)]),
     "wspm_version": (ctypes.c_char_p, []),
     "wspm_status_string": (ctypes.c_char_p, [c_int32]),
 }

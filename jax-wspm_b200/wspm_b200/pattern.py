@@ -28,10 +28,78 @@ DIA_MAX = 16
 class Pattern:
     """Host arrays of a SELL-32 (or DIA) pattern + node->element incidence."""
 
-    def __init__(self, elements, n_nodes, layout="auto", extra_pairs=None):
+    def __init__(self, elements, n_nodes, layout="auto", extra_pairs=None, builder="native"):
         """``extra_pairs`` (k, 2): node pairs that must have matrix slots although no element
         contains both (boundary edges whose end points are not an element edge); both (i, j) and
-        (j, i) are added."""
+        (j, i) are added.  ``builder``: "native" (``wspm_pattern_build`` in libwspm) or "numpy" (the same
+        arrays built with NumPy; kept as the restatement the native builder is tested against)."""
+        if layout not in ("auto", "sell", "dia"):
+            raise ValueError(f"unknown layout {layout!r}")
+        if builder == "native":
+            self._build_native(elements, n_nodes, layout, extra_pairs)
+        elif builder == "numpy":
+            self._build_numpy(elements, n_nodes, layout, extra_pairs)
+        else:
+            raise ValueError(f"unknown builder {builder!r}")
+
+    def _build_native(self, elements, n_nodes, layout, extra_pairs):
+        import ctypes
+        from . import _lib
+        el = np.ascontiguousarray(elements, dtype=np.int64)
+        if el.ndim != 2:
+            raise ValueError("elements must be a 2D array")
+        E, nv = el.shape
+        N = int(n_nodes)
+        ep = np.zeros((0, 2), dtype=np.int64)
+        if extra_pairs is not None and len(extra_pairs):
+            ep = np.ascontiguousarray(np.asarray(extra_pairs, dtype=np.int64).reshape(-1, 2))
+        code = {"auto": 0, "sell": 1, "dia": 2}[layout]
+        out = ctypes.POINTER(_lib.WspmPatternHost)()
+        rc = _lib.lib.wspm_pattern_build(el.ctypes.data_as(ctypes.c_void_p), E, nv, N,
+                                         ep.ctypes.data_as(ctypes.c_void_p) if len(ep) else None, len(ep), code,
+                                         ctypes.byref(out))
+        if rc == _lib.WSPM_UNSUPPORTED:
+            raise ValueError("pattern not representable: more than 63 diagonals (DIA) or rows longer than 63 "
+                             "(SELL-32)")
+        if rc != _lib.WSPM_OK:
+            raise ValueError("invalid mesh: element ids out of bounds or nodes that belong to no element")
+        try:
+            h = out.contents
+
+            def arr(ptr, n):
+                return np.ctypeslib.as_array(ptr, shape=(int(n),)).copy()
+            self.n_rows, self.n_elems, self.nv = N, E, nv
+            self.nnz, self.n_slices, self.nnz_padded = int(h.nnz), int(h.n_slices), int(h.nnz_padded)
+            self.layout = "dia" if h.layout == 2 else "sell"
+            self.ld = int(h.ld)
+            self.max_width, self.max_inc, self.n_diags = int(h.max_width), int(h.max_inc), int(h.n_diags)
+            ns = self.n_slices
+            self.csr_indptr = arr(h.csr_indptr, N + 1)
+            self.csr_indices = arr(h.csr_indices, self.nnz)
+            self.sell_index = arr(h.sell_index, self.nnz)
+            self.slice_ptr = arr(h.slice_ptr, ns + 1)
+            self.slice_width = arr(h.slice_width, ns)
+            self.cols = arr(h.cols, self.nnz_padded)
+            self.diag_pos = arr(h.diag_pos, N)
+            self.diag_offsets = arr(h.diag_offsets, self.n_diags) if self.n_diags else np.zeros(0, dtype=np.int32)
+            self.inc_ptr = arr(h.inc_ptr, ns + 1)
+            self.inc_width = arr(h.inc_width, ns)
+            self.inc_elem = arr(h.inc_elem, h.n_inc)
+            self.inc_slots = arr(h.inc_slots, h.n_inc)
+        finally:
+            _lib.lib.wspm_pattern_free(out)
+
+    def _slot(self, rows, cols_):
+        if self.layout == "dia":
+            return np.searchsorted(self.diag_offsets.astype(np.int64), cols_ - rows)
+        keys = self.__dict__.get("_keys")
+        if keys is None:
+            counts = np.diff(self.csr_indptr)
+            keys = np.repeat(np.arange(self.n_rows, dtype=np.int64), counts) * self.n_rows + self.csr_indices
+            self._keys = keys
+        return np.searchsorted(keys, rows * self.n_rows + cols_) - self.csr_indptr[rows]
+
+    def _build_numpy(self, elements, n_nodes, layout, extra_pairs):
         el = np.ascontiguousarray(elements, dtype=np.int64)
         E, nv = el.shape
         N = int(n_nodes)
@@ -57,8 +125,6 @@ class Pattern:
         ns = (N + SLICE - 1) // SLICE
         self.n_slices = ns
         offs = np.unique(c - r)
-        if layout not in ("auto", "sell", "dia"):
-            raise ValueError(f"unknown layout {layout!r}")
         self.layout = "dia" if (layout == "dia" or (layout == "auto" and offs.size <= DIA_MAX)) else "sell"
         if self.layout == "dia":
             if offs.size > 63:
@@ -76,7 +142,6 @@ class Pattern:
             all_i = np.arange(ld, dtype=np.int64)
             self.cols = np.clip(all_i[None, :] + offs[:, None], 0, N - 1).astype(np.int32).ravel()
             self.diag_pos = np.full(N, int(np.searchsorted(offs, 0)), dtype=np.int32)
-            self._slot = lambda rows, cols_: np.searchsorted(offs, cols_ - rows)
         else:
             self.ld = 0
             self.diag_offsets = np.zeros(0, dtype=np.int32)
@@ -102,7 +167,6 @@ class Pattern:
             self.diag_pos = np.empty(N, dtype=np.int32)
             dmask = r == c
             self.diag_pos[r[dmask]] = pos[dmask].astype(np.int32)
-            self._slot = lambda rows, cols_: np.searchsorted(keys, rows * N + cols_) - rowptr[rows]
         self.n_diags = int(self.diag_offsets.size)
         # --- incidence: for each (node, element) in ascending element order
         inc_node = el.ravel()

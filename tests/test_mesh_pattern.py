@@ -119,3 +119,55 @@ def test_loader_errors(tmp_path):
     tf.write_text("1,2,3\n")
     pts, el = mesh.load_csv_mesh(str(pf), str(tf), 2)
     assert el.tolist() == [[0, 1, 2]]
+
+
+ATTRS = ("csr_indptr", "csr_indices", "sell_index", "slice_ptr", "slice_width", "cols", "diag_pos", "diag_offsets",
+         "inc_ptr", "inc_width", "inc_elem", "inc_slots")
+
+
+def _shuffled_triangles(n, seed):
+    """A structured grid with permuted node and element ids: an unstructured-looking mesh (SELL rows)."""
+    pts, tri = mesh.structured_triangles(n, 1.0)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(len(pts))
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    return pts[perm], inv[tri][rng.permutation(len(tri))]
+
+
+@pytest.mark.parametrize("case", ["tri-auto", "tri-sell", "tri-dia", "tet-auto", "tet-sell", "shuffled-auto",
+                                  "extra-pairs"])
+def test_native_pattern_builder_matches_numpy(case):
+    """wspm_pattern_build (libwspm, C++) produces the NumPy builder's arrays element for element, dtypes included."""
+    extra = None
+    if case.startswith("tri"):
+        pts, el = mesh.structured_triangles(13, 1.0)
+    elif case.startswith("tet"):
+        pts, el = mesh.kuhn_tetrahedra(5, 1.0)
+    elif case.startswith("shuffled"):
+        pts, el = _shuffled_triangles(11, 7)
+    else:
+        pts, el = mesh.structured_triangles(9, 1.0)
+        extra = np.array([[0, 20], [5, 77]])
+    layout = case.split("-")[1] if case.split("-")[1] in ("auto", "sell", "dia") else "auto"
+    a = Pattern(el, len(pts), layout=layout, extra_pairs=extra, builder="native")
+    b = Pattern(el, len(pts), layout=layout, extra_pairs=extra, builder="numpy")
+    for k in ("layout", "n_rows", "nnz", "n_slices", "nnz_padded", "ld", "max_width", "max_inc", "n_diags"):
+        assert getattr(a, k) == getattr(b, k), k
+    for k in ATTRS:
+        x, y = getattr(a, k), getattr(b, k)
+        assert x.dtype == y.dtype and np.array_equal(x, y), k
+    if case == "shuffled-auto":
+        assert a.layout == "sell"
+    rows = np.array([0, 3, len(pts) - 1])
+    np.testing.assert_array_equal(a.slot(rows, rows), b.slot(rows, rows))
+
+
+def test_native_pattern_builder_errors():
+    pts, el = mesh.structured_triangles(4, 1.0)
+    with pytest.raises(ValueError):
+        Pattern(el, len(pts) + 1, builder="native")            # a node in no element
+    bad = el.copy()
+    bad[0, 0] = len(pts)
+    with pytest.raises(ValueError):
+        Pattern(bad, len(pts), builder="native")               # id out of range
