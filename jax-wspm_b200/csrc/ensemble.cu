@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(512, 1) ensemble_step_kernel(EnsArgs a) {
 }
 
 // One CTA (CS = 1) or one cluster of CS CTAs per domain at a time, as many
-// CTAs as fit on the GPU (a whole number of clusters), at most one domain each.
+// CTAs (whole clusters) as can be resident at once, at most one per domain.
 template <int MW, int CS>
 static cudaError_t ensemble_launch(const EnsArgs &a, int TB, int sms, int n_domains, cudaStream_t st) {
     const int mw = MW > 0 ? MW : 64;
@@ -336,6 +336,17 @@ static cudaError_t ensemble_launch(const EnsArgs &a, int TB, int sms, int n_doma
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (CS > 1) {
+        // no more clusters than can be resident together: GPCs whose SM count is not a multiple of CS hold
+        // fewer, and a cluster that could only start after another finished would run its domain last
+        int fit = 0;
+        if (cudaOccupancyMaxActiveClusters(&fit, ensemble_step_kernel<MW, CS>, &cfg) == cudaSuccess && fit > 0 &&
+            clusters > fit) {
+            clusters = fit;
+            cfg.gridDim = dim3(clusters * CS);
+        }
+        cudaGetLastError();   // a failed query leaves the grid as it was
+    }
     return cudaLaunchKernelEx(&cfg, ensemble_step_kernel<MW, CS>, a);
 }
 
