@@ -127,6 +127,13 @@ typedef struct wspm_pattern_host {
 int wspm_pattern_build(const int64_t *elements, int64_t n_elems, int32_t nv, int32_t n_nodes,
                        const int64_t *extra_pairs, int64_t n_extra, int32_t layout, wspm_pattern_host **out);
 void wspm_pattern_free(wspm_pattern_host *p);
+/* Level schedule of a triangular sweep over a CSR pattern (host): level[i] =
+ * 1 + the highest level among the rows row i depends on (columns j < i when
+ * lower != 0, j > i otherwise), 0 without dependencies; *n_levels = max + 1.
+ * Used by the level-scheduled sweeps of wspm_precond_apply (the reference's
+ * ilu / ssor, src/solvers/jax_linear_solver.py:91-252, sweeps row by row). */
+int wspm_pattern_levels(const int64_t *indptr, const int32_t *indices, int32_t n_rows, int32_t lower,
+                        int32_t *level, int32_t *n_levels);
 
 /* ---- soil models -------------------------------------------------------- */
 /* van_genuchten_model, src/models/van_genuchten.py:9-47 (vmapped over nodes).

@@ -246,3 +246,25 @@ extern "C" int wspm_pattern_build(const int64_t *elements, int64_t n_elems, int3
         return WSPM_BAD_ARG;
     }
 }
+
+// Level schedule of a triangular sweep: level[i] = 1 + max level of the rows
+// row i depends on (columns j < i for the lower sweep, j > i for the upper
+// one), 0 without dependencies.  Rows of one level can be processed together.
+extern "C" int wspm_pattern_levels(const int64_t *indptr, const int32_t *indices, int32_t n_rows, int32_t lower,
+                                   int32_t *level, int32_t *n_levels) {
+    if (!indptr || !indices || n_rows <= 0 || !level || !n_levels) return WSPM_BAD_ARG;
+    int32_t top = -1;
+    for (int32_t t = 0; t < n_rows; ++t) {
+        const int32_t i = lower ? t : n_rows - 1 - t;
+        int32_t lv = 0;
+        for (int64_t q = indptr[i]; q < indptr[i + 1]; ++q) {
+            const int32_t j = indices[q];
+            if (j < 0 || j >= n_rows) return WSPM_BAD_ARG;
+            if (lower ? j < i : j > i) lv = std::max(lv, level[j] + 1);
+        }
+        level[i] = lv;
+        top = std::max(top, lv);
+    }
+    *n_levels = top + 1;
+    return WSPM_OK;
+}

@@ -144,6 +144,7 @@ _SIGS = {
     "wspm_pattern_build": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_int64, c_int32,
                                      P(P(WspmPatternHost))]),
     "wspm_pattern_free": (None, [P(WspmPatternHost)]),
+    "wspm_pattern_levels": (c_int32, [c_void_p, c_void_p, c_int32, c_int32, c_void_p, P(c_int32)]),
     "wspm_version": (ctypes.c_char_p, []),
     "wspm_status_string": (ctypes.c_char_p, [c_int32]),
 }

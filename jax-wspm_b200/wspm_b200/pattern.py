@@ -204,14 +204,17 @@ class Pattern:
         cache = self.__dict__.setdefault("_levels", {})
         if lower in cache:
             return cache[lower]
-        n, ptr, idx = self.n_rows, self.csr_indptr, self.csr_indices
-        level = np.zeros(n, dtype=np.int64)
-        order = range(n) if lower else range(n - 1, -1, -1)
-        for i in order:
-            c = idx[ptr[i]:ptr[i + 1]]
-            dep = c[c < i] if lower else c[c > i]
-            if dep.size:
-                level[i] = level[dep].max() + 1
+        import ctypes
+        from . import _lib
+        n = self.n_rows
+        ptr = np.ascontiguousarray(self.csr_indptr, dtype=np.int64)
+        idx = np.ascontiguousarray(self.csr_indices, dtype=np.int32)
+        lv = np.empty(n, dtype=np.int32)
+        nl = ctypes.c_int32(0)
+        _lib.check("pattern_levels", _lib.lib.wspm_pattern_levels(
+            ptr.ctypes.data_as(ctypes.c_void_p), idx.ctypes.data_as(ctypes.c_void_p), n, int(bool(lower)),
+            lv.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nl)))
+        level = lv.astype(np.int64)
         rows = np.argsort(level, kind="stable").astype(np.int32)
         counts = np.bincount(level, minlength=int(level.max()) + 1 if n else 0)
         level_ptr = np.zeros(counts.size + 1, dtype=np.int32)

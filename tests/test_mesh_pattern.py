@@ -171,3 +171,20 @@ def test_native_pattern_builder_errors():
     bad[0, 0] = len(pts)
     with pytest.raises(ValueError):
         Pattern(bad, len(pts), builder="native")               # id out of range
+
+
+@pytest.mark.parametrize("lower", [True, False])
+def test_native_level_schedule_matches_row_loop(lower):
+    """wspm_pattern_levels against the row-by-row definition (row i waits for every row it depends on)."""
+    pts, el = _shuffled_triangles(9, 5)
+    P = Pattern(el, len(pts))
+    level_ptr, rows = P.tri_levels(lower)
+    n, ptr, idx = P.n_rows, P.csr_indptr, P.csr_indices
+    level = np.zeros(n, dtype=np.int64)
+    for i in (range(n) if lower else range(n - 1, -1, -1)):
+        c = idx[ptr[i]:ptr[i + 1]]
+        dep = c[c < i] if lower else c[c > i]
+        if dep.size:
+            level[i] = level[dep].max() + 1
+    np.testing.assert_array_equal(rows, np.argsort(level, kind="stable"))
+    np.testing.assert_array_equal(np.diff(level_ptr), np.bincount(level))
