@@ -385,7 +385,7 @@ typedef struct wspm_ensemble {
     int32_t *its, *kits, *status;  /* [n_domains] last step's Picard its, Krylov its, status */
     double *err;               /* [n_domains] last step's Picard error       */
     uint32_t *queue;           /* device word, zeroed by the call            */
-    int32_t cluster_size;      /* CTAs per domain (thread-block cluster): 0 or 1, 2, 4, 8 */
+    int32_t cluster_size;      /* CTAs per domain (thread-block cluster): 0 or 1, 2, 4, 8, 16 (16: where the GPU allows non-portable clusters) */
 } wspm_ensemble;
 
 int64_t wspm_ensemble_workspace_doubles(int32_t n_rows, int64_t nnz_padded);

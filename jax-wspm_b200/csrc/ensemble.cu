@@ -319,6 +319,8 @@ static cudaError_t ensemble_launch(const EnsArgs &a, int TB, int sms, int n_doma
     if (smem > 48 * 1024)
         e = cudaFuncSetAttribute(ensemble_step_kernel<MW, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per = 0;
+    if (e == cudaSuccess && CS > 8)   // above the portable cluster size: opt in (the launch fails where unsupported)
+        e = cudaFuncSetAttribute(ensemble_step_kernel<MW, CS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ensemble_step_kernel<MW, CS>, TB, smem);
     if (e != cudaSuccess) return e;
     int clusters = sms * (per > 0 ? per : 1) / CS;
@@ -347,7 +349,9 @@ static cudaError_t ensemble_launch(const EnsArgs &a, int TB, int sms, int n_doma
         }
         cudaGetLastError();   // a failed query leaves the grid as it was
     }
-    return cudaLaunchKernelEx(&cfg, ensemble_step_kernel<MW, CS>, a);
+    e = cudaLaunchKernelEx(&cfg, ensemble_step_kernel<MW, CS>, a);
+    if (e != cudaSuccess) cudaGetLastError();   // a refused launch (e.g. a cluster size this GPU lacks) is not sticky
+    return e;
 }
 
 }  // namespace wspm
@@ -371,7 +375,7 @@ extern "C" int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat
     const int TB = block_threads == 0 ? 512 : block_threads;
     if (TB != 128 && TB != 256 && TB != 512) return WSPM_BAD_ARG;
     if (ens->cluster_size != 0 && ens->cluster_size != 1 && ens->cluster_size != 2 && ens->cluster_size != 4 &&
-        ens->cluster_size != 8)
+        ens->cluster_size != 8 && ens->cluster_size != 16)
         return WSPM_BAD_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     EnsArgs a;
@@ -407,7 +411,8 @@ extern "C" int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat
         if (cs == 1) e = ensemble_launch<MW, 1>(a, TB, sms, ens->n_domains, st);
         else if (cs == 2) e = ensemble_launch<MW, 2>(a, TB, sms, ens->n_domains, st);
         else if (cs == 4) e = ensemble_launch<MW, 4>(a, TB, sms, ens->n_domains, st);
-        else e = ensemble_launch<MW, 8>(a, TB, sms, ens->n_domains, st);
+        else if (cs == 8) e = ensemble_launch<MW, 8>(a, TB, sms, ens->n_domains, st);
+        else e = ensemble_launch<MW, 16>(a, TB, sms, ens->n_domains, st);
     });
     return e == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }

@@ -25,7 +25,7 @@ from .device import DeviceMesh
 from .engine import default_rule
 
 BLOCK_SIZES = (128, 256, 512)
-CLUSTER_SIZES = (1, 2, 4, 8)
+CLUSTER_SIZES = (1, 2, 4, 8, 16)
 LAUNCH_SHAPES = tuple((tb, cs) for cs in CLUSTER_SIZES for tb in ((128, 256, 512) if cs == 1 else (512,)))
 
 
@@ -170,7 +170,10 @@ class Ensemble:
             for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
                 x.copy_(s)
             self.block_threads, self.cluster_size = tb, cs
-            self.launch()                       # warm
+            try:
+                self.launch()                   # warm
+            except _lib.WspmError:
+                continue                        # shape not available on this GPU (e.g. 16-CTA clusters)
             for x, s in zip((self.h_n, self.dt, self.t, self.its, self.kits, self.status, self.err), saved):
                 x.copy_(s)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
