@@ -1318,6 +1318,18 @@ int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const doubl
     return e == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }
 
+template <typename T>
+bool pcg_eligible(const Sell &A) {
+    if (A.n_diags <= 0 || A.n_diags > 16) return false;
+    const RcgPlan pl = rcg_plan<T>(A.n_rows);
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return (int64_t)optin - 4096 >= (kNumPcgVec - 1) * (int64_t)pl.chunk * (int64_t)sizeof(T);
+}
+template bool pcg_eligible<float>(const Sell &);
+template bool pcg_eligible<double>(const Sell &);
+
 template int pcg_persistent_enqueue<double>(const Sell &, const double *, const double *, const double *, double *,
                                             const double *, const CgBuffers<double> &, double, double, int, bool,
                                             const double *, cudaStream_t, bool);

@@ -75,6 +75,10 @@ template <typename T>
 int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
                            const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
                            const double *tol_dev, cudaStream_t st, bool warp_specialized = true);
+// Whether pcg_persistent_enqueue accepts the pattern for element type T (DIA
+// with at most 16 diagonals, at least six per-block vectors on chip).
+template <typename T>
+bool pcg_eligible(const Sell &A);
 
 struct BicgBuffers {
     double *r, *rhat, *p, *phat, *q, *t;

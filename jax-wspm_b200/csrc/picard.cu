@@ -13,7 +13,10 @@
 // kernel that tests convergence, and every loop has an iteration cap, so
 // the graph always terminates.  The host launches the graph once per time
 // step and never synchronises inside it.
+#include <cstring>
+#include <mutex>
 #include <new>
+#include <vector>
 #include "krylov.cuh"
 #include "graph.cuh"
 #include "soil.cuh"
@@ -549,5 +552,155 @@ extern "C" int wspm_picard_destroy(void *plan) {
     if (P->graph) cudaGraphDestroy(P->graph);
     if (P->Ks_inc) cudaFree(P->Ks_inc);
     delete P;
+    return WSPM_OK;
+}
+
+// ---- one linear system in mixed precision ------------------------------------
+// FP32 Jacobi-CG corrections inside FP64 iterative refinement, the refinement
+// loop of the Picard graph without the Picard step around it: x = x0, r =
+// b - A x (FP64); while ||r|| > tol ||b||: solve A d = r in FP32 (pipelined CG
+// where the pattern allows it) to half the reduction still needed (floor
+// inner_tol), then x += d, r -= A d (FP64).  Captured once per argument set as
+// a CUDA graph (WHILE node for the refinements) and replayed, like
+// wspm_krylov_solve.
+namespace {
+
+__global__ void to_f32_kernel(const double *__restrict__ a, float *b, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+__global__ void mixed_result_kernel(const KrylovState *irs, int32_t *out) {
+    if (threadIdx.x == 0) {
+        out[0] = irs->status;
+        out[1] = irs->steps;     // FP32 CG iterations, all refinements
+        out[2] = irs->k;         // refinements (FP32 solves)
+        out[3] = 0;
+    }
+}
+
+struct MixedKey {
+    const void *pat_cols, *pat_ptr, *vals, *vals32, *b, *x, *dinv, *work, *result;
+    int64_t nnz_padded;
+    int n, inner_maxiter, refine_maxiter;
+    double tol, inner_tol;
+    bool operator==(const MixedKey &o) const { return std::memcmp(this, &o, sizeof(MixedKey)) == 0; }
+};
+struct MixedEntry {
+    MixedKey key;
+    cudaGraphExec_t exec;
+    cudaGraph_t graph;
+};
+std::mutex g_mixed_mu;
+std::vector<MixedEntry> g_mixed;
+constexpr size_t kMixedCacheMax = 8;
+
+int64_t mixed_vec(int n) { return (n + 31) & ~int64_t(31); }
+
+int build_mixed_graph(const wspm_pattern *pat, const double *vals, const float *vals32, const double *b, double *x,
+                      const double *dinv, double tol, double inner_tol, int inner_maxiter, int refine_maxiter,
+                      double *work, int32_t *result, cudaGraphExec_t *exec_out, cudaGraph_t *graph_out) {
+    const Sell A = make_sell(pat);
+    const int n = pat->n_rows;
+    const int nb = reduction_blocks(n);
+    const int64_t vec = mixed_vec(n);
+    // workspace: partials | refinement state | FP32 CG buffers | r64 | x32, dinv32 | vals32 (when not given),
+    // every part on a 256-byte boundary (the CG kernels move 16-byte row groups)
+    auto align = [](double *q) { return (double *)(((uintptr_t)q + 255) & ~(uintptr_t)255); };
+    double *p = align(work);
+    double *partials = p; p = align(p + 2 * kMaxPartials + 64);
+    KrylovState *irs = (KrylovState *)p; p = align(p + 64 + ((sizeof(KrylovState) + 7) / 8));
+    int64_t used = 0;
+    CgBuffers<float> cg32 = carve_cg<float>(p, n, &used); p = align(p + used + 64);
+    double *r64 = p; p = align(p + vec);
+    float *x32 = (float *)p, *dinv32 = (float *)p + vec; p = align(p + vec + 64);
+    float *v32 = vals32 ? const_cast<float *>(vals32) : (float *)p;
+    const bool pipelined = pcg_eligible<float>(A);
+    cudaStream_t cs;
+    WSPM_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    WSPM_CUDA_TRY(cudaGraphCreate(&g, 0));
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+        state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)irs, (int)(sizeof(KrylovState) / 4));
+        state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)cg32.st, (int)(sizeof(KrylovState) / 4));
+        if (!vals32) to_f32_kernel<<<reduction_blocks(pat->nnz_padded), kBlock, 0, cs>>>(vals, v32, pat->nnz_padded);
+        cudaGraphConditionalHandle h;
+        e = make_cond_handle(cs, &h);
+        float *dv32 = dinv ? dinv32 : nullptr;
+        WSPM_WIDTH_DISPATCH(A.max_width,
+                            ir_residual_kernel<MW><<<nb, kBlock, 0, cs>>>(A, vals, b, x, x, r64, dinv, dv32, partials,
+                                                                          irs, tol, inner_tol, refine_maxiter, h, 1));
+        if (e == cudaSuccess)
+            e = capture_while(cs, h, [&](cudaStream_t bs) {
+                int rc = WSPM_UNSUPPORTED;
+                if (pipelined)
+                    rc = pcg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0,
+                                                       inner_maxiter, true, &irs->inner_tol, bs);
+                if (rc == WSPM_UNSUPPORTED)
+                    cg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0, inner_maxiter,
+                                                 true, &irs->inner_tol, bs);
+                WSPM_WIDTH_DISPATCH(A.max_width,
+                                    ir_update_kernel<MW><<<nb, kBlock, 0, bs>>>(A, vals, x32, x, r64, partials, irs,
+                                                                                cg32.st, tol, inner_tol,
+                                                                                refine_maxiter, h, 1));
+            });
+        mixed_result_kernel<<<1, 32, 0, cs>>>(irs, result);
+        cudaGraph_t out = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(cs, &out);
+        if (e == cudaSuccess) e = e2;
+    }
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return WSPM_CUDA_ERROR; }
+    e = cudaGraphInstantiate(exec_out, g, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return WSPM_CUDA_ERROR; }
+    *graph_out = g;
+    return WSPM_OK;
+}
+
+}  // namespace
+
+extern "C" int64_t wspm_krylov_mixed_workspace_doubles(int32_t n_rows, int64_t nnz_padded) {
+    if (n_rows <= 0 || nnz_padded <= 0) return 0;
+    const int64_t vec = mixed_vec(n_rows);
+    return 2 * kMaxPartials + 64 + 64 + ((sizeof(KrylovState) + 7) / 8) + cg_workspace_doubles(n_rows, 4) + 64 +
+           vec + vec + 64 + (nnz_padded + 1) / 2 + 64 + 6 * 32;   // + alignment slack of six parts
+}
+
+extern "C" int wspm_krylov_solve_mixed(const wspm_pattern *pat, const double *vals, const float *vals32,
+                                       const double *b, double *x, const double *dinv, double tol, double inner_tol,
+                                       int32_t inner_maxiter, int32_t refine_maxiter, double *work,
+                                       int64_t work_doubles, int32_t *result, void *stream) {
+    if (!pat || pat->n_rows <= 0 || !pat->slice_ptr || !pat->slice_width || !pat->cols || pat->max_width <= 0)
+        return WSPM_BAD_ARG;
+    if (!vals || !b || !x || !work || !result) return WSPM_BAD_ARG;
+    if (!(tol > 0.0) || !(inner_tol > 0.0) || inner_tol >= 1.0 || inner_maxiter < 1 || refine_maxiter < 1)
+        return WSPM_BAD_ARG;
+    if (work_doubles < wspm_krylov_mixed_workspace_doubles(pat->n_rows, pat->nnz_padded)) return WSPM_BAD_ARG;
+    MixedKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.pat_cols = pat->cols; key.pat_ptr = pat->slice_ptr; key.vals = vals; key.vals32 = vals32; key.b = b;
+    key.x = x; key.dinv = dinv; key.work = work; key.result = result; key.nnz_padded = pat->nnz_padded;
+    key.n = pat->n_rows; key.inner_maxiter = inner_maxiter; key.refine_maxiter = refine_maxiter; key.tol = tol;
+    key.inner_tol = inner_tol;
+    cudaGraphExec_t exec = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mixed_mu);
+        for (auto &en : g_mixed)
+            if (en.key == key) { exec = en.exec; break; }
+        if (!exec) {
+            cudaGraph_t graph = nullptr;
+            const int rc = build_mixed_graph(pat, vals, vals32, b, x, dinv, tol, inner_tol, inner_maxiter,
+                                             refine_maxiter, work, result, &exec, &graph);
+            if (rc != WSPM_OK) return rc;
+            if (g_mixed.size() >= kMixedCacheMax) {
+                cudaGraphExecDestroy(g_mixed.front().exec);
+                cudaGraphDestroy(g_mixed.front().graph);
+                g_mixed.erase(g_mixed.begin());
+            }
+            g_mixed.push_back({key, exec, graph});
+        }
+    }
+    WSPM_CUDA_TRY(cudaGraphLaunch(exec, (cudaStream_t)stream));
     return WSPM_OK;
 }

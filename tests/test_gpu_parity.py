@@ -191,6 +191,33 @@ def test_krylov_solve_matches_oracle(solver, precond, layout):
     np.testing.assert_allclose(host(x), x_ref, rtol=1e-7, atol=1e-7)
 
 
+@pytest.mark.parametrize("layout,n", [("dia", 30), ("dia", 256), ("sell", 30)])
+def test_krylov_solve_mixed_reaches_fp64_residual(layout, n):
+    """wspm_krylov_solve_mixed: FP32 corrections (pipelined CG on the DIA layout, single-reduction CG on SELL)
+    inside FP64 refinement reach the FP64 residual 1e-8 ||b|| and the FP64 solution; a second call replays the
+    cached graph and gives bitwise the same x."""
+    pts, el, A, b, h = _linear_system(n=n)
+    D = dev()
+    dm = D.DeviceMesh(pts, el, layout=layout)
+    vals = cu(dm.pattern.sell_from_csr_values(A.data))
+    dinv = D.jacobi_dinv(dm, vals)
+    ws = torch.empty(int(D.lib.wspm_krylov_mixed_workspace_doubles(dm.n_nodes, dm.nnz_padded)),
+                     dtype=torch.float64, device="cuda")
+    bb, xx = cu(b), torch.empty(dm.n_nodes, dtype=torch.float64, device="cuda")
+    res = torch.zeros(4, dtype=torch.int32, device="cuda")
+    x, res = D.krylov_solve_mixed(dm, vals, bb, cu(h), dinv=dinv, tol=1e-8, workspace=ws, x_out=xx, result=res)
+    status, inner, corrections = host(res)[:3]
+    assert status == 0 and corrections >= 1 and inner > 0
+    xh = host(x)
+    assert np.linalg.norm(b - A @ xh) <= 1.0001e-8 * np.linalg.norm(b)
+    exact = np.linalg.solve(A.toarray(), b) if n <= 30 else okry.cg(A, b, h, tol=1e-12, maxiter=20000,
+                                                                     dinv=okry.jacobi_inverse_diagonal(A))[0]
+    np.testing.assert_allclose(xh, exact, rtol=1e-6, atol=1e-6)
+    first = x.clone()
+    x2, _ = D.krylov_solve_mixed(dm, vals, bb, cu(h), dinv=dinv, tol=1e-8, workspace=ws, x_out=xx, result=res)
+    assert torch.equal(first, x2)
+
+
 def test_krylov_maxiter_status_is_reported():
     pts, el, A, b, h = _linear_system(dirichlet=False)
     D = dev()
