@@ -96,6 +96,19 @@ class SparseMatrix:
     def nse(self):
         return self.dmesh.pattern.nnz
 
+    # CSR view (the fields a CSR matrix object has; the storage stays DIA / SELL-32 on the device)
+    @property
+    def indptr(self):
+        return self.dmesh.pattern.csr_indptr
+
+    @property
+    def indices(self):
+        return self.dmesh.pattern.csr_indices
+
+    @property
+    def data(self):
+        return self.csr_values()
+
     def __matmul__(self, x):
         return spmv(self.dmesh, self.vals, x)
 
@@ -110,6 +123,9 @@ class SparseMatrix:
 
     def diagonal(self):
         return jacobi_dinv(self.dmesh, self.vals).reciprocal()
+
+
+CSRMatrix = SparseMatrix   # the name under which the C-ABI shims describe the matrix object
 
 
 # ---------------------------------------------------------------- soil

@@ -153,6 +153,14 @@ def test_spmv(dtype, layout):
     A = dm.pattern.to_scipy(dm.pattern.sell_from_csr_values(data))
     tol = 1e-13 if dtype == torch.float64 else 2e-5
     np.testing.assert_allclose(y, A @ x, rtol=0, atol=tol * np.abs(A).sum(axis=1).max() * np.abs(x).max())
+    if dtype == torch.float64:
+        # the matrix object of the shims: CSR fields, @, todense
+        M = D.CSRMatrix(dm, vals)
+        np.testing.assert_array_equal(M.indptr, A.indptr)
+        np.testing.assert_array_equal(M.indices, A.indices)
+        np.testing.assert_array_equal(host(M.data), A.data)
+        np.testing.assert_allclose(host(M @ cu(x)), y, rtol=0, atol=0)
+        np.testing.assert_array_equal(host(M.todense()), A.toarray())
 
 
 def _linear_system(n=30, dirichlet=True):
