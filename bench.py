@@ -521,6 +521,7 @@ def run_config2(args):
     dm3 = DeviceMesh(pts, tets)
     eng = PicardEngine(dm3, "vg", VG_PHI_UNIT_KS, bc_val=merge_dirichlet(len(pts), [(top, -0.1)]),
                        solver="bicgstab", precond="jacobi", krylov_tol=1e-8, krylov_maxiter=1000)
+    eng.host_loop = args.host_loop          # host-driven loops: the same kernels, visible to profilers
     h0 = -np.ones(len(pts))
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     t3 = time_path(eng, h0, 1e-4, args.steps3d, args.warmup, 1, lambda: flush_buf.fill_(1.0))
