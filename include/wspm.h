@@ -252,7 +252,7 @@ int wspm_krylov_solve(const wspm_pattern *pat, const double *vals,
  * cannot reach): FP32 Jacobi-CG corrections inside FP64 iterative refinement.
  * x = x0 (in x), r = b - A x in FP64; while ||r|| > tol ||b||: solve A d = r in
  * FP32 -- the pipelined CG on DIA patterns whose vectors fit on chip, the
- * single-reduction CG otherwise -- to half the reduction still needed (never
+ * single-reduction CG otherwise -- to the reduction still needed (never
  * tighter than inner_tol, at most inner_maxiter iterations), then x += d and
  * r -= A d in FP64; at most refine_maxiter corrections.  vals32: the FP32 copy
  * of vals in the same layout, or NULL (made in the workspace on each call).
