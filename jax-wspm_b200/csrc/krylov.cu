@@ -581,31 +581,64 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     }
     const int last = n - 1;
     const int64_t ld = A.ld;
-    // ---- init: x, M into place; r = b - A x0 ; z = M r
+    T *const wbase = kVW < NS ? sm + kVW * chunk : gvW;
+    // ---- init: x, M into place; r = b - A x0 ; z = M r.  On DIA patterns A x0
+    // comes from the same row-group SpMV as the iterations (into w, which is
+    // free until w0 = A z0); then a thread's rows l = tid + j T are handled
+    // kBatch at a time, their loads issued before any store, the per-thread sums
+    // in row order.
     {
+        constexpr int kBatch = sizeof(T) == 4 ? 8 : 4;
+        const bool ax_dia = !a.zero_x0 && dia;
+        if (ax_dia) {
+            __syncthreads();       // s_off (written by thread 0 above) is read by every thread
+            T unused = T(0);
+            rcg_spmv_dia<T, (MW > 0 ? MW : 1)>(nl, lo_i, hi_i, unused, vals, ld, r0, last, nd, s_off, xg, wbase,
+                                                zflag, nbr_lo, nbr_hi, 0u, false, bar);
+            __syncthreads();
+        }
         T v[3] = {T(0), T(0), T(0)};
-        for (int l = threadIdx.x; l < nl; l += blockDim.x) {
-            const int i = r0 + l;
-            const T bi = a.b64 ? (T)a.b64[i] : a.b[i];
-            T ri;
-            if (a.zero_x0) {
-                xg[i] = T(0);
-                if (kVX < NS) RCG(kVX, l) = T(0);
-                ri = bi;
-            } else {
-                if (kVX < NS) RCG(kVX, l) = xg[i];
-                ri = bi - sell_row_dot<T, MW>(A, vals, i, [xg](int c) { return xg[c]; });
+        for (int l0 = threadIdx.x; l0 < nl; l0 += kBatch * (int)blockDim.x) {
+            T bq[kBatch], xq[kBatch], dq[kBatch], aq[kBatch];
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                const int l = l0 + q * (int)blockDim.x;
+                bq[q] = xq[q] = aq[q] = T(0);
+                dq[q] = T(1);
+                if (l < nl) {
+                    const int i = r0 + l;
+                    bq[q] = a.b64 ? (T)a.b64[i] : a.b[i];
+                    if (dg) dq[q] = dg[i];
+                    if (!a.zero_x0) xq[q] = xg[i];
+                    if (ax_dia) aq[q] = wbase[l];
+                }
             }
-            const T di = dg ? dg[i] : T(1);
-            if (kVD < NS) RCG(kVD, l) = di;
-            const T zi = di * ri;
-            RCG(kVR, l) = ri;
-            RCG(kVP, l) = T(0);
-            RCG(kVS, l) = T(0);
-            z[i] = zi;
-            v[0] += ri * zi;
-            v[1] += ri * ri;
-            v[2] += bi * bi;
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                const int l = l0 + q * (int)blockDim.x;
+                if (l >= nl) continue;
+                const int i = r0 + l;
+                const T bi = bq[q];
+                T ri;
+                if (a.zero_x0) {
+                    xg[i] = T(0);
+                    if (kVX < NS) RCG(kVX, l) = T(0);
+                    ri = bi;
+                } else {
+                    if (kVX < NS) RCG(kVX, l) = xq[q];
+                    ri = bi - (ax_dia ? aq[q] : sell_row_dot<T, MW>(A, vals, i, [xg](int c) { return xg[c]; }));
+                }
+                const T di = dq[q];
+                if (kVD < NS) RCG(kVD, l) = di;
+                const T zi = di * ri;
+                RCG(kVR, l) = ri;
+                RCG(kVP, l) = T(0);
+                RCG(kVS, l) = T(0);
+                z[i] = zi;
+                v[0] += ri * zi;
+                v[1] += ri * ri;
+                v[2] += bi * bi;
+            }
         }
         block_sum<T, 3>(v);
         if (threadIdx.x == 0) {
@@ -628,7 +661,6 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     bool done = !(rs > atol2 && 0 < a.maxiter);
     if (!isfinite(rs)) { done = true; status = WSPM_NAN; }
     unsigned int red = 0;      // counting barriers passed
-    T *const wbase = kVW < NS ? sm + kVW * chunk : gvW;
 #define RCG_SPMV_DIA(acc, epoch, poll)                                                                       \
     rcg_spmv_dia<T, (MW > 0 ? MW : 1)>(nl, lo_i, hi_i, (acc), vals, ld, r0, last, nd, s_off, z, wbase, zflag, \
                                        nbr_lo, nbr_hi, (epoch), (poll), bar)
@@ -1000,6 +1032,8 @@ __device__ __forceinline__ bool pcg_spmv_dia(int nl, int lo_i, int hi_i, const T
     return true;
 }
 
+constexpr int kInitBatch = 8;   // rows per thread whose loads the start-up loops issue together
+
 template <typename T, int MW, bool XS, bool WS>
 __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a) {
     using VT = Vec16<T>;
@@ -1050,28 +1084,53 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
     int nbr_hi = min(nb - 1, min(n - 1, r1 - 1 + mx) / chunk);
     if (nl == 0) { nbr_lo = 1; nbr_hi = 0; }
     __syncthreads();
-    // ---- init: r = b - A x0, p = s = z = 0, u0 = M r -> ex0
+    // ---- init: r = b - A x0, p = s = z = 0, u0 = M r -> ex0.  A thread's rows are
+    // l = tid + j TB; with x0 = 0 the loads of kInitBatch of them are issued before
+    // any store (one memory latency per batch instead of one per row), and the
+    // per-thread sum keeps the row order.
     {
         T v[1] = {T(0)};
-        for (int l = tid; l < nl; l += TB) {
-            const int i = r0 + l;
-            const T bi = a.b64 ? (T)a.b64[i] : a.b[i];
-            T ri;
-            if (a.zero_x0) {
-                xg[i] = T(0);
-                if (XS) vX[l] = T(0);
-                ri = bi;
-            } else {
-                if (XS) vX[l] = xg[i];
-                ri = bi - dia_row_z<T, MW>(vals, ld, i, last, nd, s_off, xg);
+        if (a.zero_x0) {
+            for (int l0 = tid; l0 < nl; l0 += kInitBatch * TB) {
+                T bq[kInitBatch], dq[kInitBatch];
+#pragma unroll
+                for (int q = 0; q < kInitBatch; ++q) {
+                    const int l = l0 + q * TB;
+                    bq[q] = T(0);
+                    dq[q] = T(1);
+                    if (l < nl) {
+                        bq[q] = a.b64 ? (T)a.b64[r0 + l] : a.b[r0 + l];
+                        if (dg) dq[q] = dg[r0 + l];
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kInitBatch; ++q) {
+                    const int l = l0 + q * TB;
+                    if (l < nl) {
+                        vX[l] = T(0);      // on chip, copied to x at the end; else x itself
+                        vR[l] = bq[q];
+                        vS[l] = T(0);
+                        vP[l] = T(0);
+                        vZ[l] = T(0);
+                        ex0[r0 + l] = dq[q] * bq[q];
+                        v[0] += bq[q] * bq[q];
+                    }
+                }
             }
-            const T di = dg ? dg[i] : T(1);
-            vR[l] = ri;
-            vS[l] = T(0);
-            vP[l] = T(0);
-            vZ[l] = T(0);
-            ex0[i] = di * ri;
-            v[0] += bi * bi;
+        } else {
+            for (int l = tid; l < nl; l += TB) {
+                const int i = r0 + l;
+                const T bi = a.b64 ? (T)a.b64[i] : a.b[i];
+                if (XS) vX[l] = xg[i];
+                const T ri = bi - dia_row_z<T, MW>(vals, ld, i, last, nd, s_off, xg);
+                const T di = dg ? dg[i] : T(1);
+                vR[l] = ri;
+                vS[l] = T(0);
+                vP[l] = T(0);
+                vZ[l] = T(0);
+                ex0[i] = di * ri;
+                v[0] += bi * bi;
+            }
         }
         block_sum<T, 1>(v);
         if (tid == 0) part[6 * (int64_t)nb + blockIdx.x] = v[0];
@@ -1100,15 +1159,25 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
                                  false, bar, tid, TB, false);
         __syncthreads();
         T v[3] = {T(0), T(0), T(0)};
-        for (int l = tid; l < nl; l += TB) {
-            const int i = r0 + l;
-            const T di = dg ? dg[i] : T(1);
-            const T ri = vR[l], wi = vW[l];
-            const T ui = di * ri;
-            ex1[i] = di * wi;
-            v[0] += ri * ui;
-            v[1] += wi * ui;
-            v[2] += ri * ri;
+        for (int l0 = tid; l0 < nl; l0 += kInitBatch * TB) {
+            T dq[kInitBatch];
+#pragma unroll
+            for (int q = 0; q < kInitBatch; ++q) {
+                const int l = l0 + q * TB;
+                dq[q] = (dg && l < nl) ? dg[r0 + l] : T(1);
+            }
+#pragma unroll
+            for (int q = 0; q < kInitBatch; ++q) {
+                const int l = l0 + q * TB;
+                if (l < nl) {
+                    const T ri = vR[l], wi = vW[l];
+                    const T ui = dq[q] * ri;
+                    ex1[r0 + l] = dq[q] * wi;
+                    v[0] += ri * ui;
+                    v[1] += wi * ui;
+                    v[2] += ri * ri;
+                }
+            }
         }
         publish(part, 2u, v);
     }

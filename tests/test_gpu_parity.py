@@ -226,6 +226,24 @@ def test_krylov_solve_mixed_reaches_fp64_residual(layout, n):
     assert torch.equal(first, x2)
 
 
+@pytest.mark.parametrize("iters", [3, 25])
+def test_warm_started_cg_iterates_match_oracle_on_many_blocks(iters):
+    """The resident FP64 CG from a non-zero x0 on a DIA system spread over every block (256^2 mesh): its start-up
+    computes r = b - A x0 with the row-group SpMV of the iterations, so a wrong start shows in the iterates.  The
+    system is the symmetric one (no Dirichlet rows): on a non-symmetric matrix the single-reduction form and the
+    textbook iteration differ beyond rounding."""
+    pts, el, A, b, h = _linear_system(n=256, dirichlet=False)
+    D = dev()
+    dm = D.DeviceMesh(pts, el, layout="dia")
+    vals = cu(dm.pattern.sell_from_csr_values(A.data))
+    dinv = D.jacobi_dinv(dm, vals)
+    x, res = D.krylov_solve(dm, vals, cu(b), cu(h), solver="cg", dinv=dinv, tol=1e-14, maxiter=iters)
+    status, k = host(res)[:2]
+    x_ref, k_ref = okry.cg(A, b, h, tol=1e-14, maxiter=iters, dinv=okry.jacobi_inverse_diagonal(A))
+    assert status == 1 and k == iters == k_ref
+    np.testing.assert_allclose(host(x), x_ref, rtol=1e-9, atol=1e-9)
+
+
 def test_krylov_maxiter_status_is_reported():
     pts, el, A, b, h = _linear_system(dirichlet=False)
     D = dev()
