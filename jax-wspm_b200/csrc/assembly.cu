@@ -17,6 +17,7 @@
 // which is compute_local_matrices_mixed_form (assembly_re_v2.py:13-60) and its
 // 3D twin (assembly_re_3D.py:12-70).
 #include "common.cuh"
+#include "krylov.cuh"
 #include "soil.cuh"
 
 namespace wspm {
@@ -57,6 +58,7 @@ struct RichardsAsmArgs {
     double *vals;
     float *vals32;
     double *rhs, *dinv;
+    RefineStart res;           // used by the RES instantiations only
 };
 
 template <int DIM>
@@ -194,7 +196,7 @@ __global__ void incidence_gather_kernel(int n_slices, const int64_t *__restrict_
 //
 // The element-local row index li selects a column of G by selects: an indexed
 // register array would live in local memory.
-template <int DIM, int MW, int KSM, bool STAGE, int TB, int MINB>
+template <int DIM, int MW, int KSM, bool STAGE, int TB, int MINB, bool RES>
 __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs a) {
     constexpr int NV = DIM + 1;
     constexpr int CH = STAGE ? 4 : 1;   // incidences whose loads are issued together
@@ -206,7 +208,9 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
     if (dia)
         for (int k = threadIdx.x; k < a.n_diags; k += TB) s_off[k] = a.diag_off[k];
     __syncthreads();
-    if (s >= ((a.n_rows + kSlice - 1) >> 5)) return;
+    double res_v[2] = {0.0, 0.0};   // RES: this row's (r.r, b.b)
+    do {   // one pass; break = this thread has no row (every thread reaches the RES reduction)
+    if (s >= ((a.n_rows + kSlice - 1) >> 5)) break;
     const int width = dia ? a.n_diags : a.slice_width[s];
     // entry k of this row lives at vb + kstride * k
     const int64_t vb = dia ? (int64_t)i : a.slice_ptr[s] + lane;
@@ -217,7 +221,7 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
             a.vals[vb + kstride * k] = 0.0;
             if (a.vals32) a.vals32[vb + kstride * k] = 0.0f;
         }
-        return;
+        break;
     }
     double *acc = acc_sm + threadIdx.x;
     double *colv = acc_sm + MW * TB + threadIdx.x;   // column k, component c at colv[(k * NV + c) * TB]
@@ -344,12 +348,61 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
         diag = acc[dpos * TB];
     }
     a.rhs[i] = rhs_i;
-    if (a.dinv) a.dinv[i] = 1.0 / (diag != 0.0 ? diag : 1.0);
+    const double dinv_i = 1.0 / (diag != 0.0 ? diag : 1.0);
+    if (a.dinv) a.dinv[i] = dinv_i;
     for (int k = 0; k < width; ++k) {
         const double v = acc[k * TB];
         a.vals[vb + kstride * k] = v;
         if (a.vals32) a.vals32[vb + kstride * k] = (float)v;
     }
+    if constexpr (RES) {
+        // start of the refinement loop: r = b - A x0 with the row just built
+        // (entries and columns in storage order, as the stand-alone kernel sums them)
+        const int last = a.n_rows - 1;
+        const double *x0 = a.res.x0;
+        double dot = 0.0;
+        for (int k = 0; k < width; ++k) {
+            int c = dia ? i + s_off[k] : __ldg(a.cols + vb + kstride * k);
+            c = c < 0 ? 0 : (c > last ? last : c);
+            dot = fma(acc[k * TB], x0[c], dot);
+        }
+        const double ri = rhs_i - dot;
+        a.res.r[i] = ri;
+        a.res.x[i] = x0[i];
+        if (a.res.dinv32) a.res.dinv32[i] = (float)dinv_i;
+        res_v[0] = ri * ri;
+        res_v[1] = rhs_i * rhs_i;
+    }
+    } while (false);
+    if constexpr (RES) {
+        // the block's partial sums; refine_start_kernel adds them up (no fence or ticket
+        // here: every block of this latency-bound launch would hold its slot for them)
+        block_sum<double, 2>(res_v);
+        if (threadIdx.x == 0) {
+            a.res.partials[blockIdx.x] = res_v[0];
+            a.res.partials[gridDim.x + blockIdx.x] = res_v[1];
+        }
+    }
+}
+
+// One block after the assembly: (r.r, b.b) from the assembly blocks' partials in a
+// fixed order, then the refinement loop's first decision.
+__global__ void __launch_bounds__(1024) refine_start_kernel(RefineStart rs, int nb) {
+    double v[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const double *pj = rs.partials + (int64_t)j * nb;
+        double a0 = 0.0, a1 = 0.0;
+        int b = threadIdx.x;
+        for (; b + (int)blockDim.x < nb; b += 2 * (int)blockDim.x) {
+            a0 += pj[b];
+            a1 += pj[b + blockDim.x];
+        }
+        if (b < nb) a0 += pj[b];
+        v[j] = a0 + a1;
+    }
+    block_sum<double, 2>(v);
+    if (threadIdx.x == 0) ir_decide(v, rs.irs, nullptr, 1, rs.tol, rs.inner_floor, rs.maxit, rs.cond, rs.use_cond);
 }
 
 // Host-side quadrature constants from the reference rule.
@@ -375,16 +428,32 @@ void quadrature_constants(int dim, const double *Q, const double *W, int nq, dou
 }
 
 template <int DIM, int MW, bool STAGE, int TB, int MINB>
-static void launch_rows(const RichardsAsmArgs &a, int ksm, int n_slices, cudaStream_t st) {
+static void launch_rows(const RichardsAsmArgs &a, int ksm, int n_slices, bool res, cudaStream_t st) {
     const int blocks = (n_slices * kSlice + TB - 1) / TB;
     const size_t smem = (size_t)MW * TB * sizeof(double) * (STAGE ? 1 + (DIM + 1) : 1);
     auto run = [&](auto kfn) {
         if (smem > 48 * 1024) cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kfn<<<blocks, TB, smem, st>>>(a);
     };
-    if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB>);
-    else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB>);
-    else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB>);
+    if (res) {
+        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, true>);
+        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, true>);
+        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, true>);
+    } else {
+        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, false>);
+        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, false>);
+        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, false>);
+    }
+}
+
+// Blocks of the assembly launch (the partial-sum slots a fused refinement start needs).
+int richards_assembly_blocks(const wspm_mesh *mesh, const wspm_pattern *pat) {
+    const int rows = pat->n_slices * kSlice;
+    const int mw = pat->max_width;
+    int tb;
+    if (mesh->dim == 2) tb = mw <= 8 ? 256 : mw <= 16 ? 128 : mw <= 32 ? 64 : 32;
+    else tb = (pat->n_diags > 0 && mw <= 16) ? 128 : mw <= 16 ? 128 : mw <= 32 ? 64 : 32;
+    return (rows + tb - 1) / tb;
 }
 
 static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_pattern *pat,
@@ -392,8 +461,10 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
                                          const double *K, const double *C, const double *Ks_elem,
                                          const double *Ks_inc, const double s[4], const double mc[4], double dt,
                                          const double *dt_dev, const double *bc_val, double *vals, float *vals32,
-                                         double *rhs, double *dinv, cudaStream_t st) {
+                                         double *rhs, double *dinv, const RefineStart *res, cudaStream_t st) {
     RichardsAsmArgs a;
+    const bool fused = res != nullptr;
+    if (fused) a.res = *res;
     a.n_rows = pat->n_rows;
     a.slice_ptr = pat->slice_ptr; a.slice_width = pat->slice_width; a.diag_pos = pat->diag_pos;
     a.inc_ptr = pat->inc_ptr; a.inc_width = pat->inc_width; a.inc_elem = pat->inc_elem; a.inc_slots = pat->inc_slots;
@@ -414,17 +485,18 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     const int mw = pat->max_width;
     // launch shapes measured on the 1024^2 triangle and 96^3 Kuhn-tetrahedron grids (B200)
     if (mesh->dim == 2) {
-        if (mw <= 8) launch_rows<2, 8, true, 256, 3>(a, ksm, ns, st);
-        else if (mw <= 16) launch_rows<2, 16, true, 128, 1>(a, ksm, ns, st);
-        else if (mw <= 32) launch_rows<2, 32, true, 64, 1>(a, ksm, ns, st);
-        else launch_rows<2, 64, true, 32, 1>(a, ksm, ns, st);
+        if (mw <= 8) launch_rows<2, 8, true, 256, 3>(a, ksm, ns, fused, st);
+        else if (mw <= 16) launch_rows<2, 16, true, 128, 1>(a, ksm, ns, fused, st);
+        else if (mw <= 32) launch_rows<2, 32, true, 64, 1>(a, ksm, ns, fused, st);
+        else launch_rows<2, 64, true, 32, 1>(a, ksm, ns, fused, st);
     } else {
-        if (pat->n_diags > 0 && mw <= 16) launch_rows<3, 16, false, 128, 8>(a, ksm, ns, st);
-        else if (mw <= 8) launch_rows<3, 8, true, 128, 1>(a, ksm, ns, st);
-        else if (mw <= 16) launch_rows<3, 16, true, 128, 1>(a, ksm, ns, st);
-        else if (mw <= 32) launch_rows<3, 32, true, 64, 1>(a, ksm, ns, st);
-        else launch_rows<3, 64, true, 32, 1>(a, ksm, ns, st);
+        if (pat->n_diags > 0 && mw <= 16) launch_rows<3, 16, false, 128, 8>(a, ksm, ns, fused, st);
+        else if (mw <= 8) launch_rows<3, 8, true, 128, 1>(a, ksm, ns, fused, st);
+        else if (mw <= 16) launch_rows<3, 16, true, 128, 1>(a, ksm, ns, fused, st);
+        else if (mw <= 32) launch_rows<3, 32, true, 64, 1>(a, ksm, ns, fused, st);
+        else launch_rows<3, 64, true, 32, 1>(a, ksm, ns, fused, st);
     }
+    if (fused) refine_start_kernel<<<1, 1024, 0, st>>>(*res, richards_assembly_blocks(mesh, pat));
     return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }
 
@@ -434,16 +506,17 @@ int launch_richards_assembly(const wspm_mesh *mesh, const wspm_pattern *pat, con
                              const double *bc_val, double *vals, float *vals32, double *rhs, double *dinv,
                              cudaStream_t st) {
     return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, nullptr, s, mc, dt,
-                                         nullptr, bc_val, vals, vals32, rhs, dinv, st);
+                                         nullptr, bc_val, vals, vals32, rhs, dinv, nullptr, st);
 }
 
 int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
                                     const double *theta_n, const double *h_m, const double *K, const double *C,
                                     const double *Ks_elem, const double *Ks_inc, const double s[4],
                                     const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
-                                    float *vals32, double *rhs, double *dinv, cudaStream_t st) {
+                                    float *vals32, double *rhs, double *dinv, const RefineStart *res,
+                                    cudaStream_t st) {
     return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, Ks_inc, s, mc, 1.0,
-                                         dt_dev, bc_val, vals, vals32, rhs, dinv, st);
+                                         dt_dev, bc_val, vals, vals32, rhs, dinv, res, st);
 }
 
 int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st) {

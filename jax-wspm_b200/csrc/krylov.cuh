@@ -23,6 +23,53 @@ struct KrylovState {
     unsigned int ticket[4];
 };
 
+// Reduction tail of the refinement steps (the start, fused into the assembly or
+// as ir_residual_kernel, and ir_update_kernel): tot = (r.r, b.b); sets
+// the next inner tolerance, the continue flag and the graph condition.
+__device__ __forceinline__ void ir_decide(const double (&tot)[2], KrylovState *irs, const KrylovState *inner,
+                                          int is_init, double tol, double inner_floor, int maxit,
+                                          cudaGraphConditionalHandle cond, int use_cond) {
+    if (is_init) {
+        irs->bs = tot[1];
+        irs->atol2 = tol * tol * tot[1];
+        irs->k = 0;
+        irs->steps = 0;
+        irs->pad0 = 0;
+        irs->status = WSPM_OK;
+    } else {
+        irs->k += 1;
+        irs->steps += inner->k;
+        irs->pad0 += 1;
+    }
+    irs->rr = tot[0];
+    // the next FP32 solve aims at the reduction the FP64 residual still needs,
+    // never tighter than the floor FP32 can reach (a margin below it measured
+    // slower: the inner iterations it adds cost more than the corrections it
+    // saves; the FP64 residual decides when the loop ends)
+    const double need = sqrt(irs->atol2 / fmax(tot[0], 1e-300));
+    irs->inner_tol = fmin(0.5, fmax(inner_floor, need));
+    int cont = tot[0] > irs->atol2 && irs->k < maxit;
+    if (!cont && tot[0] > irs->atol2) irs->status = WSPM_MAXITER;
+    if (!isfinite(tot[0])) { cont = 0; irs->status = WSPM_NAN; }
+    irs->done = !cont;
+    if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+}
+
+// Start of the FP64 refinement loop fused into the assembly: with this set, the
+// row kernel also writes r = b - A x0, x = x0 and the FP32 1/diag of its row
+// and ends with the (r.r, b.b) reduction and ir_decide.
+struct RefineStart {
+    const double *x0;
+    double *x, *r;
+    float *dinv32;             // may be null
+    double *partials;          // 2 x (assembly blocks)
+    KrylovState *irs;
+    double tol, inner_floor;
+    int maxit;
+    cudaGraphConditionalHandle cond;
+    int use_cond;
+};
+
 // Precision-generic CG over one matrix.  Buffers are carved from a workspace.
 template <typename T>
 struct CgBuffers {

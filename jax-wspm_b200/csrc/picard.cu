@@ -32,7 +32,9 @@ int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *p
                                     const double *theta_n, const double *h_m, const double *K, const double *C,
                                     const double *Ks_elem, const double *Ks_inc, const double s[4],
                                     const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
-                                    float *vals32, double *rhs, double *dinv, cudaStream_t st);
+                                    float *vals32, double *rhs, double *dinv, const RefineStart *res,
+                                    cudaStream_t st);
+int richards_assembly_blocks(const wspm_mesh *mesh, const wspm_pattern *pat);
 int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st);
 
 struct PicardState {
@@ -137,36 +139,6 @@ __global__ void step_finish_kernel(int n, const double *__restrict__ h_m, double
 // ir state (KrylovState): bs, atol2, rr, k (refinement iterations), steps (inner
 // iterations summed), status.
 
-// Reduction tail shared by the two refinement kernels: tot = (r.r, b.b); sets
-// the next inner tolerance, the continue flag and the graph condition.
-__device__ __forceinline__ void ir_decide(const double (&tot)[2], KrylovState *irs, const KrylovState *inner,
-                                          int is_init, double tol, double inner_floor, int maxit,
-                                          cudaGraphConditionalHandle cond, int use_cond) {
-    if (is_init) {
-        irs->bs = tot[1];
-        irs->atol2 = tol * tol * tot[1];
-        irs->k = 0;
-        irs->steps = 0;
-        irs->pad0 = 0;
-        irs->status = WSPM_OK;
-    } else {
-        irs->k += 1;
-        irs->steps += inner->k;
-        irs->pad0 += 1;
-    }
-    irs->rr = tot[0];
-    // the next FP32 solve aims at the reduction the FP64 residual still needs,
-    // never tighter than the floor FP32 can reach (a margin below it measured
-    // slower: the inner iterations it adds cost more than the corrections it
-    // saves; the FP64 residual decides when the loop ends)
-    const double need = sqrt(irs->atol2 / fmax(tot[0], 1e-300));
-    irs->inner_tol = fmin(0.5, fmax(inner_floor, need));
-    int cont = tot[0] > irs->atol2 && irs->k < maxit;
-    if (!cont && tot[0] > irs->atol2) irs->status = WSPM_MAXITER;
-    if (!isfinite(tot[0])) { cont = 0; irs->status = WSPM_NAN; }
-    irs->done = !cont;
-    if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
-}
 
 // Start of the refinement loop: x = x0, r = b - A x0 (FP64), the FP32 copy of
 // 1/diag, and the loop state.
@@ -238,6 +210,23 @@ struct PicardPlan {
     double *Ks_inc = nullptr;   // Ks_elem in incidence order (owned by the plan), refreshed at every step start
 };
 
+// The mixed path starts each refinement loop inside the assembly launch (r = b - A h_m
+// from the rows just built) when nothing is added to the rows after it (no Neumann or
+// drainage edges) and its partial sums fit the plan's slots.
+static bool fuse_refine_start(const PicardPlan *P) {
+    return P->d.mixed && P->neumann.n_bnodes <= 0 && P->drainage.n_bnodes <= 0 &&
+           richards_assembly_blocks(&P->mesh, &P->pat) <= kMaxPartials;
+}
+
+static RefineStart refine_start(const PicardPlan *P, cudaGraphConditionalHandle cond, int use_cond) {
+    RefineStart r;
+    r.x0 = P->d.h_m; r.x = P->d.x; r.r = P->r64; r.dinv32 = P->dinv32;
+    r.partials = P->partials; r.irs = P->irs;
+    r.tol = P->d.krylov_tol; r.inner_floor = P->d.inner_tol; r.maxit = P->d.refine_maxiter;
+    r.cond = cond; r.use_cond = use_cond;
+    return r;
+}
+
 int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
     const int64_t vec = (n + 31) & ~int64_t(31);
     int64_t t = 64 + ((sizeof(PicardState) + 7) / 8) + 2 * kMaxPartials + 64;
@@ -294,9 +283,13 @@ static int build_picard_graph(PicardPlan *P) {
                                             d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, hp, 1);
     if (e == cudaSuccess) e = capture_while(cs, hp, [&](cudaStream_t bs) {
         launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, bs);
+        cudaGraphConditionalHandle hir = cudaGraphConditionalHandle();
+        if (d.mixed) make_cond_handle(bs, &hir);
+        const RefineStart rs = refine_start(P, hir, 1);
+        const bool fused = fuse_refine_start(P);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                         P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
-                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, bs);
+                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr, bs);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           bs);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
@@ -304,13 +297,13 @@ static int build_picard_graph(PicardPlan *P) {
         const KrylovState *ks = nullptr;
         const KrylovState *irs = nullptr;
         if (d.mixed) {
-            cudaGraphConditionalHandle hir;
-            make_cond_handle(bs, &hir);
-            WSPM_WIDTH_DISPATCH(A.max_width,
-                                ir_residual_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, d.rhs, d.h_m, d.x, P->r64,
-                                                                              d.dinv, P->dinv32, P->partials, P->irs,
-                                                                              d.krylov_tol, d.inner_tol,
-                                                                              d.refine_maxiter, hir, 1));
+            if (!fused)
+                WSPM_WIDTH_DISPATCH(A.max_width,
+                                    ir_residual_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, d.rhs, d.h_m, d.x,
+                                                                                  P->r64, d.dinv, P->dinv32,
+                                                                                  P->partials, P->irs, d.krylov_tol,
+                                                                                  d.inner_tol, d.refine_maxiter, hir,
+                                                                                  1));
             capture_while(bs, hir, [&](cudaStream_t ibs) {
                 const float *dv32 = dinv ? P->dinv32 : nullptr;
                 inner_cg_enqueue(A, d, P, dv32, ibs);
@@ -390,20 +383,24 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                                             d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, none, 0);
     for (int it = 0; it < d.picard_maxiter && rc == WSPM_OK; ++it) {
         launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, st);
+        const RefineStart rs = refine_start(P, none, 0);
+        const bool fused = fuse_refine_start(P);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                         P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
-                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, st);
+                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr, st);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           st);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
                           st);
         const KrylovState *ks = nullptr, *irs = nullptr;
         if (d.mixed) {
-            WSPM_WIDTH_DISPATCH(A.max_width,
-                                ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.h_m, d.x, P->r64,
-                                                                              d.dinv, P->dinv32, P->partials, P->irs,
-                                                                              d.krylov_tol, d.inner_tol,
-                                                                              d.refine_maxiter, none, 0));
+            if (!fused)
+                WSPM_WIDTH_DISPATCH(A.max_width,
+                                    ir_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, d.rhs, d.h_m, d.x,
+                                                                                  P->r64, d.dinv, P->dinv32,
+                                                                                  P->partials, P->irs, d.krylov_tol,
+                                                                                  d.inner_tol, d.refine_maxiter, none,
+                                                                                  0));
             const float *dv32 = dinv ? P->dinv32 : nullptr;
             for (int r = 0; r <= d.refine_maxiter && rc == WSPM_OK; ++r) {
                 if ((rc = read_flag(&P->irs->done, st, &flag, pinned)) != WSPM_OK || flag) break;

@@ -144,6 +144,8 @@ class PicardEngine:
         edge-term kernels, the x0 copy, the Krylov init kernels, picard_update.  The Krylov
         loop itself is counted on the device (one persistent kernel per CG solve, 4 kernels per
         BiCGSTAB iteration, 4m+4 per GMRES cycle); each refinement adds correction + residual.
+        The mixed path's refinement start is one kernel either way (the stand-alone residual, or
+        the one-block decision after an assembly that computed the residual of its rows).
         """
         cfg = self.config
         e = self._edge_kernels
