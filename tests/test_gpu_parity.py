@@ -423,6 +423,33 @@ def test_mixed_precision_refinement_reaches_fp64_residual(layout):
     np.testing.assert_allclose(out[True]["pressure_head"], out[False]["pressure_head"], rtol=1e-6, atol=1e-7)
 
 
+def test_fused_refinement_start_matches_standalone_residual():
+    """Without edge terms the mixed path starts its refinement loop inside the assembly launch; with a zero-flux
+    Neumann edge (the same linear systems) it runs the stand-alone residual kernel.  Both reach the FP64 residual,
+    the same Picard iterations and the same heads to the solver tolerance."""
+    from wspm_b200.device import DeviceMesh, merge_dirichlet, spmv
+    from wspm_b200.engine import PicardEngine
+    pts, tri = mesh.structured_triangles(96, 1.0)
+    rng = np.random.default_rng(6)
+    Ks = 0.0922 * np.exp(rng.standard_normal(len(tri)))
+    top = np.where(pts[:, 1] == 1.0)[0]
+    bottom = np.where(pts[:, 1] == 0.0)[0]
+    bc = merge_dirichlet(len(pts), [(top, -0.1)])
+    phi = opic.VG_UNIT_PHI[:5] + (1.0,)
+    dm = DeviceMesh(pts, tri)
+    out = {}
+    for edges in (None, bottom):
+        eng = PicardEngine(dm, "vg", phi, Ks_elem=Ks, bc_val=bc, solver="cg", precond="jacobi", krylov_tol=1e-8,
+                           krylov_maxiter=5000, mixed=True, neumann_nodes=edges, neumann_flux=0.0)
+        res = eng.run(-np.ones(len(pts)), 1e-4, 1e-3, fixed_dt=True, max_steps=3)
+        assert np.all(res["status"] == 0)
+        r = eng.rhs - spmv(dm, eng.vals, eng.x)
+        assert float(torch.linalg.norm(r) / torch.linalg.norm(eng.rhs)) <= 1.01e-8
+        out[edges is None] = res
+    np.testing.assert_array_equal(out[True]["iterations"], out[False]["iterations"])
+    np.testing.assert_allclose(out[True]["pressure_head"], out[False]["pressure_head"], rtol=1e-7, atol=1e-8)
+
+
 def test_picard_step_is_bitwise_repeatable():
     pts, tri, eng, h0 = _engine_test_case("Test2", 50, "cg", "jacobi")
     a = eng.run(h0, 1e-3, 0.02)
