@@ -21,7 +21,7 @@
  * The reference (JAX-WSPM) is pure Python + JAX; each entry point below names
  * the reference function whose behaviour it implements (file:line within the
  * reference project).  Python shims with the reference's own signatures live
- * in jax-wspm_b200/src/ (see INTEGRATION.md).
+ * in jax-wspm_b200/src/.
  */
 #ifndef WSPM_H
 #define WSPM_H
@@ -288,18 +288,21 @@ int wspm_cg_iterations(const wspm_pattern *pat, int32_t mode, const void *vals, 
  * for callers that cannot allocate device memory -- typically code running
  * inside a JAX program (the reference's runtime), whose allocator reserves
  * most of the GPU's memory up front, or code where cudaMalloc is not allowed
- * (inside a stream capture) or too slow.  Same solve as wspm_krylov_solve with
- * WSPM_SOLVER_CG (x holds x0 on entry, the solution on exit; dinv == NULL:
- * no preconditioner; result = {status, iterations, 0, 0}), but the Krylov
- * vectors and solver state live in a static device array inside the library
- * instead of a caller-supplied workspace, and nothing is allocated.
- * Limits: at most WSPM_NOALLOC_MAX_ROWS rows (larger systems return
- * WSPM_BAD_ARG before anything is launched); the scratch (about 11 MB) is held
- * by every GPU that loads the library until the process exits.  All calls on
- * a device share that one array: calls that overlap on the GPU (two streams,
- * or two host threads on one device) race and corrupt each other.  The first
- * call on each device looks up the array's address and caches it; make that
- * first call before any stream capture.                                    */
+ * (inside a stream capture) or too slow.  It runs the kernel that
+ * wspm_krylov_solve runs for WSPM_SOLVER_CG, with the same arguments (x holds
+ * x0 on entry, the solution on exit; dinv == NULL: no preconditioner; result =
+ * {status, iterations, 0, 0}), so the iteration count and the iterate are
+ * those of that call; but the Krylov vectors and solver state live in a
+ * static device array inside the library instead of a caller-supplied
+ * workspace, and nothing is allocated.  One kernel launch per call, whatever
+ * maxiter is.  vals, x, dinv must start on 16-byte boundaries (WSPM_BAD_ARG
+ * otherwise).  Limits: at most WSPM_NOALLOC_MAX_ROWS rows (larger systems
+ * return WSPM_BAD_ARG before anything else is looked at); the scratch (about
+ * 11 MB) is held by every GPU that loads the library until the process exits.
+ * All calls on a device share that one array: calls that overlap on the GPU
+ * (two streams, or two host threads on one device) race and corrupt each
+ * other.  The first call on each device looks up the array's address and
+ * caches it; make that first call before any stream capture.               */
 #define WSPM_NOALLOC_MAX_ROWS 262144
 int wspm_cg_solve_noalloc(const wspm_pattern *pat, const double *vals, const double *b, double *x,
                           const double *dinv, double tol, double atol, int32_t maxiter,
@@ -352,9 +355,15 @@ typedef struct wspm_picard_desc {
     int32_t *result;           /* device int32[8]: status, picard its,
                                   total Krylov its, refinement its, ...     */
     double *result_f64;        /* device double[4]: picard error, ...       */
+    double *Ks_inc;            /* with Ks_elem: wspm_picard_ks_inc_doubles(pat)
+                                  doubles, Ks_elem gathered in incidence order
+                                  at every step start; NULL without Ks_elem */
 } wspm_picard_desc;
 
 int64_t wspm_picard_workspace_doubles(int32_t n_rows, int32_t mixed);
+/* Size of wspm_picard_desc.Ks_inc: one double per incidence slot
+ * (n_slices * 32 * max_inc).                                               */
+int64_t wspm_picard_ks_inc_doubles(const wspm_pattern *pat);
 int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out);
 int wspm_picard_step(void *plan, void *stream);
 /* The same step with the loops driven from the host (identical kernels; the

@@ -56,9 +56,12 @@ __global__ void write_result_kernel(const KrylovState *st, int32_t *result) {
 }
 
 // ---- cache of instantiated stand-alone solve graphs ------------------------
+// Everything a captured solve graph depends on, the pattern's whole storage
+// description and the device included.
 struct SolveKey {
-    const void *pat_cols, *pat_ptr, *pat_width, *vals, *b, *x, *dinv, *work, *result;
-    int n, solver, maxiter, restart;
+    const void *pat_cols, *pat_ptr, *pat_width, *pat_diag_off, *vals, *b, *x, *dinv, *work, *result;
+    int64_t nnz_padded;
+    int n, n_slices, max_width, n_diags, device, solver, maxiter, restart;
     double tol, atol;
     bool operator==(const SolveKey &o) const { return std::memcmp(this, &o, sizeof(SolveKey)) == 0; }
 };
@@ -150,11 +153,7 @@ extern "C" int wspm_soil_exponential(const double *h, int64_t n, const double *p
     return soil_entry(WSPM_SOIL_EXPONENTIAL, h, n, phi, 4, C, K, theta, stream);
 }
 
-static bool pattern_ok(const wspm_pattern *p) {
-    return p && p->n_rows > 0 && p->n_slices == (p->n_rows + 31) / 32 && p->slice_ptr && p->slice_width &&
-           p->cols && p->diag_pos && p->max_width > 0 && p->max_width <= 63 &&
-           (p->n_diags == 0 || (p->n_diags == p->max_width && p->diag_offsets));
-}
+static bool pattern_ok(const wspm_pattern *p) { return pattern_layout_ok(p) && p->diag_pos; }
 
 extern "C" int wspm_assemble_richards(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
                                       const double *theta_n, const double *h_m, const double *K, const double *C,
@@ -274,8 +273,13 @@ extern "C" int wspm_krylov_solve(const wspm_pattern *pat, const double *vals, co
     if (need < 0 || work_doubles < need) return WSPM_BAD_ARG;
     SolveKey key;
     std::memset(&key, 0, sizeof(key));
-    key.pat_cols = pat->cols; key.pat_ptr = pat->slice_ptr; key.pat_width = pat->slice_width; key.vals = vals; key.b = b; key.x = x; key.dinv = dinv; key.work = work;
-    key.result = result; key.n = pat->n_rows; key.solver = solver; key.maxiter = maxiter;
+    key.pat_cols = pat->cols; key.pat_ptr = pat->slice_ptr; key.pat_width = pat->slice_width;
+    key.pat_diag_off = pat->n_diags > 0 ? pat->diag_offsets : nullptr;
+    key.vals = vals; key.b = b; key.x = x; key.dinv = dinv; key.work = work;
+    key.result = result; key.nnz_padded = pat->nnz_padded; key.n = pat->n_rows; key.n_slices = pat->n_slices;
+    key.max_width = pat->max_width; key.n_diags = pat->n_diags;
+    WSPM_CUDA_TRY(cudaGetDevice(&key.device));
+    key.solver = solver; key.maxiter = maxiter;
     key.restart = solver == WSPM_SOLVER_GMRES ? restart : 0; key.tol = tol; key.atol = atol;
     cudaGraphExec_t exec = nullptr;
     {

@@ -19,6 +19,16 @@ constexpr int kSlice = 32;          // SELL slice height == warp size
 constexpr int kBlock = 256;         // threads per block for vector kernels
 constexpr int kMaxPartials = 16384; // partial-sum slots: one block per 256 rows up to 4M rows
 
+// Host-side consistency check of a pattern's storage description (everything
+// the sparse kernels index with, except the diagonal positions, which only the
+// entry points that read the diagonal need): slices cover the rows, DIA
+// patterns have one width, widths fit the unrolled row loops.
+inline bool pattern_layout_ok(const wspm_pattern *p) {
+    return p && p->n_rows > 0 && p->n_slices == (p->n_rows + 31) / 32 && p->slice_ptr && p->slice_width &&
+           p->cols && p->max_width > 0 && p->max_width <= 63 && p->nnz_padded > 0 &&
+           (p->n_diags == 0 || (p->n_diags == p->max_width && p->diag_offsets));
+}
+
 // Grid of a reducing kernel: one thread per row (or element) up to 8 blocks
 // per SM, grid-stride beyond.  Every block publishes one partial through an
 // atomic ticket on a single word, so the cap bounds that serialised tail

@@ -23,10 +23,11 @@
 //  * the first call on each device looks up the array's device address
 //    (cudaGetSymbolAddress, with that device current) and caches it; make that
 //    first call before any stream capture.
-// The solve launches the same kernels as wspm_krylov_solve's CG, as a fixed
-// sequence of (maxiter + 1) / 2 two-iteration bodies whose kernels return at
-// once after convergence, so it never synchronises with the host and calls no
-// allocating CUDA routine.
+// The solve is one launch of the same resident (cooperative) CG kernel that
+// wspm_krylov_solve runs for WSPM_SOLVER_CG, so it takes the same iterations
+// and returns the same iterate bit for bit; the iteration loop runs inside
+// the kernel, so the number of launches does not grow with maxiter.  It never
+// synchronises with the host and calls no allocating CUDA routine.
 #include <mutex>
 #include "krylov.cuh"
 #include "graph.cuh"
@@ -59,9 +60,12 @@ static int noalloc_scratch(double **out) {
     return WSPM_OK;
 }
 
+// Result words of the solve.  The CG kernel sets `done` when it leaves its
+// loop; a state that is not done (the kernel did not run to its end) is
+// reported as an error, never as success.
 __global__ void noalloc_result_kernel(const KrylovState *st, int32_t *result) {
     if (threadIdx.x == 0) {
-        result[0] = st->status;
+        result[0] = st->done ? st->status : WSPM_CUDA_ERROR;
         result[1] = st->k;
         result[2] = 0;
         result[3] = 0;
@@ -75,11 +79,10 @@ using namespace wspm;
 extern "C" int wspm_cg_solve_noalloc(const wspm_pattern *pat, const double *vals, const double *b, double *x,
                                      const double *dinv, double tol, double atol, int32_t maxiter, int32_t *result,
                                      void *stream) {
-    if (!pat || !vals || !b || !x || !result || maxiter < 0 || !(tol >= 0.0) || !(atol >= 0.0)) return WSPM_BAD_ARG;
-    if (pat->n_rows <= 0 || pat->n_rows > kNoallocMaxRows) return WSPM_BAD_ARG;
-    if (!pat->slice_ptr || !pat->slice_width || !pat->cols || pat->max_width <= 0 || pat->max_width > 63 ||
-        (pat->n_diags != 0 && !pat->diag_offsets))
-        return WSPM_BAD_ARG;
+    // size first: a system beyond the scratch is refused whatever the other arguments are
+    if (!pat || pat->n_rows <= 0 || pat->n_rows > kNoallocMaxRows) return WSPM_BAD_ARG;
+    if (!pattern_layout_ok(pat)) return WSPM_BAD_ARG;
+    if (!vals || !b || !x || !result || maxiter < 0 || !(tol >= 0.0) || !(atol >= 0.0)) return WSPM_BAD_ARG;
     if (cg_workspace_doubles(pat->n_rows, 8) > kNoallocScratchDoubles) return WSPM_BAD_ARG;
     double *scratch = nullptr;
     int rc = noalloc_scratch(&scratch);
@@ -88,12 +91,10 @@ extern "C" int wspm_cg_solve_noalloc(const wspm_pattern *pat, const double *vals
     const Sell A = make_sell(pat);
     int64_t used = 0;
     CgBuffers<double> w = carve_cg<double>(scratch, pat->n_rows, &used);
+    // the previous call's state and barrier words are still in the scratch: clear them
     state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)w.st, (int)(sizeof(KrylovState) / 4));
-    cg_enqueue_init<double>(A, vals, b, nullptr, x, x, dinv, w, tol, atol, maxiter, false,
-                            cudaGraphConditionalHandle(), 0, st);
-    const int bodies = (maxiter + 1) / 2;
-    for (int k = 0; k < bodies; ++k)
-        cg_enqueue_body<double>(A, vals, x, dinv, w, maxiter, cudaGraphConditionalHandle(), 0, st);
+    rc = cg_persistent_enqueue<double>(A, vals, b, nullptr, x, dinv, w, tol, atol, maxiter, false, nullptr, st);
+    if (rc != WSPM_OK) return rc;      // WSPM_BAD_ARG: an array not on a 16-byte boundary
     noalloc_result_kernel<<<1, 32, 0, st>>>(w.st, result);
     return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }

@@ -207,7 +207,7 @@ struct PicardPlan {
     KrylovState *irs = nullptr;
     double *r64 = nullptr;
     float *x32 = nullptr, *dinv32 = nullptr;
-    double *Ks_inc = nullptr;   // Ks_elem in incidence order (owned by the plan), refreshed at every step start
+    double *Ks_inc = nullptr;   // Ks_elem in incidence order (caller's buffer), refreshed at every step start
 };
 
 // The mixed path starts each refinement loop inside the assembly launch (r = b - A h_m
@@ -470,6 +470,11 @@ extern "C" int64_t wspm_picard_workspace_doubles(int32_t n_rows, int32_t mixed) 
     return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
 
+extern "C" int64_t wspm_picard_ks_inc_doubles(const wspm_pattern *pat) {
+    if (!pat || pat->n_slices <= 0) return -1;
+    return (int64_t)pat->n_slices * kSlice * (int64_t)(pat->max_inc > 0 ? pat->max_inc : 1);
+}
+
 extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out) {
     if (!desc || !plan_out || !desc->mesh || !desc->pat) return WSPM_BAD_ARG;
     const wspm_picard_desc &d = *desc;
@@ -480,6 +485,7 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
         !d.work || !d.dt_dev || !d.result || !d.result_f64)
         return WSPM_BAD_ARG;
     if (d.mixed && !d.vals32) return WSPM_BAD_ARG;
+    if (d.Ks_elem && !d.Ks_inc) return WSPM_BAD_ARG;
     if (d.mixed && d.solver != WSPM_SOLVER_CG) return WSPM_UNSUPPORTED;
     if (d.solver == WSPM_SOLVER_GMRES && (d.restart < 1 || d.restart > 32)) return WSPM_UNSUPPORTED;
     if (d.solver < WSPM_SOLVER_CG || d.solver > WSPM_SOLVER_GMRES) return WSPM_BAD_ARG;
@@ -518,18 +524,9 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     } else {
         P->cg64 = carve_cg<double>(p, n, &used); p += used;
     }
-    if (d.Ks_elem) {
-        // incidence slots: at most n_slices * 32 * max_inc
-        const size_t slots = (size_t)P->pat.n_slices * kSlice * (size_t)(P->pat.max_inc > 0 ? P->pat.max_inc : 1);
-        if (cudaMalloc(&P->Ks_inc, slots * sizeof(double)) != cudaSuccess) {
-            P->Ks_inc = nullptr;
-            delete P;
-            return WSPM_CUDA_ERROR;
-        }
-    }
+    P->Ks_inc = d.Ks_elem ? d.Ks_inc : nullptr;
     int rc = build_picard_graph(P);
     if (rc != WSPM_OK) {
-        if (P->Ks_inc) cudaFree(P->Ks_inc);
         delete P;
         return rc;
     }
@@ -549,7 +546,6 @@ extern "C" int wspm_picard_destroy(void *plan) {
     PicardPlan *P = (PicardPlan *)plan;
     if (P->exec) cudaGraphExecDestroy(P->exec);
     if (P->graph) cudaGraphDestroy(P->graph);
-    if (P->Ks_inc) cudaFree(P->Ks_inc);
     delete P;
     return WSPM_OK;
 }
@@ -578,10 +574,14 @@ __global__ void mixed_result_kernel(const KrylovState *irs, int32_t *out) {
     }
 }
 
+// Everything a captured graph depends on: the arrays it reads and writes, the
+// whole storage description of the pattern (a pattern rebuilt into reused
+// buffers with another layout or width must not replay a graph captured for
+// the old one) and the device.
 struct MixedKey {
-    const void *pat_cols, *pat_ptr, *vals, *vals32, *b, *x, *dinv, *work, *result;
+    const void *pat_cols, *pat_ptr, *pat_width, *pat_diag_off, *vals, *vals32, *b, *x, *dinv, *work, *result;
     int64_t nnz_padded;
-    int n, inner_maxiter, refine_maxiter;
+    int n, n_slices, max_width, n_diags, device, inner_maxiter, refine_maxiter, pad_;
     double tol, inner_tol;
     bool operator==(const MixedKey &o) const { return std::memcmp(this, &o, sizeof(MixedKey)) == 0; }
 };
@@ -670,17 +670,20 @@ extern "C" int wspm_krylov_solve_mixed(const wspm_pattern *pat, const double *va
                                        const double *b, double *x, const double *dinv, double tol, double inner_tol,
                                        int32_t inner_maxiter, int32_t refine_maxiter, double *work,
                                        int64_t work_doubles, int32_t *result, void *stream) {
-    if (!pat || pat->n_rows <= 0 || !pat->slice_ptr || !pat->slice_width || !pat->cols || pat->max_width <= 0)
-        return WSPM_BAD_ARG;
+    if (!pattern_layout_ok(pat)) return WSPM_BAD_ARG;
     if (!vals || !b || !x || !work || !result) return WSPM_BAD_ARG;
     if (!(tol > 0.0) || !(inner_tol > 0.0) || inner_tol >= 1.0 || inner_maxiter < 1 || refine_maxiter < 1)
         return WSPM_BAD_ARG;
     if (work_doubles < wspm_krylov_mixed_workspace_doubles(pat->n_rows, pat->nnz_padded)) return WSPM_BAD_ARG;
     MixedKey key;
     std::memset(&key, 0, sizeof(key));
-    key.pat_cols = pat->cols; key.pat_ptr = pat->slice_ptr; key.vals = vals; key.vals32 = vals32; key.b = b;
+    key.pat_cols = pat->cols; key.pat_ptr = pat->slice_ptr; key.pat_width = pat->slice_width;
+    key.pat_diag_off = pat->n_diags > 0 ? pat->diag_offsets : nullptr;
+    key.vals = vals; key.vals32 = vals32; key.b = b;
     key.x = x; key.dinv = dinv; key.work = work; key.result = result; key.nnz_padded = pat->nnz_padded;
-    key.n = pat->n_rows; key.inner_maxiter = inner_maxiter; key.refine_maxiter = refine_maxiter; key.tol = tol;
+    key.n = pat->n_rows; key.n_slices = pat->n_slices; key.max_width = pat->max_width; key.n_diags = pat->n_diags;
+    WSPM_CUDA_TRY(cudaGetDevice(&key.device));
+    key.inner_maxiter = inner_maxiter; key.refine_maxiter = refine_maxiter; key.tol = tol;
     key.inner_tol = inner_tol;
     cudaGraphExec_t exec = nullptr;
     {

@@ -4,6 +4,7 @@ The library is compiled for ``sm_100a`` only (``-gencode
 arch=compute_100a,code=sm_100a``) and written next to this file, so it
 travels with the source tree.  cudart is linked statically.
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -36,16 +37,18 @@ def build_library(force=False, verbose=False, extra_flags=()):
     """Compile every .cu in csrc/ into libwspm.so; returns the library path."""
     if not force and up_to_date():
         return LIB
-    objs = []
     build_dir = os.path.join(PKG_ROOT, "_build")
     os.makedirs(build_dir, exist_ok=True)
-    for src in SOURCES:
-        obj = os.path.join(build_dir, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, *extra_flags, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
+    objs = [os.path.join(build_dir, src.replace(".cu", ".o")) for src in SOURCES]
+    cmds = [[NVCC, *FLAGS, *extra_flags, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+            for src, obj in zip(SOURCES, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    # translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static", *objs, "-o", tmp]
     subprocess.run(cmd, check=True)

@@ -98,6 +98,10 @@ class PicardEngine:
             setattr(d, name, getattr(self, name).data_ptr())
         d.vals32 = self.vals32.data_ptr() if self.vals32 is not None else None
         d.work_doubles = self.work.numel()
+        self.Ks_inc = None
+        if self.Ks_elem is not None:        # Ks_elem in incidence order, refreshed by the step graph
+            self.Ks_inc = torch.empty(int(lib.wspm_picard_ks_inc_doubles(ctypes.byref(dm.c_pat))), **f64)
+            d.Ks_inc = self.Ks_inc.data_ptr()
         # boundary-edge rhs terms (Neumann flux, free drainage of water), applied after assembly
         self.neumann = BoundaryEdges(dm, neumann_nodes) if neumann_nodes is not None else None
         self.drainage = BoundaryEdges(dm, drainage_nodes) if drainage_nodes is not None else None

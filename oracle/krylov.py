@@ -1,7 +1,7 @@
 """Krylov solvers and preconditioners (oracle restatement).
 
 The reference calls ``jax.scipy.sparse.linalg.{cg, bicgstab, gmres}``
-(src/solvers/jax_linear_solver.py:349-397) with ``tol=1e-10, atol=0,
+(src/solvers/jax_linear_solver.py:255-329) with ``tol=1e-10, atol=0,
 maxiter=100, restart=30`` (config/settings.py:104-106) and x0 = the current
 Picard iterate.  jax/jaxlib are third-party and unpinned
 (requirements.txt:1-2) and absent here, so these are restatements of the

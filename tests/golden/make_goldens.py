@@ -1,9 +1,10 @@
 """Regenerate the committed golden fixtures from the reference tree.
 
-Run in a container that has the reference checked out (read-only) at
-/root/reference:
+Run where a checkout of the reference project is available (read-only is
+fine), giving its root directory as the argument or in the environment
+variable WSPM_REFERENCE_ROOT:
 
-    python tests/golden/make_goldens.py [/root/reference]
+    python tests/golden/make_goldens.py /path/to/JAX-WSPM
 
 It writes, next to this script:
   * ``re2d_metrics.json``  -- every row of resultsRE2D/benchmark_results_*_WA.csv
@@ -82,4 +83,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WSPM_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_goldens.py REFERENCE_ROOT (or set WSPM_REFERENCE_ROOT)")
+    main(root)

@@ -36,35 +36,61 @@ def test_noalloc_rejects_oversized_systems_before_launching():
     assert rc == _lib.WSPM_BAD_ARG
 
 
+def _noalloc(dm, vals, bt, x0, dinv, tol, maxiter, stream):
+    from wspm_b200 import _lib
+    x = x0.clone()
+    result = torch.full((4,), -7, dtype=torch.int32, device="cuda")
+    rc = _lib.lib.wspm_cg_solve_noalloc(ctypes.byref(dm.c_pat), _lib.dptr(vals), _lib.dptr(bt), _lib.dptr(x),
+                                        _lib.dptr(dinv), tol, 0.0, maxiter, _lib.dptr(result), stream)
+    assert rc == _lib.WSPM_OK
+    torch.cuda.synchronize()
+    return x.cpu().numpy(), result.cpu().numpy()
+
+
 @pytest.mark.gpu
-def test_noalloc_cg_matches_workspace_cg_twice():
+@pytest.mark.parametrize("precond", ["jacobi", "none"])
+def test_noalloc_cg_matches_workspace_cg_twice(precond):
+    """Two calls in a row on the shared static scratch, each equal bit for bit to wspm_krylov_solve's CG (the
+    same resident kernel, the Krylov vectors in the library's array instead of the caller's workspace); without
+    a preconditioner (dinv NULL) also checked against the oracle's textbook CG."""
+    from oracle import krylov as okry
     from wspm_b200 import _lib
     from wspm_b200.device import DeviceMesh, jacobi_dinv, krylov_solve
     pts, el, A, b, h = _system()
     dm = DeviceMesh(pts, el)
     vals = torch.as_tensor(dm.pattern.sell_from_csr_values(A.data), device="cuda")
     bt = torch.as_tensor(b, device="cuda")
-    dinv = jacobi_dinv(dm, vals)
-    x_ref, res_ref = krylov_solve(dm, vals, bt, torch.as_tensor(h, device="cuda"), solver="cg", dinv=dinv,
-                                  tol=1e-10, maxiter=500)
-    x_ref = x_ref.clone()
+    h0 = torch.as_tensor(h, device="cuda")
+    dinv = jacobi_dinv(dm, vals) if precond == "jacobi" else None
+    maxiter = 2000
+    x_ref, res_ref = krylov_solve(dm, vals, bt, h0, solver="cg", dinv=dinv, tol=1e-10, maxiter=maxiter)
+    x_ref = x_ref.cpu().numpy().copy()
     ref = res_ref.cpu().numpy().copy()
+    assert ref[0] == 0
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    first = None
-    for call in range(2):                      # two calls in a row share the static scratch
-        x = torch.as_tensor(h, device="cuda").clone()
-        result = torch.full((4,), -7, dtype=torch.int32, device="cuda")
-        rc = _lib.lib.wspm_cg_solve_noalloc(ctypes.byref(dm.c_pat), _lib.dptr(vals), _lib.dptr(bt), _lib.dptr(x),
-                                            _lib.dptr(dinv), 1e-10, 0.0, 500, _lib.dptr(result), stream)
-        assert rc == _lib.WSPM_OK, call
-        torch.cuda.synchronize()
-        got = result.cpu().numpy()
-        assert got[0] == ref[0] == 0 and got[1] == ref[1], (call, got, ref)
-        # the workspace entry runs the single-reduction CG kernel, this one the two-reduction form: the same
-        # iteration count, iterates equal to the accuracy of a 1e-10 relative-residual solve
-        np.testing.assert_allclose(x.cpu().numpy(), x_ref.cpu().numpy(), rtol=1e-8, atol=1e-9)
-        # the second call on the reused scratch repeats the first bit for bit
-        if first is None:
-            first = x.cpu().numpy().copy()
-        else:
-            np.testing.assert_array_equal(x.cpu().numpy(), first)
+    for call in range(2):
+        x, got = _noalloc(dm, vals, bt, h0, dinv, 1e-10, maxiter, stream)
+        assert got[0] == _lib.WSPM_OK and got[1] == ref[1], (call, got, ref)
+        np.testing.assert_array_equal(x, x_ref)
+    if precond == "none":
+        x_or, k_or = okry.solve_system(A, b, h, "cg", "none", tol=1e-10, maxiter=maxiter)
+        assert abs(int(got[1]) - k_or) <= max(2, k_or // 20), (got[1], k_or)
+        exact = np.linalg.solve(A.toarray(), b)
+        err = np.linalg.norm(x - exact) / np.linalg.norm(exact)
+        err_or = np.linalg.norm(x_or - exact) / np.linalg.norm(exact)
+        assert err <= max(10 * err_or, 1e-9), (err, err_or)
+        np.testing.assert_allclose(x, x_or, rtol=1e-7, atol=1e-7)
+
+
+@pytest.mark.gpu
+def test_noalloc_cg_reports_the_iteration_cap():
+    """A cap below the iterations the solve needs ends with WSPM_MAXITER and exactly `maxiter` iterations."""
+    from wspm_b200 import _lib
+    from wspm_b200.device import DeviceMesh, jacobi_dinv
+    pts, el, A, b, h = _system()
+    dm = DeviceMesh(pts, el)
+    vals = torch.as_tensor(dm.pattern.sell_from_csr_values(A.data), device="cuda")
+    bt = torch.as_tensor(b, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _, got = _noalloc(dm, vals, bt, torch.as_tensor(h, device="cuda"), jacobi_dinv(dm, vals), 1e-10, 3, stream)
+    assert got[0] == _lib.WSPM_MAXITER and got[1] == 3, got
