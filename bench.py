@@ -13,9 +13,12 @@ inside FP64 iterative refinement on the true residual (the headline `value`).
 A "step" is one implicit time step (a full device-resident Picard loop).  The
 timed region runs K steps from the initial state after W untimed warm-up
 steps; L2 is flushed (a 256 MiB write) between timed steps, outside the
-events.  `--impl reference` times the CPU oracle (the NumPy/SciPy
-restatement of the reference's algorithm; JAX is not installed) on a bounded
-sample: one Picard iteration of the same workload per step.
+events.  After the timed runs both GPU paths run the same K steps once more
+(untimed) and every step's pressure head and theta are compared with the FP64
+oracle's (the C + OpenMP restatement, oracle/richards2d.c, on all host cores;
+its time for the whole workload is the CPU baseline).  `--impl reference`
+times that oracle (JAX, the reference's runtime, is not installed) on the
+same workload: W warm-up steps, then K time steps from the initial state.
 """
 import argparse
 import json
@@ -40,11 +43,7 @@ KS_MEAN = 0.0922
 
 def workload(n, seed):
     from wspm_b200 import mesh
-    pts, tri = mesh.structured_triangles(n, 1.0)
-    rng = np.random.default_rng(seed)
-    Ks = np.exp(np.log(KS_MEAN) + 1.0 * rng.standard_normal(len(tri)))
-    top = np.where(pts[:, 1] == 1.0)[0]
-    return pts, tri, Ks, top
+    return mesh.lognormal_ks_square(n, seed, 1.0, KS_MEAN)
 
 
 def algorithmic_bytes_cg(N, nnz, w):
@@ -153,6 +152,7 @@ def time_path(eng, h0, dt, steps, warmup, world, flush):
     torch.cuda.synchronize()
     eng.set_state(h0)
     res_buf = torch.zeros((steps, 8), dtype=torch.int32, device="cuda")
+    res_f64 = torch.zeros((steps, 4), dtype=torch.float64, device="cuda")
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     barrier(world)
     for k in range(steps):
@@ -161,13 +161,17 @@ def time_path(eng, h0, dt, steps, warmup, world, flush):
         eng.launch_step(dt)
         ev[k][1].record()
         res_buf[k].copy_(eng.result)
+        res_f64[k].copy_(eng.result_f64)
     barrier(world)
     ms = sum(a.elapsed_time(b) for a, b in ev)
     r = res_buf.cpu().numpy()
     its, kits, refs, bodies = int(r[:, 1].sum()), int(r[:, 2].sum()), int(r[:, 3].sum()), r[:, 6]
     launches = sum(eng.kernel_launches(int(r[k, 1]), int(r[k, 3]), int(bodies[k])) for k in range(steps))
+    # seconds the resident CG kernels ran inside the timed steps (their own %globaltimer: a kernel node
+    # inside a graph cannot be bracketed by CUDA events)
+    krylov_s = float(res_f64[:, 1].sum().item())
     return {"ms": ms, "picard_its": its, "krylov_its": kits, "refinements": refs, "status": r[:, 0].tolist(),
-            "launches": launches}
+            "launches": launches, "krylov_kernel_s": krylov_s}
 
 
 def time_e2e(eng, h0, dt, steps, world, flush):
@@ -195,43 +199,53 @@ def time_e2e(eng, h0, dt, steps, world, flush):
     return {"ms": ms, "picard_its": its, "h2d": N * 8, "d2h": N * 8 + 32}
 
 
-def roofline_probe(dm, eng, fp32, reps=200, pipelined=False):
-    """Average duration of one Jacobi-CG iteration of the persistent CG kernel on the assembled system
-    (pipelined: the kernel of the mixed path's FP32 inner solve).
-
-    The solve starts from x = 0 (so the residual cannot reach zero within `reps` iterations) and the kernel
-    reports how many iterations it ran; a short run raises instead of being timed."""
+def l2_read_bandwidth(nbytes, reps=(40, 200)):
+    """Streaming-read bandwidth (GB/s) of a buffer of `nbytes` bytes (wspm_read_probe, 16-byte loads that bypass
+    L1, each block its own contiguous share): the difference of two launches with different pass counts, timed
+    with CUDA events, so the launch and the first (cold) pass cancel.  Best of three."""
     import ctypes
     import torch
     from wspm_b200 import _lib
     from wspm_b200._lib import check, lib
-    N = dm.n_nodes
-    if fp32:
-        vals, dinv, b = eng.vals32, eng.dinv.float(), eng.rhs.float()
-    else:
-        vals, dinv, b = eng.vals, eng.dinv, eng.rhs.clone()
-    x = torch.zeros_like(b)
-    mode = (1 if fp32 else 0) | (2 if pipelined else 0)
-    done = torch.zeros(1, dtype=torch.int32, device="cuda")
-    work = torch.empty(int(lib.wspm_krylov_workspace_doubles(N, 0, 0)), dtype=torch.float64, device="cuda")
+    n16 = max(1, int(nbytes) // 16)
+    buf = torch.ones(4 * n16, dtype=torch.float32, device="cuda")
+    out = torch.zeros(1, dtype=torch.float32, device="cuda")
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
-    def run(iters):
-        x.zero_()
+    def run(r):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        check("cg_iterations", lib.wspm_cg_iterations(ctypes.byref(dm.c_pat), mode, _lib.dptr(vals),
-                                                       _lib.dptr(b), _lib.dptr(x), _lib.dptr(dinv), iters,
-                                                       _lib.dptr(work), work.numel(), _lib.dptr(done), st))
+        check("read_probe", lib.wspm_read_probe(_lib.dptr(buf), n16, r, 2, _lib.dptr(out), st))
         e1.record()
         torch.cuda.synchronize()
-        if int(done.item()) != iters:
-            raise RuntimeError(f"CG probe ran {int(done.item())} of {iters} iterations")
-        return e0.elapsed_time(e1)
-    run(20)
-    t0 = min(run(0) for _ in range(3))
-    tr = min(run(reps) for _ in range(3))
-    return (tr - t0) / reps * 1e-3     # seconds per CG iteration
+        return e0.elapsed_time(e1) * 1e-3
+    run(reps[0])
+    best = 0.0
+    for _ in range(3):
+        t0, t1 = run(reps[0]), run(reps[1])
+        best = max(best, (reps[1] - reps[0]) * n16 * 16 / (t1 - t0) / 1e9)
+    return best
+
+
+def assembly_seconds(eng, dm, reps=20):
+    """Average duration (CUDA events) of the Richards row-assembly launch on the engine's current state, through
+    the C ABI (wspm_assemble_richards: rows, Dirichlet rows, Jacobi 1/diag and the FP32 copy)."""
+    import torch
+    from wspm_b200.device import assemble_richards, soil
+    from wspm_b200.engine import default_rule
+    C, K, th = soil("vg", eng.h_n, VG_PHI_UNIT_KS)
+    Q, W = default_rule(2)
+    args = (dm, th, th, eng.h_n, K, C, Q, W, 1e-4)
+    kw = dict(bc_val=eng.bc_val, Ks_elem=eng.Ks_elem, want_f32=True)
+    assemble_richards(*args, **kw)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        assemble_richards(*args, **kw)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / reps
 
 
 def load_peaks():
@@ -249,22 +263,51 @@ def load_traffic(key):
     return None
 
 
-def cpu_baseline(n, seed, picard_its=1):
-    """Oracle (NumPy/SciPy, single thread) on one Picard iteration of the same workload."""
-    from oracle import picard as opic
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def oracle_run(n, seed, steps, keep_steps=False, threads=None):
+    """The FP64 oracle (C + OpenMP restatement, oracle/richards2d.c) on the same workload: `steps` fixed-dt
+    steps from h0; returns the oracle's result dict (h per step when keep_steps, Picard/CG iterations, seconds
+    of the time loop, threads)."""
+    from oracle import picard as opic, richards2d_c
+    richards2d_c.build()
     pts, tri, Ks, top = workload(n, seed)
-    prob, h0 = opic.vg_dirichlet_case(pts, tri, top, Ks_elem=Ks, tol=1e-8, maxiter=100000)
-    _, _, theta_n = prob.model(h0)
-    t0 = time.perf_counter()
-    h = h0.copy()
-    for _ in range(picard_its):
-        A, b = prob.linear_system(h, theta_n, 1e-4)
-        from oracle.krylov import solve_system
-        h, _ = solve_system(A, b, h, "cg", "jacobi", tol=1e-8, maxiter=100000)
-    dt = time.perf_counter() - t0
-    return {"value": len(pts) * picard_its / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{picard_its} Picard iteration(s) of the {n}^2 workload (assembly + Jacobi-CG to 1e-8), "
-                      f"NumPy/SciPy oracle, 1 thread, {dt:.1f} s"}
+    nodes, vals = opic.dirichlet_arrays(len(pts), [(top, -0.1)])
+    out = richards2d_c.run_vg_fixed_dt(pts, tri, VG_PHI_UNIT_KS, nodes, vals, -np.ones(len(pts)), 1e-4, steps,
+                                       Ks_elem=Ks, picard_tol=1e-6, picard_max=100, picard_relative=True,
+                                       cg_tol=1e-8, cg_maxiter=100000, threads=threads or host_cores(),
+                                       keep_steps=keep_steps)
+    out["nodes"] = len(pts)
+    return out
+
+
+def cpu_baseline_from(ref, n, steps):
+    v = ref["nodes"] * int(ref["picard_its"].sum()) / ref["seconds"]
+    return {"value": v, "unit": UNIT, "cores": int(ref["threads"]), "kind": "port",
+            "sample": f"the whole workload: {steps} steps of the {n}^2 case ({int(ref['picard_its'].sum())} Picard "
+                      f"iterations, {int(ref['cg_its'].sum())} Jacobi-CG iterations to 1e-8), FP64 oracle "
+                      f"restated in C + OpenMP (oracle/richards2d.c), {int(ref['threads'])} threads, "
+                      f"{ref['seconds']:.1f} s (JAX, the reference's runtime, is not installed)"}
+
+
+def parity_vs_oracle(ref, runs):
+    """Max over steps of the relative L2 error of pressure head and theta against the oracle, per GPU path."""
+    from oracle import soil as osoil
+    th_ref = [osoil.van_genuchten_model(h, VG_PHI_UNIT_KS)[2] for h in ref["h_steps"]]
+    out = {}
+    for name, res in runs.items():
+        eh = max(float(np.linalg.norm(res["pressure_head"][s] - ref["h_steps"][s]) / np.linalg.norm(ref["h_steps"][s]))
+                 for s in range(len(th_ref)))
+        et = max(float(np.linalg.norm(res["theta"][s] - th_ref[s]) / np.linalg.norm(th_ref[s]))
+                 for s in range(len(th_ref)))
+        out[name] = {"h_rel_err": eh, "theta_rel_err": et,
+                     "picard_its_equal": bool(np.array_equal(res["iterations"], ref["picard_its"]))}
+    return out
 
 
 def run_reference(args):
@@ -272,36 +315,31 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import picard as opic
-    from oracle.krylov import solve_system
-    pts, tri, Ks, top = workload(args.n, args.seed)
-    prob, h0 = opic.vg_dirichlet_case(pts, tri, top, Ks_elem=Ks, tol=1e-8, maxiter=100000)
-    _, _, theta_n = prob.model(h0)
-
-    def one():
-        A, b = prob.linear_system(h0, theta_n, 1e-4)
-        solve_system(A, b, h0, "cg", "jacobi", tol=1e-8, maxiter=100000)
-
-    for _ in range(args.warmup):
-        one()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        one()
-    dt = time.perf_counter() - t0
-    v = len(pts) * args.steps / dt
+    cores = host_cores()
+    oracle_run(args.n, args.seed, max(1, args.warmup), threads=cores)       # warm-up (not timed)
+    ref = oracle_run(args.n, args.seed, args.steps, threads=cores)
+    its = int(ref["picard_its"].sum())
+    v = ref["nodes"] * its / ref["seconds"]
+    cb = cpu_baseline_from(ref, args.n, args.steps)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ref["seconds"] / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)",
-            "config": {"workload": f"2D Richards {args.n}^2 VG, per-element log-normal Ks, dt 1e-4, "
-                                   "1 Picard iteration per step (bounded CPU sample)",
-                       "nodes": len(pts), "elements": len(tri), "seed": args.seed},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": "one Picard iteration (assembly + Jacobi-CG to 1e-8) of the same workload "
-                                       "per step; NumPy/SciPy oracle (JAX, the reference's runtime, is not "
-                                       "installed), single thread"},
+            "data": "synthetic (seeded log-normal Ks)",
+            "config": workload_config(args),
+            "picard_its": its, "krylov_its": int(ref["cg_its"].sum()),
+            "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def workload_config(args, world=1, host_loop=False):
+    return {"workload": f"2D Richards {args.n}^2 P1 triangles, VG soil, per-element log-normal Ks "
+                        f"(sigma_lnK 1, seed {args.seed}), h0 -1, top Dirichlet -0.1, dt 1e-4 fixed, "
+                        f"{args.steps} steps from the initial state",
+            "nodes": (args.n + 1) ** 2, "elements": 2 * args.n * args.n, "picard_tol": 1e-6,
+            "krylov_residual": 1e-8, "l2_policy": "L2 flushed (256 MiB write) between timed steps",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "loop_control": "host" if host_loop else "device (CUDA graph conditional nodes)"}
 
 
 def cg_probe(args):
@@ -649,16 +687,35 @@ def main():
         r = eng.rhs - spmv(dm, eng.vals, eng.x)
         res_true[name] = float(torch.linalg.norm(r) / torch.linalg.norm(eng.rhs))
     rel_diff = float(torch.linalg.norm(hmx - h64) / torch.linalg.norm(h64))
-    # roofline of the dominant kernels (one Jacobi-CG iteration = fused K1 + K2)
-    t_it32 = roofline_probe(dm, engmx, fp32=True, pipelined=True)
-    t_it64 = roofline_probe(dm, eng64, fp32=False)
     nnz = dm.pattern.nnz
-    peak, peak_kind = load_peaks()
+    nd, ld = dm.pattern.n_diags, 32 * dm.pattern.n_slices
+    peak_hbm, peak_kind = load_peaks()
+    # ---- rooflines.  The resident CG kernels keep their vectors in shared memory and read the matrix from L2
+    # every iteration: their roof is the L2 read bandwidth, measured here with a streaming-read probe over a
+    # buffer the size of the matrix.  Per-iteration times are the kernels' own live durations in the timed steps.
+    t_it32 = rmx["krylov_kernel_s"] / max(1, rmx["krylov_its"])
+    t_it64 = r64["krylov_kernel_s"] / max(1, r64["krylov_its"])
+    # L2 bytes one iteration must move: pipelined FP32 = the matrix (nd diagonals of ld rows) + 1/diag read +
+    # m = M w written and read by the SpMV; FP64 = the matrix + z written and read, x read and written, 1/diag
+    l2_32 = nd * ld * 4 + 3 * N * 4
+    l2_64 = nd * ld * 8 + 5 * N * 8
+    l2_peak32 = l2_read_bandwidth(nd * ld * 4)
+    l2_peak64 = l2_read_bandwidth(nd * ld * 8)
     b32 = algorithmic_bytes_cg(N, nnz, 4)
     b64 = algorithmic_bytes_cg(N, nnz, 8)
+    # the assembly is the HBM-streaming kernel of the step (SURVEY-style algorithmic bytes, per launch)
+    t_asm = assembly_seconds(engmx, dm)
+    b_asm = E * 12 + N * 16 + 2 * N * 8 + E * 8 + nnz * 8 + N * 8 + N * 8
     ms64 = allreduce_max(r64["ms"], world)
     msmx = allreduce_max(rmx["ms"], world)
     mse2e = allreduce_max(e2e["ms"], world)
+    # parity: both paths again over the same steps (untimed), every step against the FP64 oracle
+    parity, ref = None, None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        runs = {name: eng.run(h0, dt, 1.0, fixed_dt=True, max_steps=args.steps)
+                for name, eng in (("fp64", eng64), ("mixed", engmx))}
+        ref = oracle_run(args.n, args.seed, args.steps, keep_steps=True)
+        parity = parity_vs_oracle(ref, runs)
     if rank != 0:
         barrier(world)
         if world > 1:
@@ -667,37 +724,55 @@ def main():
     v64 = world * N * r64["picard_its"] / (ms64 * 1e-3)
     vmx = world * N * rmx["picard_its"] / (msmx * 1e-3)
     ve2e = world * N * e2e["picard_its"] / (mse2e * 1e-3)
-    ach32 = b32 / t_it32 / 1e9
-    ach64 = b64 / t_it64 / 1e9
+    ach32 = l2_32 / t_it32 / 1e9
+    ach64 = l2_64 / t_it64 / 1e9
+    ach_asm = b_asm / t_asm / 1e9
     line = {
         "metric": METRIC, "value": vmx, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": msmx / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 Krylov + f64 refinement/assembly", "data": "synthetic (seeded log-normal Ks)",
-        "config": {"workload": f"2D Richards {args.n}^2 P1 triangles, VG soil, per-element log-normal Ks "
-                               f"(sigma_lnK 1, seed {args.seed}), h0 -1, top Dirichlet -0.1, dt 1e-4 fixed, "
-                               f"{args.steps} steps from the initial state",
-                   "nodes": N, "elements": E, "nnz": nnz, "picard_tol": 1e-6, "krylov_residual": 1e-8,
-                   "l2_policy": "L2 flushed (256 MiB write) between timed steps",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "loop_control": "host" if args.host_loop else "device (CUDA graph conditional nodes)"},
+        "config": dict(workload_config(args, world, args.host_loop), nnz=nnz),
         "fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "picard_its": r64["picard_its"],
-                 "krylov_its": r64["krylov_its"], "true_rel_residual": res_true["fp64"]},
+                 "krylov_its": r64["krylov_its"], "true_rel_residual": res_true["fp64"],
+                 "cg_kernel_share": r64["krylov_kernel_s"] / (ms64 * 1e-3)},
         "mixed": {"value": vmx, "picard_its": rmx["picard_its"], "inner_krylov_its": rmx["krylov_its"],
                   "refinements": rmx["refinements"], "true_rel_residual": res_true["mixed"],
-                  "rel_diff_vs_fp64": rel_diff, "speedup_vs_fp64": vmx / v64},
+                  "rel_diff_vs_fp64": rel_diff, "speedup_vs_fp64": vmx / v64,
+                  "cg_kernel_share": rmx["krylov_kernel_s"] / (msmx * 1e-3)},
         "status": {"fp64": r64["status"], "mixed": rmx["status"]},
         "e2e": {"value": ve2e, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
         "gpu_launches": rmx["launches"] + r64["launches"],
-        "roofline": {"bound": "hbm", "kernel": "one FP32 Jacobi-CG iteration of the resident pipelined CG kernel (mixed path inner solve)",
-                     "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak, "peak_kind": peak_kind,
-                     "traffic": load_traffic("cg_iteration_f32"), "algorithmic_bytes": b32,
-                     "seconds_per_iteration": t_it32,
-                     "fp64": {"achieved": ach64, "frac": ach64 / peak, "algorithmic_bytes": b64,
-                              "seconds_per_iteration": t_it64, "traffic": load_traffic("cg_iteration_f64")}},
+        "roofline": {"bound": "l2",
+                     "kernel": "pcg_resident_kernel: FP32 pipelined Jacobi-CG, the mixed path's inner solve "
+                               "(vectors in shared memory, matrix read from L2 every iteration)",
+                     "achieved": ach32, "peak": l2_peak32, "unit": "GB/s", "frac": ach32 / l2_peak32,
+                     "peak_kind": "measured in this run: wspm_read_probe, 16-byte L1-bypassing reads over a "
+                                  "buffer the size of the FP32 matrix, CUDA events",
+                     "l2_bytes_per_iteration": l2_32, "seconds_per_iteration": t_it32,
+                     "timing": "the kernel's own %globaltimer entry-to-exit durations summed over the timed "
+                               "steps / inner iterations",
+                     "traffic": load_traffic("cg_iteration_f32"),
+                     "hbm_convention": {"bytes_per_iteration": b32, "achieved": b32 / t_it32 / 1e9,
+                                        "peak": peak_hbm, "frac": b32 / t_it32 / 1e9 / peak_hbm,
+                                        "note": "B_spmv + 11 N w counted as HBM bytes; the kernel moves almost "
+                                                "none of them from HBM (traffic)"},
+                     "fp64": {"kernel": "cg_resident_kernel (FP64 single-reduction Jacobi-CG)", "bound": "l2",
+                              "achieved": ach64, "peak": l2_peak64, "frac": ach64 / l2_peak64,
+                              "l2_bytes_per_iteration": l2_64, "seconds_per_iteration": t_it64,
+                              "traffic": load_traffic("cg_iteration_f64"),
+                              "hbm_convention": {"bytes_per_iteration": b64, "frac": b64 / t_it64 / 1e9 / peak_hbm}},
+                     "assembly": {"kernel": "richards_rows_kernel (rows, Dirichlet, 1/diag, FP32 copy)",
+                                  "bound": "hbm", "achieved": ach_asm, "peak": peak_hbm, "frac": ach_asm / peak_hbm,
+                                  "peak_kind": peak_kind, "algorithmic_bytes": b_asm, "seconds": t_asm}},
         "clocks": clk.summary(),
     }
-    if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(args.n, args.seed)
+    if parity is not None:
+        line["fp64_err_vs_oracle"] = parity["fp64"]["h_rel_err"]
+        line["mixed_err_vs_oracle"] = parity["mixed"]["h_rel_err"]
+        line["parity"] = {"oracle": f"FP64 oracle, C + OpenMP restatement (oracle/richards2d.c), "
+                                    f"{int(ref['threads'])} threads", "steps": args.steps,
+                          "measure": "max over steps of ||x_gpu - x_oracle|| / ||x_oracle||", **parity}
+        line["cpu_baseline"] = cpu_baseline_from(ref, args.n, args.steps)
     if world == 1 and not args.no_adjoint:
         # second part of the metric: adjoint / forward time of the per-element-parameter run
         a = adjoint_measure(args.adjoint_n, args.adjoint_steps, args.seed, 0)

@@ -284,6 +284,15 @@ int wspm_cg_iterations(const wspm_pattern *pat, int32_t mode, const void *vals, 
                        const void *dinv, int32_t iters, double *work, int64_t work_doubles,
                        int32_t *iters_done, void *stream);
 
+/* Measurement hook (no reference counterpart): `reps` streaming passes of 16-byte
+ * reads over buf[0 .. n16) (buf 16-byte aligned), each of blocks_per_sm (1 or 2)
+ * x SMs blocks of 1024 threads reading its own contiguous share with loads that
+ * bypass L1; *out (device float, zeroed by the caller) receives a checksum.  With
+ * a buffer that fits in L2 the passes after the first are L2 hits: bench.py times
+ * two launches with CUDA events to obtain the L2 read bandwidth that bounds the
+ * resident CG kernels (their matrix stays in L2 between iterations).          */
+int wspm_read_probe(const void *buf, int64_t n16, int32_t reps, int32_t blocks_per_sm, float *out, void *stream);
+
 /* Allocation-free Jacobi-CG solve.  No counterpart in the reference: it is
  * for callers that cannot allocate device memory -- typically code running
  * inside a JAX program (the reference's runtime), whose allocator reserves
@@ -354,7 +363,9 @@ typedef struct wspm_picard_desc {
     double *dt_dev;            /* device double: the step's dt               */
     int32_t *result;           /* device int32[8]: status, picard its,
                                   total Krylov its, refinement its, ...     */
-    double *result_f64;        /* device double[4]: picard error, ...       */
+    double *result_f64;        /* device double[4]: picard error; seconds the
+                                  resident CG kernels ran in this step (their
+                                  %globaltimer, entry to exit of block 0) */
     double *Ks_inc;            /* with Ks_elem: wspm_picard_ks_inc_doubles(pat)
                                   doubles, Ks_elem gathered in incidence order
                                   at every step start; NULL without Ks_elem */

@@ -533,6 +533,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     extern __shared__ __align__(16) unsigned char rcg_smem[];
     __shared__ int s_off[MW > 0 ? MW : 1];
     T *const sm = reinterpret_cast<T *>(rcg_smem);
+    const unsigned long long t_entry = (blockIdx.x == 0 && threadIdx.x == 0) ? global_ns() : 0ull;
     const int n = a.A.n_rows;
     const int nb = gridDim.x;
     const int chunk = a.chunk;
@@ -792,6 +793,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
         st->k = k;
         st->status = ok ? status : WSPM_CUDA_ERROR;
         st->done = 1;
+        st->ns = global_ns() - t_entry;
     }
 }
 
@@ -1044,6 +1046,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
     __shared__ T s_scal[3];
     __shared__ int s_ok;
     T *const sm = reinterpret_cast<T *>(rcg_smem);
+    const unsigned long long t_entry = (blockIdx.x == 0 && threadIdx.x == 0) ? global_ns() : 0ull;
     const int n = a.A.n_rows;
     const int nb = gridDim.x;
     const int chunk = a.chunk;
@@ -1321,6 +1324,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
         st->k = k;
         st->status = ok ? status : WSPM_CUDA_ERROR;
         st->done = 1;
+        st->ns = global_ns() - t_entry;
     }
 }
 

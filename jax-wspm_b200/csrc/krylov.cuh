@@ -21,7 +21,16 @@ struct KrylovState {
     double inner_tol;                                      // refinement: tolerance of the next inner solve
     int k, done, status, exit_early, broken, steps, pad0, pad1;
     unsigned int ticket[4];
+    // resident CG kernels: %globaltimer ns from block 0's entry to its exit of the
+    // last launch; refinement state: the sum over the loop's inner solves
+    unsigned long long ns;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // Reduction tail of the refinement steps (the start, fused into the assembly or
 // as ir_residual_kernel, and ir_update_kernel): tot = (r.r, b.b); sets
@@ -35,11 +44,13 @@ __device__ __forceinline__ void ir_decide(const double (&tot)[2], KrylovState *i
         irs->k = 0;
         irs->steps = 0;
         irs->pad0 = 0;
+        irs->ns = 0ull;
         irs->status = WSPM_OK;
     } else {
         irs->k += 1;
         irs->steps += inner->k;
         irs->pad0 += 1;
+        irs->ns += inner->ns;
     }
     irs->rr = tot[0];
     // the next FP32 solve aims at the reduction the FP64 residual still needs,

@@ -46,6 +46,7 @@ struct PicardState {
     int cont;          // 1 while the Picard loop continues (read by the host-driven mode)
     int restart_m;     // GMRES restart length (launch accounting)
     unsigned int ticket[4];
+    unsigned long long krylov_ns;   // resident CG kernels: summed %globaltimer duration of this step's launches
 };
 
 __global__ void state_reset_kernel(unsigned int *words, int n_words) {
@@ -67,6 +68,7 @@ __global__ void step_init_kernel(SoilParams sp, int n, const double *__restrict_
         ps->tol = tol; ps->it = 0; ps->maxit = maxit; ps->relative = relative; ps->status = WSPM_OK;
         ps->krylov_total = 0; ps->refine_total = 0; ps->krylov_maxiter_hits = 0; ps->last_krylov_status = 0;
         ps->bodies = 0;
+        ps->krylov_ns = 0ull;
         ps->solver = solver;
         ps->cont = maxit > 0 ? 1 : 0;
         ps->restart_m = restart_m;
@@ -96,6 +98,7 @@ __global__ void __launch_bounds__(kBlock) picard_update_kernel(int n, const doub
             ps->err = err;
             ps->it += 1;
             if (irs) {
+                ps->krylov_ns += irs->ns;
                 ps->refine_total += irs->k;
                 ps->krylov_total += irs->steps;   // inner iterations accumulated by the refinement loop
                 ps->bodies += irs->pad0;          // inner CG launches accumulated by the refinement loop
@@ -103,6 +106,7 @@ __global__ void __launch_bounds__(kBlock) picard_update_kernel(int n, const doub
             } else {
                 const int kk = ks->k > 0 ? ks->k : 0;
                 ps->krylov_total += kk;
+                if (ps->solver == WSPM_SOLVER_CG) ps->krylov_ns += ks->ns;
                 // Krylov-loop launches: CG is one persistent kernel; BiCGSTAB 4 kernels per
                 // iteration; GMRES 4 m + 4 kernels per restart cycle
                 if (ps->solver == WSPM_SOLVER_CG) ps->bodies += 1;
@@ -132,6 +136,7 @@ __global__ void step_finish_kernel(int n, const double *__restrict__ h_m, double
         result[5] = ps->last_krylov_status;
         result[6] = ps->bodies;
         result_f64[0] = ps->err;
+        result_f64[1] = 1e-9 * (double)ps->krylov_ns;
     }
 }
 

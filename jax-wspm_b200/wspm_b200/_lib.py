@@ -137,6 +137,7 @@ _SIGS = {
                                           c_double, c_int32, c_int32, c_void_p, c_int64, c_void_p, c_void_p]),
     "wspm_cg_iterations": (c_int32, [P(WspmPattern), c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                                      c_void_p, c_int64, c_void_p, c_void_p]),
+    "wspm_read_probe": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_void_p]),
     "wspm_cg_solve_noalloc": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double,
                                         c_int32, c_void_p, c_void_p]),
     "wspm_picard_workspace_doubles": (c_int64, [c_int32, c_int32]),

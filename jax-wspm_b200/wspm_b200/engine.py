@@ -166,7 +166,7 @@ class PicardEngine:
         f = self.result_f64.cpu().numpy()
         out = {"status": int(r[0]), "iterations": int(r[1]), "krylov_iterations": int(r[2]),
                "refinements": int(r[3]), "krylov_cap_hits": int(r[4]), "krylov_status": int(r[5]),
-               "krylov_launches": int(r[6]), "error": float(f[0])}
+               "krylov_launches": int(r[6]), "error": float(f[0]), "krylov_kernel_seconds": float(f[1])}
         out["launches"] = self.kernel_launches(out["iterations"], out["refinements"], out["krylov_launches"])
         return out
 

@@ -94,3 +94,18 @@ def validate_elements(points, elements):
     if elements.size and (elements.min() < 0 or elements.max() >= points.shape[0]):
         raise ValueError("Element indices out of bounds")
     return True
+
+
+KS_MEAN = 0.0922       # m/day, the van Genuchten unit-square soil's saturated conductivity
+
+
+def lognormal_ks_square(n, seed, sigma_lnk=1.0, ks_mean=KS_MEAN):
+    """The 1024^2-style Richards workload on an n x n unit square: (points, triangles, Ks per element, top nodes).
+
+    Per-element saturated conductivity ln Ks ~ N(ln ks_mean, sigma_lnk^2), i.i.d., drawn with
+    numpy.random.default_rng(seed); the top nodes (y == 1) carry the Dirichlet value."""
+    pts, tri = structured_triangles(n, 1.0)
+    rng = np.random.default_rng(seed)
+    Ks = np.exp(np.log(ks_mean) + sigma_lnk * rng.standard_normal(len(tri)))
+    top = np.where(pts[:, 1] == 1.0)[0]
+    return pts, tri, Ks, top

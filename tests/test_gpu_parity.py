@@ -372,8 +372,8 @@ def test_picard_engine_matches_oracle_vg_unit_square():
     eng = PicardEngine(DeviceMesh(pts, tri), "vg", opic.VG_UNIT_PHI, bc_val=bc, solver="cg", precond="jacobi")
     res = eng.run(h0, 1e-4, 0.02)
     np.testing.assert_array_equal(res["iterations"], ref["iterations"])
-    np.testing.assert_allclose(res["pressure_head"], ref["pressure_head"], rtol=1e-9, atol=1e-10)
-    np.testing.assert_allclose(res["theta"], ref["theta"], rtol=1e-9, atol=1e-11)
+    np.testing.assert_allclose(res["pressure_head"], ref["pressure_head"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(res["theta"], ref["theta"], rtol=1e-10, atol=1e-12)
 
 
 @pytest.mark.parametrize("solver", ["bicgstab", "gmres"])
