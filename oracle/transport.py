@@ -274,3 +274,40 @@ def peclet_courant(points, triangles, qx, qz, theta, Dxx, Dzz, dt):
     pe = np.maximum(vx * h / (2 * Dxx[t]), vz * h / (2 * Dzz[t])).max()
     cr = np.maximum(vx * dt / h, vz * dt / h).max()
     return float(pe), float(cr)
+
+
+def coupled_time_loop(points, tri, phi, neumann_nodes, cauchy_nodes, dt0, tmax, DL=0.5, DT=0.1, Dm=0.0,
+                      c_init=0.1, c_inlet=1.0, neumann_flux=-0.1, cauchy_flux=-0.1, h0=-1.3, solver="gmres",
+                      precond="none", tol=1e-10, maxiter=100, restart=30, m_it=5, M_it=7, lambda_amp=2.0,
+                      lambda_red=0.5, max_steps=None):
+    """CoupledSolver.solve, src/solvers/coupled_solver_v2.py:223-300, on the oracle's step functions.
+
+    Per step: theta_n at the previous head; the Richards step with the Neumann inflow and the absolute
+    Picard error (< 1e-4, at most 100 iterations, :80-140); fluxes and dispersion at the new head; the
+    solute step (:147-197); dt_new from the iteration count with the floor max(dt_new, 1e-6) (:200-221;
+    the reference's upper clamp to 0.5 is overwritten by that line and has no effect); the clock advances
+    by the step's own dt, then dt = dt_new (:291-292).  Returns per-step lists: time after the step,
+    Picard error, iterations, dt_new, and the heads and concentrations."""
+    n = points.shape[0]
+    h_n = float(h0) * np.ones(n)
+    c_n = float(c_init) * np.ones(n)
+    kw = dict(solver=solver, precond=precond, tol=tol, maxiter=maxiter, restart=restart)
+    out = {k: [] for k in ("time", "error", "iterations", "dt", "pressure_head", "solute")}
+    t, dt, steps = 0.0, float(dt0), 0
+    while t < tmax and (max_steps is None or steps < max_steps):
+        _, _, th_n = van_genuchten_model(h_n, phi)
+        h, err, it = richards_neumann_step(points, tri, h_n, th_n, dt, phi, neumann_nodes, neumann_flux,
+                                           picard_tol=1e-4, picard_max=100, **kw)
+        qx, qz, aq, Dxx, Dxz, Dzz, th = fluxes_and_dispersion(points, tri, h, phi, DL, DT, Dm)
+        c = solute_step(points, tri, c_n, th, th_n, qx, qz, Dxx, Dxz, Dzz, dt, cauchy_nodes, cauchy_flux, c_inlet,
+                        **kw)
+        dt_r = lambda_amp * dt if it <= m_it else (dt if it <= M_it else lambda_red * dt)
+        dt_new = max(dt_r, 1e-6)
+        h_n, c_n = h, c
+        t += dt
+        dt = dt_new
+        steps += 1
+        for k, v in (("time", t), ("error", float(err)), ("iterations", it), ("dt", dt_new),
+                     ("pressure_head", h), ("solute", c)):
+            out[k].append(v)
+    return out
