@@ -264,10 +264,9 @@ def load_traffic(key):
 
 
 def host_cores():
-    try:
-        return len(os.sched_getaffinity(0))
-    except AttributeError:
-        return os.cpu_count() or 1
+    """Host cores this process may use (affinity mask capped by a cgroup CPU quota)."""
+    from oracle import richards2d_c
+    return richards2d_c.default_threads()
 
 
 def oracle_run(n, seed, steps, keep_steps=False, threads=None):

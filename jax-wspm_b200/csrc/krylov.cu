@@ -286,8 +286,23 @@ struct RcgArgs {
     GridBarrier *bar;
     double tol, atol;
     const double *tol_dev; // when set, the relative tolerance is read here
+    const int *skip;       // when set and nonzero at launch: no iteration, k = 0 (refinement already done)
     int maxiter, zero_x0;
 };
+
+// Early exit of a resident CG launch whose refinement loop has already met its
+// tolerance: every block reads the same word (written before the launch) and
+// returns before touching any barrier; block 0 records an empty solve.
+__device__ __forceinline__ bool resident_skip(const int *skip, KrylovState *st) {
+    if (!skip || *(volatile const int *)skip == 0) return false;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->k = 0;
+        st->status = WSPM_OK;
+        st->done = 1;
+        st->ns = 0ull;
+    }
+    return true;
+}
 
 constexpr int kRcgBlock = 512;    // 128 registers: the 2D instances run without spills
 
@@ -533,6 +548,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     extern __shared__ __align__(16) unsigned char rcg_smem[];
     __shared__ int s_off[MW > 0 ? MW : 1];
     T *const sm = reinterpret_cast<T *>(rcg_smem);
+    if (resident_skip(a.skip, a.st)) return;
     const unsigned long long t_entry = (blockIdx.x == 0 && threadIdx.x == 0) ? global_ns() : 0ull;
     const int n = a.A.n_rows;
     const int nb = gridDim.x;
@@ -849,7 +865,7 @@ static cudaError_t rcg_launch(const RcgPlan &pl, const RcgArgs<T> &a, cudaStream
 template <typename T>
 int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
                           const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
-                          const double *tol_dev, cudaStream_t st) {
+                          const double *tol_dev, cudaStream_t st, const int *skip) {
     // the 16-byte row groups need 16-byte aligned arrays
     const uintptr_t al = (uintptr_t)vals | (uintptr_t)x | (uintptr_t)w.z | (uintptr_t)w.r | (uintptr_t)w.p0 |
                          (uintptr_t)w.p1 | (uintptr_t)w.q | (uintptr_t)(dinv ? dinv : vals);
@@ -861,6 +877,7 @@ int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double
     a.bar = (GridBarrier *)&w.st->ticket[0];
     a.zflag = reinterpret_cast<unsigned int *>(w.partials + 16 * 1024);    // after 11 * grid <= 11264 slots
     a.tol = tol; a.atol = atol; a.tol_dev = tol_dev; a.maxiter = maxiter; a.zero_x0 = zero_x0 ? 1 : 0;
+    a.skip = skip;
     // global homes of the vectors that stay off chip (x: the caller's array; M: read in place)
     a.gvec[kVR] = w.r; a.gvec[kVP] = w.p0; a.gvec[kVS] = w.p1; a.gvec[kVW] = w.q;
     a.gvec[kVX] = x;
@@ -878,10 +895,10 @@ int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double
 
 template int cg_persistent_enqueue<double>(const Sell &, const double *, const double *, const double *, double *,
                                            const double *, const CgBuffers<double> &, double, double, int, bool,
-                                           const double *, cudaStream_t);
+                                           const double *, cudaStream_t, const int *);
 template int cg_persistent_enqueue<float>(const Sell &, const float *, const float *, const double *, float *,
                                           const float *, const CgBuffers<float> &, double, double, int, bool,
-                                          const double *, cudaStream_t);
+                                          const double *, cudaStream_t, const int *);
 
 // ---------------------------------------------------------------- pipelined CG
 // Pipelined Jacobi-CG (Ghysels & Vanroose, Parallel Computing 40 (2014)
@@ -927,6 +944,7 @@ struct PcgArgs {
     GridBarrier *bar;
     double tol, atol;
     const double *tol_dev;
+    const int *skip;       // as RcgArgs::skip
     int maxiter, zero_x0;
 };
 
@@ -1046,6 +1064,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
     __shared__ T s_scal[3];
     __shared__ int s_ok;
     T *const sm = reinterpret_cast<T *>(rcg_smem);
+    if (resident_skip(a.skip, a.st)) return;
     const unsigned long long t_entry = (blockIdx.x == 0 && threadIdx.x == 0) ? global_ns() : 0ull;
     const int n = a.A.n_rows;
     const int nb = gridDim.x;
@@ -1349,7 +1368,7 @@ static cudaError_t pcg_launch(int grid, size_t smem, const PcgArgs<T> &a, cudaSt
 template <typename T>
 int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
                            const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
-                           const double *tol_dev, cudaStream_t st, bool warp_specialized) {
+                           const double *tol_dev, cudaStream_t st, bool warp_specialized, const int *skip) {
     if (A.n_diags <= 0 || A.n_diags > 16) return WSPM_UNSUPPORTED;       // DIA patterns only
     const uintptr_t al = (uintptr_t)vals | (uintptr_t)x | (uintptr_t)w.z | (uintptr_t)w.q |
                          (uintptr_t)(dinv ? dinv : vals);
@@ -1375,6 +1394,7 @@ int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const doubl
     a.bar = (GridBarrier *)&w.st->ticket[0];
     a.flag = reinterpret_cast<unsigned int *>(w.partials + 16 * 1024);   // after 7 * grid <= 7168 slots
     a.tol = tol; a.atol = atol; a.tol_dev = tol_dev; a.maxiter = maxiter; a.zero_x0 = zero_x0 ? 1 : 0;
+    a.skip = skip;
     const size_t smem = (size_t)(nsv * per_vec);
     cudaError_t e = cudaSuccess;
     const bool xs = nsv == kNumPcgVec;
@@ -1405,10 +1425,10 @@ template bool pcg_eligible<double>(const Sell &);
 
 template int pcg_persistent_enqueue<double>(const Sell &, const double *, const double *, const double *, double *,
                                             const double *, const CgBuffers<double> &, double, double, int, bool,
-                                            const double *, cudaStream_t, bool);
+                                            const double *, cudaStream_t, bool, const int *);
 template int pcg_persistent_enqueue<float>(const Sell &, const float *, const float *, const double *, float *,
                                            const float *, const CgBuffers<float> &, double, double, int, bool,
-                                           const double *, cudaStream_t, bool);
+                                           const double *, cudaStream_t, bool, const int *);
 
 // ---------------------------------------------------------------- BiCGSTAB (FP64)
 template <int MW>

@@ -120,10 +120,13 @@ void cg_enqueue_body(const Sell &A, const T *vals, T *x, const T *dinv, const Cg
 // Whole CG solve in one cooperative launch (x0 in x unless zero_x0); the final
 // scalars, iteration count and status are written to w.st.  The barrier words
 // live in w.st->ticket and must be zero before the launch (state reset).
+// skip: optional device word; nonzero when the launch starts means "no solve"
+// (k = 0), for the first refinement of a loop whose start already met its
+// tolerance (the launch is a plain graph node, not inside the loop's WHILE node).
 template <typename T>
 int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
                           const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
-                          const double *tol_dev, cudaStream_t st);
+                          const double *tol_dev, cudaStream_t st, const int *skip = nullptr);
 
 // Pipelined Jacobi-CG (one reduction per iteration, overlapped with the SpMV)
 // in one cooperative launch, same buffers and state as cg_persistent_enqueue.
@@ -132,7 +135,8 @@ int cg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double
 template <typename T>
 int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
                            const CgBuffers<T> &w, double tol, double atol, int maxiter, bool zero_x0,
-                           const double *tol_dev, cudaStream_t st, bool warp_specialized = true);
+                           const double *tol_dev, cudaStream_t st, bool warp_specialized = true,
+                           const int *skip = nullptr);
 // Whether pcg_persistent_enqueue accepts the pattern for element type T (DIA
 // with at most 16 diagonals, at least six per-block vectors on chip).
 template <typename T>

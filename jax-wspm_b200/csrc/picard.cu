@@ -1,12 +1,12 @@
 // One implicit Richards time step as a single CUDA graph.
 //
-//   step_init:  theta_n = theta(h_n); h_m = h_n; Picard counters reset
+//   step_init:  theta_n = theta(h_n); h_m = h_n; C, K, theta_m at h_m; Picard counters reset
 //   WHILE picard (err >= tol && it < maxit):                richards_solver_v2.py:160-165
-//     soil:       C, K, theta_m at h_m                       :114-115
 //     assembly:   A, b, Dirichlet rows, Jacobi 1/diag        :118-146
 //     Krylov:     FP64 CG | BiCGSTAB | GMRES(m), x0 = h_m    :148-153
 //                 or FP32 CG inside FP64 iterative refinement on the true residual
 //     update:     err = ||x - h_m|| (/ ||x||); h_m = x; it++ :155
+//                 and the soil fields C, K, theta_m at the new h_m (:114-115 of the next iteration)
 //   step_finish: h_n = h_m, counters to the caller's result words
 //
 // Every loop is a conditional WHILE node whose handle is cleared by the
@@ -53,15 +53,21 @@ __global__ void state_reset_kernel(unsigned int *words, int n_words) {
     for (int i = threadIdx.x; i < n_words; i += blockDim.x) words[i] = 0u;
 }
 
+// theta_n = theta(h_n), h_m = h_n, and the soil fields of the first Picard
+// iteration (C, K, theta_m at h_m = h_n: theta_m = theta_n).
 __global__ void step_init_kernel(SoilParams sp, int n, const double *__restrict__ h_n, double *theta_n, double *h_m,
-                                 PicardState *ps, double tol, int maxit, int relative, int solver, int restart_m,
-                                 cudaGraphConditionalHandle cond, int use_cond) {
+                                 double *C, double *K, double *theta_m, PicardState *ps, double tol, int maxit,
+                                 int relative, int solver, int restart_m, cudaGraphConditionalHandle cond,
+                                 int use_cond) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double c, k, t;
         const double h = h_n[i];
         soil_eval(sp, h, c, k, t);
         theta_n[i] = t;
         h_m[i] = h;
+        C[i] = c;
+        K[i] = k;
+        theta_m[i] = t;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ps->err = __longlong_as_double(0x7ff0000000000000ULL);  // +inf, like the reference's carry
@@ -77,7 +83,10 @@ __global__ void step_init_kernel(SoilParams sp, int n, const double *__restrict_
     }
 }
 
+// Picard norm and test; h_m = x, and the soil fields of the next Picard
+// iteration at the new h_m (C, K, theta_m; unused after the last iteration).
 __global__ void __launch_bounds__(kBlock) picard_update_kernel(int n, const double *__restrict__ x, double *h_m,
+                                                               SoilParams sp, double *C, double *K, double *theta_m,
                                                                double *partials, PicardState *ps,
                                                                const KrylovState *ks, const KrylovState *irs,
                                                                cudaGraphConditionalHandle cond, int use_cond) {
@@ -88,6 +97,11 @@ __global__ void __launch_bounds__(kBlock) picard_update_kernel(int n, const doub
         v[0] += d * d;
         v[1] += xi * xi;
         h_m[i] = xi;
+        double c, k, t;
+        soil_eval(sp, xi, c, k, t);
+        C[i] = c;
+        K[i] = k;
+        theta_m[i] = t;
     }
     if (publish_partials<double, 2>(v, partials, &ps->ticket[0])) {
         double tot[2];
@@ -172,13 +186,18 @@ __global__ void __launch_bounds__(kBlock) ir_residual_kernel(Sell A, const doubl
 }
 
 // After an FP32 correction d: x += d and r -= A d (FP64; equal to b - A x up to
-// FP64 rounding, without re-reading b and the previous x).
+// FP64 rounding, without re-reading b and the previous x).  skip: as for the
+// resident CG launch before it (the first refinement, outside the WHILE node):
+// nonzero at launch = the loop is already done, nothing to apply.
 template <int MW>
 __global__ void __launch_bounds__(kBlock) ir_update_kernel(Sell A, const double *__restrict__ vals,
                                                            const float *__restrict__ d, double *x, double *r,
                                                            double *partials, KrylovState *irs,
                                                            const KrylovState *inner, double tol, double inner_floor,
-                                                           int maxit, cudaGraphConditionalHandle cond, int use_cond) {
+                                                           int maxit, const int *skip,
+                                                           cudaGraphConditionalHandle cond, int use_cond) {
+    // every block reads the word before any block can reach the reduction tail that rewrites it
+    if (skip && *(volatile const int *)skip) return;
     double v[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
         const double ri = r[i] - sell_row_dot<double, MW>(A, vals, i, [&](int c) { return (double)d[c]; });
@@ -198,8 +217,7 @@ struct PicardPlan {
     wspm_pattern pat;
     wspm_picard_desc d;
     wspm_edges neumann, drainage;   // copies (n_bnodes == 0: unused)
-    SoilParams sp_field;   // soil for the assembly (Ks = 1 when Ks_elem is given)
-    SoilParams sp_theta;   // soil for theta_n
+    SoilParams sp_field;   // soil law of the step (theta_n, and C, K, theta_m for the assembly)
     double s[4], mc[4];
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
@@ -253,12 +271,12 @@ int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
 // outer loop measures the true FP64 residual, so the pipelined recurrences
 // cannot hide an inaccurate inner solve), else the single-reduction form.
 static void inner_cg_enqueue(const Sell &A, const wspm_picard_desc &d, PicardPlan *P, const float *dv32,
-                             cudaStream_t s) {
+                             cudaStream_t s, const int *skip = nullptr) {
     const int rc = pcg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol,
-                                                 0.0, d.inner_maxiter, true, &P->irs->inner_tol, s);
+                                                 0.0, d.inner_maxiter, true, &P->irs->inner_tol, s, true, skip);
     if (rc == WSPM_UNSUPPORTED)
         cg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
-                                     d.inner_maxiter, true, &P->irs->inner_tol, s);
+                                     d.inner_maxiter, true, &P->irs->inner_tol, s, skip);
 }
 
 static int build_picard_graph(PicardPlan *P) {
@@ -284,10 +302,10 @@ static int build_picard_graph(PicardPlan *P) {
         if (P->irs) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)P->irs, (int)(sizeof(KrylovState) / 4));
     }
     if (P->Ks_inc) launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, cs);
-    step_init_kernel<<<nb, kBlock, 0, cs>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
-                                            d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, hp, 1);
+    step_init_kernel<<<nb, kBlock, 0, cs>>>(P->sp_field, n, d.h_n, d.theta_n, d.h_m, d.C, d.K, d.theta_m, P->ps,
+                                            d.picard_tol, d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, hp,
+                                            1);
     if (e == cudaSuccess) e = capture_while(cs, hp, [&](cudaStream_t bs) {
-        launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, bs);
         cudaGraphConditionalHandle hir = cudaGraphConditionalHandle();
         if (d.mixed) make_cond_handle(bs, &hir);
         const RefineStart rs = refine_start(P, hir, 1);
@@ -309,14 +327,23 @@ static int build_picard_graph(PicardPlan *P) {
                                                                                   P->partials, P->irs, d.krylov_tol,
                                                                                   d.inner_tol, d.refine_maxiter, hir,
                                                                                   1));
+            // the first correction as plain nodes (both kernels return at once when the start already met
+            // the tolerance), the rest inside the WHILE node: one body launch fewer per Picard iteration
+            const float *dv32 = dinv ? P->dinv32 : nullptr;
+            inner_cg_enqueue(A, d, P, dv32, bs, &P->irs->done);
+            WSPM_WIDTH_DISPATCH(A.max_width,
+                                ir_update_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, P->x32, d.x, P->r64,
+                                                                            P->partials, P->irs, P->cg32.st,
+                                                                            d.krylov_tol, d.inner_tol,
+                                                                            d.refine_maxiter, &P->irs->done, hir,
+                                                                            1));
             capture_while(bs, hir, [&](cudaStream_t ibs) {
-                const float *dv32 = dinv ? P->dinv32 : nullptr;
                 inner_cg_enqueue(A, d, P, dv32, ibs);
                 WSPM_WIDTH_DISPATCH(A.max_width,
                                     ir_update_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, P->x32, d.x, P->r64,
                                                                                  P->partials, P->irs, P->cg32.st,
                                                                                  d.krylov_tol, d.inner_tol,
-                                                                                 d.refine_maxiter, hir, 1));
+                                                                                 d.refine_maxiter, nullptr, hir, 1));
             });
             irs = P->irs;
         } else if (d.solver == WSPM_SOLVER_BICGSTAB) {
@@ -343,7 +370,8 @@ static int build_picard_graph(PicardPlan *P) {
                                           d.krylov_maxiter, false, nullptr, bs);
             ks = P->cg64.st;
         }
-        picard_update_kernel<<<nb, kBlock, 0, bs>>>(n, d.x, d.h_m, P->partials, P->ps, ks, irs, hp, 1);
+        picard_update_kernel<<<nb, kBlock, 0, bs>>>(n, d.x, d.h_m, P->sp_field, d.C, d.K, d.theta_m, P->partials,
+                                                    P->ps, ks, irs, hp, 1);
     });
     step_finish_kernel<<<nb, kBlock, 0, cs>>>(n, d.h_m, d.h_n, P->ps, d.result, d.result_f64);
     cudaGraph_t out = nullptr;
@@ -384,10 +412,10 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
     for (KrylovState *k : sts)
         if (k) state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
     if (P->Ks_inc) launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, st);
-    step_init_kernel<<<nb, kBlock, 0, st>>>(P->sp_theta, n, d.h_n, d.theta_n, d.h_m, P->ps, d.picard_tol,
-                                            d.picard_maxiter, d.picard_relative, d.solver, P->gm.m, none, 0);
+    step_init_kernel<<<nb, kBlock, 0, st>>>(P->sp_field, n, d.h_n, d.theta_n, d.h_m, d.C, d.K, d.theta_m, P->ps,
+                                            d.picard_tol, d.picard_maxiter, d.picard_relative, d.solver, P->gm.m,
+                                            none, 0);
     for (int it = 0; it < d.picard_maxiter && rc == WSPM_OK; ++it) {
-        launch_soil(P->sp_field, d.h_m, n, d.C, d.K, d.theta_m, st);
         const RefineStart rs = refine_start(P, none, 0);
         const bool fused = fuse_refine_start(P);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
@@ -414,7 +442,7 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                                     ir_update_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, P->x32, d.x, P->r64,
                                                                                 P->partials, P->irs, P->cg32.st,
                                                                                 d.krylov_tol, d.inner_tol,
-                                                                                d.refine_maxiter, none, 0));
+                                                                                d.refine_maxiter, nullptr, none, 0));
             }
             irs = P->irs;
         } else {
@@ -448,7 +476,8 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
             }
             ks = kst;
         }
-        picard_update_kernel<<<nb, kBlock, 0, st>>>(n, d.x, d.h_m, P->partials, P->ps, ks, irs, none, 0);
+        picard_update_kernel<<<nb, kBlock, 0, st>>>(n, d.x, d.h_m, P->sp_field, d.C, d.K, d.theta_m, P->partials,
+                                                    P->ps, ks, irs, none, 0);
         if (rc == WSPM_OK && (rc = read_flag(&P->ps->cont, st, &flag, pinned)) == WSPM_OK && !flag) break;
     }
     step_finish_kernel<<<nb, kBlock, 0, st>>>(n, d.h_m, d.h_n, P->ps, d.result, d.result_f64);
@@ -507,8 +536,7 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     P->d.mesh = &P->mesh;
     P->d.pat = &P->pat;
     P->sp_field.model = d.soil_model;
-    P->sp_theta.model = d.soil_model;
-    for (int j = 0; j < 6; ++j) P->sp_field.p[j] = P->sp_theta.p[j] = d.phi[j];
+    for (int j = 0; j < 6; ++j) P->sp_field.p[j] = d.phi[j];
     quadrature_constants(d.mesh->dim, d.quad_points, d.weights, d.nq, P->s, P->mc);
     // carve the workspace
     double *p = d.work;
@@ -635,20 +663,23 @@ int build_mixed_graph(const wspm_pattern *pat, const double *vals, const float *
         WSPM_WIDTH_DISPATCH(A.max_width,
                             ir_residual_kernel<MW><<<nb, kBlock, 0, cs>>>(A, vals, b, x, x, r64, dinv, dv32, partials,
                                                                           irs, tol, inner_tol, refine_maxiter, h, 1));
-        if (e == cudaSuccess)
-            e = capture_while(cs, h, [&](cudaStream_t bs) {
-                int rc = WSPM_UNSUPPORTED;
-                if (pipelined)
-                    rc = pcg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0,
-                                                       inner_maxiter, true, &irs->inner_tol, bs);
-                if (rc == WSPM_UNSUPPORTED)
-                    cg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0, inner_maxiter,
-                                                 true, &irs->inner_tol, bs);
-                WSPM_WIDTH_DISPATCH(A.max_width,
-                                    ir_update_kernel<MW><<<nb, kBlock, 0, bs>>>(A, vals, x32, x, r64, partials, irs,
-                                                                                cg32.st, tol, inner_tol,
-                                                                                refine_maxiter, h, 1));
-            });
+        // one correction: the FP32 solve (skipped when `skip` is set at launch) and x += d, r -= A d
+        auto correction = [&](cudaStream_t bs, const int *skip) {
+            int rc = WSPM_UNSUPPORTED;
+            if (pipelined)
+                rc = pcg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0,
+                                                   inner_maxiter, true, &irs->inner_tol, bs, true, skip);
+            if (rc == WSPM_UNSUPPORTED)
+                cg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0, inner_maxiter,
+                                             true, &irs->inner_tol, bs, skip);
+            WSPM_WIDTH_DISPATCH(A.max_width,
+                                ir_update_kernel<MW><<<nb, kBlock, 0, bs>>>(A, vals, x32, x, r64, partials, irs,
+                                                                            cg32.st, tol, inner_tol, refine_maxiter,
+                                                                            skip, h, 1));
+        };
+        // the first correction as plain nodes, the rest inside the WHILE node
+        if (e == cudaSuccess) correction(cs, &irs->done);
+        if (e == cudaSuccess) e = capture_while(cs, h, [&](cudaStream_t bs) { correction(bs, nullptr); });
         mixed_result_kernel<<<1, 32, 0, cs>>>(irs, result);
         cudaGraph_t out = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(cs, &out);

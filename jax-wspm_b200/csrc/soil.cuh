@@ -19,7 +19,18 @@ __device__ __forceinline__ void soil_eval(const SoilParams &sp, double h,
                                           double &C, double &K, double &theta) {
     if (sp.model == WSPM_SOIL_VAN_GENUCHTEN) {
         const double alpha = sp.p[0], thS = sp.p[1], thR = sp.p[2], n = sp.p[3], m = sp.p[4], Ks = sp.p[5];
-        if (h < 0.0) {
+        if (h < 0.0 && n == 2.0 && m == 0.5) {
+            // n = 2, m = 1/2 (the Mualem pair for n = 2): every power is a square or a square root.
+            //   a = (alpha|h|)^2, Se = (1 + a)^-1/2, (a/(1+a))^1/2 = alpha|h| Se,
+            //   1 - (a/(1+a))^1/2 = Se^2 / (1 + alpha|h| Se)   (no cancellation at large a)
+            const double ah = alpha * fabs(h);
+            const double onep = 1.0 + ah * ah;
+            const double tm = 1.0 / sqrt(onep);
+            theta = (thS - thR) * tm + thR;
+            const double t = (tm * tm) / (1.0 + ah * tm);
+            K = Ks * (sqrt(tm) * (t * t));
+            C = (thS - thR) * alpha * m * n * ah * (tm / onep);
+        } else if (h < 0.0) {
             // Same functions as the reference, with its six pow() calls reduced algebraically:
             //   a = (alpha|h|)^n, Se = (1 + a)^-m, Se^(1/m) = 1/(1 + a), 1 - Se^(1/m) = a/(1 + a)
             //   K = Ks sqrt(Se) (1 - (a/(1+a))^m)^2,  (a/(1+a))^m = exp(m log(a/(1+a)))

@@ -144,8 +144,9 @@ class PicardEngine:
     def kernel_launches(self, its, refinements, krylov_launches):
         """Kernels the step graph launched (device counters; graph structure in picard.cu).
 
-        Per step: state resets, step_init, step_finish.  Per Picard iteration: soil, assembly,
-        edge-term kernels, the x0 copy, the Krylov init kernels, picard_update.  The Krylov
+        Per step: state resets, step_init, step_finish.  Per Picard iteration: assembly, edge-term
+        kernels, the x0 copy, the Krylov init kernels, picard_update (which also evaluates the soil
+        law at the new iterate).  The Krylov
         loop itself is counted on the device (one persistent kernel per CG solve, 4 kernels per
         BiCGSTAB iteration, 4m+4 per GMRES cycle); each refinement adds correction + residual.
         The mixed path's refinement start is one kernel either way (the stand-alone residual, or
@@ -154,12 +155,12 @@ class PicardEngine:
         cfg = self.config
         e = self._edge_kernels
         if cfg["mixed"]:
-            return 5 + (5 + e) * its + 2 * refinements + krylov_launches
+            return 5 + (4 + e) * its + 2 * refinements + krylov_launches
         if cfg["solver"] == "gmres":
-            return 4 + (6 + e) * its + krylov_launches
-        if cfg["solver"] == "bicgstab":
             return 4 + (5 + e) * its + krylov_launches
-        return 4 + (4 + e) * its + krylov_launches
+        if cfg["solver"] == "bicgstab":
+            return 4 + (4 + e) * its + krylov_launches
+        return 4 + (3 + e) * its + krylov_launches
 
     def read_result(self):
         r = self.result.cpu().numpy()

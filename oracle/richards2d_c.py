@@ -54,6 +54,31 @@ def max_threads():
     return int(_load().oracle_max_threads())
 
 
+def default_threads():
+    """Host cores this process may use: the affinity mask, capped by a cgroup CPU quota when one is set
+    (OpenMP's default would start one spinning thread per visible core even under a smaller quota)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    quota = None
+    try:
+        q, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]      # cgroup v2: "max 100000" or "Q P"
+        if q != "max":
+            quota = int(q) / int(period)
+    except (OSError, ValueError):
+        try:
+            q = int(open("/sys/fs/cgroup/cpu/cpu.cfs_quota_us").read())    # cgroup v1
+            period = int(open("/sys/fs/cgroup/cpu/cpu.cfs_period_us").read())
+            if q > 0:
+                quota = q / period
+        except (OSError, ValueError):
+            pass
+    if quota is not None:
+        n = max(1, min(n, int(quota)))
+    return n
+
+
 def run_vg_fixed_dt(points, triangles, phi, bc_nodes, bc_vals, h0, dt, n_steps, Ks_elem=None, picard_tol=1e-6,
                     picard_max=100, picard_relative=True, cg_tol=1e-8, cg_maxiter=100000, threads=0,
                     keep_steps=False):
@@ -74,6 +99,7 @@ def run_vg_fixed_dt(points, triangles, phi, bc_nodes, bc_vals, h0, dt, n_steps, 
     pits = np.zeros(n_steps, dtype=np.int32)
     kits = np.zeros(n_steps, dtype=np.int64)
     sec = ctypes.c_double(0.0)
+    threads = int(threads) if threads and threads > 0 else default_threads()
     ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
     rc = lib.oracle_richards2d_vg_run(n, e, ptr(pts), ptr(tri), ptr(ks), ptr(ph), ptr(bn), ptr(bv), bn.size,
                                       float(dt), int(n_steps), float(picard_tol), int(picard_max),
@@ -81,5 +107,4 @@ def run_vg_fixed_dt(points, triangles, phi, bc_nodes, bc_vals, h0, dt, n_steps, 
                                       ptr(hs), ptr(pits), ptr(kits), ctypes.byref(sec))
     if rc != 0:
         raise RuntimeError(f"oracle_richards2d_vg_run failed ({rc})")
-    return {"h": h, "h_steps": hs, "picard_its": pits, "cg_its": kits, "seconds": sec.value,
-            "threads": threads if threads > 0 else max_threads()}
+    return {"h": h, "h_steps": hs, "picard_its": pits, "cg_its": kits, "seconds": sec.value, "threads": threads}
