@@ -247,23 +247,27 @@ int wspm_krylov_solve(const wspm_pattern *pat, const double *vals,
                       int32_t restart, double *work, int64_t work_doubles,
                       int32_t *result, void *stream);
 
-/* One linear system in mixed precision (the reference's solve_system with
- * cg + jacobi, src/solvers/solver_types.py:7-67, at a tolerance FP32 alone
- * cannot reach): FP32 Jacobi-CG corrections inside FP64 iterative refinement.
- * x = x0 (in x), r = b - A x in FP64; while ||r|| > tol ||b||: solve A d = r in
- * FP32 -- the pipelined CG on DIA patterns whose vectors fit on chip, the
- * single-reduction CG otherwise -- to the reduction still needed (never
- * tighter than inner_tol, at most inner_maxiter iterations), then x += d and
- * r -= A d in FP64; at most refine_maxiter corrections.  vals32: the FP32 copy
- * of vals in the same layout, or NULL (made in the workspace on each call).
- * dinv: FP64 Jacobi 1/diag, or NULL for no preconditioner.  result (device
- * int32[4]): status, FP32 CG iterations, corrections, 0.  Captured once per
- * argument set as a CUDA graph and replayed on `stream`; no host sync.     */
-int64_t wspm_krylov_mixed_workspace_doubles(int32_t n_rows, int64_t nnz_padded);
+/* One linear system in mixed precision (the reference's solve_system,
+ * src/solvers/solver_types.py:7-67, with cg / bicgstab / gmres at a tolerance
+ * FP32 alone cannot reach): FP32 Krylov corrections inside FP64 iterative
+ * refinement.  x = x0 (in x), r = b - A x in FP64; while ||r|| > tol ||b||:
+ * solve A d = r in FP32 from d = 0 with `solver` -- CG: the pipelined
+ * resident kernel on DIA patterns whose vectors fit on chip, the
+ * single-reduction one otherwise; BiCGSTAB; GMRES(restart) -- to the reduction
+ * still needed (never tighter than inner_tol; at most inner_maxiter
+ * iterations, restart cycles for GMRES), then x += d and r -= A d in FP64; at
+ * most refine_maxiter corrections.  FP32 vectors, FP32 accumulation; the
+ * residual and the decision are FP64.  vals32: the FP32 copy of vals in the
+ * same layout, or NULL (made in the workspace on each call).  dinv: FP64
+ * Jacobi 1/diag, or NULL for no preconditioner.  result (device int32[4]):
+ * status, FP32 iterations (cycles for GMRES) over all corrections,
+ * corrections, 0.  Captured once per argument set as a CUDA graph and
+ * replayed on `stream`; no host sync.                                      */
+int64_t wspm_krylov_mixed_workspace_doubles(int32_t n_rows, int64_t nnz_padded, int32_t solver, int32_t restart);
 int wspm_krylov_solve_mixed(const wspm_pattern *pat, const double *vals, const float *vals32,
-                            const double *b, double *x, const double *dinv, double tol, double inner_tol,
-                            int32_t inner_maxiter, int32_t refine_maxiter, double *work,
-                            int64_t work_doubles, int32_t *result, void *stream);
+                            const double *b, double *x, const double *dinv, int32_t solver, int32_t restart,
+                            double tol, double inner_tol, int32_t inner_maxiter, int32_t refine_maxiter,
+                            double *work, int64_t work_doubles, int32_t *result, void *stream);
 
 /* Measurement hook (no reference counterpart): runs up to `iters` Jacobi-CG
  * iterations of a persistent CG kernel with tolerance 0 from x on the given
@@ -338,7 +342,8 @@ typedef struct wspm_picard_desc {
     double  krylov_tol;        /* relative tolerance                         */
     int32_t krylov_maxiter;    /* iterations (CG, BiCGSTAB) or cycles (GMRES) */
     int32_t restart;           /* GMRES restart length m (1..32)             */
-    int32_t mixed;             /* 1: FP32 Krylov inside FP64 refinement      */
+    int32_t mixed;             /* 1: FP32 Krylov (the same solver) inside FP64
+                                  refinement on the true residual           */
     double  inner_tol;         /* mixed: relative tolerance of each FP32 solve */
     int32_t inner_maxiter;
     int32_t refine_maxiter;

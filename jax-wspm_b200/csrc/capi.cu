@@ -98,23 +98,23 @@ static int build_solve_graph(const wspm_pattern *pat, const double *vals, const 
                                               cs) != WSPM_OK && e == cudaSuccess)
                 e = cudaErrorLaunchFailure;
         } else if (solver == WSPM_SOLVER_BICGSTAB) {
-            BicgBuffers w = carve_bicgstab(work, n, &used);
+            BicgBuffers<double> w = carve_bicgstab<double>(work, n, &used);
             kst = w.st;
             state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)kst, (int)(sizeof(KrylovState) / 4));
-            bicgstab_enqueue_init(A, vals, b, x, x, w, tol, atol, maxiter, h, 1, cs);
+            bicgstab_enqueue_init<double>(A, vals, b, nullptr, x, x, w, tol, atol, nullptr, maxiter, h, 1, cs);
             if (e == cudaSuccess)
                 e = capture_while(cs, h, [&](cudaStream_t bs) {
-                    bicgstab_enqueue_body(A, vals, b, x, dinv, w, maxiter, h, 1, bs);
+                    bicgstab_enqueue_body<double>(A, vals, x, dinv, w, maxiter, h, 1, bs);
                 });
         } else {
             const int m = restart < n ? restart : n;
-            GmresBuffers w = carve_gmres(work, n, m, &used);
+            GmresBuffers<double> w = carve_gmres<double>(work, n, m, &used);
             kst = w.st;
             state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)kst, (int)(sizeof(KrylovState) / 4));
-            gmres_enqueue_init(A, vals, b, x, x, dinv, w, tol, atol, maxiter, h, 1, cs);
+            gmres_enqueue_init<double>(A, vals, b, nullptr, x, x, dinv, w, tol, atol, nullptr, maxiter, h, 1, cs);
             if (e == cudaSuccess)
                 e = capture_while(cs, h, [&](cudaStream_t bs) {
-                    gmres_enqueue_body(A, vals, b, x, dinv, w, maxiter, h, 1, bs);
+                    gmres_enqueue_body<double>(A, vals, b, nullptr, x, dinv, w, maxiter, h, 1, bs);
                 });
         }
         write_result_kernel<<<1, 32, 0, cs>>>(kst, result);

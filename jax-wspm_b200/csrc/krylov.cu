@@ -1430,119 +1430,133 @@ template int pcg_persistent_enqueue<float>(const Sell &, const float *, const fl
                                            const float *, const CgBuffers<float> &, double, double, int, bool,
                                            const double *, cudaStream_t, bool, const int *);
 
-// ---------------------------------------------------------------- BiCGSTAB (FP64)
-template <int MW>
-__global__ void __launch_bounds__(kBlock) bicg_init_kernel(Sell A, const double *__restrict__ vals,
-                                                           const double *__restrict__ b, const double *x0,
-                                                           double *r, double *rhat, double *p, double *q,
-                                                           double *partials, KrylovState *st, double tol,
-                                                           double atol, int maxiter,
+// ---------------------------------------------------------------- BiCGSTAB
+// Templated on the vector/matrix type T: FP64 for the plain path, FP32 for the
+// mixed path's inner corrections (FP32 vectors and FP32 accumulation; the
+// solver scalars are kept in the FP64 KrylovState).  Inner-solve options:
+// b64 (the FP64 residual of the refinement loop, converted on the fly), x0 ==
+// NULL (start from zero), tol_dev (relative tolerance read on the device).
+template <typename T>
+__device__ __forceinline__ T rhs_at(const T *b, const double *b64, int i) {
+    return b64 ? (T)b64[i] : b[i];
+}
+
+template <typename T, int MW>
+__global__ void __launch_bounds__(kBlock) bicg_init_kernel(Sell A, const T *__restrict__ vals,
+                                                           const T *__restrict__ b, const double *__restrict__ b64,
+                                                           const T *x0, T *x, T *r, T *rhat, T *p, T *q, T *partials,
+                                                           KrylovState *st, double tol, double atol,
+                                                           const double *tol_dev, int maxiter,
                                                            cudaGraphConditionalHandle cond, int use_cond) {
-    double v[2] = {0.0, 0.0};
+    T v[2] = {T(0), T(0)};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
-        const double ri = b[i] - sell_row<double, MW>(A, vals, i, [&](int c) { return x0[c]; });
+        const T bi = rhs_at(b, b64, i);
+        T ri = bi;
+        if (x0) ri = bi - sell_row<T, MW>(A, vals, i, [&](int c) { return x0[c]; });
+        else x[i] = T(0);
         r[i] = ri; rhat[i] = ri; p[i] = ri; q[i] = ri;
         v[0] += ri * ri;
-        v[1] += b[i] * b[i];
+        v[1] += bi * bi;
     }
-    if (publish_partials<double, 2>(v, partials, &st->ticket[2])) {
-        double tot[2];
-        final_sum<double, 2>(partials, tot, &st->ticket[2]);
+    if (publish_partials<T, 2>(v, partials, &st->ticket[2])) {
+        T tot[2];
+        final_sum<T, 2>(partials, tot, &st->ticket[2]);
         if (threadIdx.x == 0) {
-            st->rr = tot[0]; st->bs = tot[1];
-            st->atol2 = fmax(tol * tol * tot[1], atol * atol);
+            const double rr = (double)tot[0], bs = (double)tot[1];
+            const double tl = tol_dev ? *tol_dev : tol;
+            st->rr = rr; st->bs = bs;
+            st->atol2 = fmax(tl * tl * bs, atol * atol);
             st->rho = st->alpha = st->omega = 1.0;
-            st->rho_next = tot[0];
+            st->rho_next = rr;
             st->k = 0; st->status = WSPM_OK; st->exit_early = 0;
-            int done = !(tot[0] > st->atol2 && 0 < maxiter);
-            if (!isfinite(tot[0])) { done = 1; st->status = WSPM_NAN; }
+            int done = !(rr > st->atol2 && 0 < maxiter);
+            if (!isfinite(rr)) { done = 1; st->status = WSPM_NAN; }
             st->done = done;
             set_cond(cond, use_cond, done ? 0u : 1u);
         }
     }
 }
 
-__global__ void bicg_p_kernel(int n, const double *__restrict__ r, double *p, const double *__restrict__ q,
-                              double *phat, const double *__restrict__ dinv, const KrylovState *st) {
+template <typename T>
+__global__ void bicg_p_kernel(int n, const T *__restrict__ r, T *p, const T *__restrict__ q, T *phat,
+                              const T *__restrict__ dinv, const KrylovState *st) {
     if (st->done) return;
-    const double beta = st->rho_next / st->rho * st->alpha / st->omega;
-    const double om = st->omega;
+    const T beta = (T)(st->rho_next / st->rho * st->alpha / st->omega);
+    const T om = (T)st->omega;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double pi = r[i] + beta * (p[i] - om * q[i]);
+        const T pi = r[i] + beta * (p[i] - om * q[i]);
         p[i] = pi;
         phat[i] = dinv ? dinv[i] * pi : pi;
     }
 }
 
-template <int MW>
-__global__ void __launch_bounds__(kBlock) bicg_q_kernel(Sell A, const double *__restrict__ vals,
-                                                        const double *__restrict__ phat,
-                                                        const double *__restrict__ rhat, double *q,
-                                                        double *partials, KrylovState *st) {
+template <typename T, int MW>
+__global__ void __launch_bounds__(kBlock) bicg_q_kernel(Sell A, const T *__restrict__ vals, const T *__restrict__ phat,
+                                                        const T *__restrict__ rhat, T *q, T *partials,
+                                                        KrylovState *st) {
     if (st->done) return;
-    double v[1] = {0.0};
+    T v[1] = {T(0)};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
-        const double qi = sell_row<double, MW>(A, vals, i, [&](int c) { return __ldg(phat + c); });
+        const T qi = sell_row<T, MW>(A, vals, i, [&](int c) { return __ldg(phat + c); });
         q[i] = qi;
         v[0] += rhat[i] * qi;
     }
-    if (publish_partials<double, 1>(v, partials, &st->ticket[0])) {
-        double tot[1];
-        final_sum<double, 1>(partials, tot, &st->ticket[0]);
+    if (publish_partials<T, 1>(v, partials, &st->ticket[0])) {
+        T tot[1];
+        final_sum<T, 1>(partials, tot, &st->ticket[0]);
         if (threadIdx.x == 0) {
-            st->sigma = tot[0];
-            st->rho = st->rho_next;               // rho of this iteration
-            st->alpha = st->rho_next / tot[0];    // alpha of this iteration
+            st->sigma = (double)tot[0];
+            st->rho = st->rho_next;                       // rho of this iteration
+            st->alpha = st->rho_next / (double)tot[0];    // alpha of this iteration
         }
     }
 }
 
-template <int MW>
-__global__ void __launch_bounds__(kBlock) bicg_t_kernel(Sell A, const double *__restrict__ vals,
-                                                        const double *__restrict__ r, const double *__restrict__ q,
-                                                        const double *__restrict__ dinv, double *t,
-                                                        double *partials, KrylovState *st) {
+template <typename T, int MW>
+__global__ void __launch_bounds__(kBlock) bicg_t_kernel(Sell A, const T *__restrict__ vals, const T *__restrict__ r,
+                                                        const T *__restrict__ q, const T *__restrict__ dinv, T *t,
+                                                        T *partials, KrylovState *st) {
     if (st->done) return;
-    const double alpha = st->alpha;
-    double v[3] = {0.0, 0.0, 0.0};
+    const T alpha = (T)st->alpha;
+    T v[3] = {T(0), T(0), T(0)};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
-        const double ti = sell_row<double, MW>(A, vals, i, [&](int c) {
-            const double sc = __ldg(r + c) - alpha * __ldg(q + c);
+        const T ti = sell_row<T, MW>(A, vals, i, [&](int c) {
+            const T sc = __ldg(r + c) - alpha * __ldg(q + c);
             return dinv ? __ldg(dinv + c) * sc : sc;
         });
-        const double si = r[i] - alpha * q[i];
+        const T si = r[i] - alpha * q[i];
         t[i] = ti;
         v[0] += si * si;
         v[1] += ti * si;
         v[2] += ti * ti;
     }
-    if (publish_partials<double, 3>(v, partials, &st->ticket[1])) {
-        double tot[3];
-        final_sum<double, 3>(partials, tot, &st->ticket[1]);
+    if (publish_partials<T, 3>(v, partials, &st->ticket[1])) {
+        T tot[3];
+        final_sum<T, 3>(partials, tot, &st->ticket[1]);
         if (threadIdx.x == 0) {
-            st->ss = tot[0]; st->ts = tot[1]; st->tt = tot[2];
-            st->omega = tot[1] / tot[2];
-            st->exit_early = tot[0] < st->atol2;
+            st->ss = (double)tot[0]; st->ts = (double)tot[1]; st->tt = (double)tot[2];
+            st->omega = st->ts / st->tt;
+            st->exit_early = st->ss < st->atol2;
         }
     }
 }
 
-__global__ void __launch_bounds__(kBlock) bicg_x_kernel(int n, double *x, double *r, const double *__restrict__ rhat,
-                                                        const double *__restrict__ p, const double *__restrict__ q,
-                                                        const double *__restrict__ t,
-                                                        const double *__restrict__ dinv, double *partials,
-                                                        KrylovState *st, int maxiter,
+template <typename T>
+__global__ void __launch_bounds__(kBlock) bicg_x_kernel(int n, T *x, T *r, const T *__restrict__ rhat,
+                                                        const T *__restrict__ p, const T *__restrict__ q,
+                                                        const T *__restrict__ t, const T *__restrict__ dinv,
+                                                        T *partials, KrylovState *st, int maxiter,
                                                         cudaGraphConditionalHandle cond, int use_cond) {
     if (st->done) return;
-    const double alpha = st->alpha, omega = st->omega;
+    const T alpha = (T)st->alpha, omega = (T)st->omega;
     const int early = st->exit_early;
-    double v[2] = {0.0, 0.0};
+    T v[2] = {T(0), T(0)};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double si = r[i] - alpha * q[i];
-        const double di = dinv ? dinv[i] : 1.0;
-        const double phat = dinv ? di * p[i] : p[i];
-        const double shat = dinv ? di * si : si;
-        double ri;
+        const T si = r[i] - alpha * q[i];
+        const T di = dinv ? dinv[i] : T(1);
+        const T phat = dinv ? di * p[i] : p[i];
+        const T shat = dinv ? di * si : si;
+        T ri;
         if (early) {
             x[i] = x[i] + alpha * phat;
             ri = si;
@@ -1554,84 +1568,113 @@ __global__ void __launch_bounds__(kBlock) bicg_x_kernel(int n, double *x, double
         v[0] += ri * ri;
         v[1] += rhat[i] * ri;
     }
-    if (publish_partials<double, 2>(v, partials, &st->ticket[2])) {
-        double tot[2];
-        final_sum<double, 2>(partials, tot, &st->ticket[2]);
+    if (publish_partials<T, 2>(v, partials, &st->ticket[2])) {
+        T tot[2];
+        final_sum<T, 2>(partials, tot, &st->ticket[2]);
         if (threadIdx.x == 0) {
-            st->rr = tot[0];
-            st->rho_next = tot[1];
+            const double rr = (double)tot[0];
+            st->rr = rr;
+            st->rho_next = (double)tot[1];
             int k = (st->omega == 0.0 || st->alpha == 0.0) ? -11 : st->k + 1;
             if (st->rho == 0.0) k = -10;
             st->k = k;
-            int done = !(tot[0] > st->atol2 && k < maxiter && k >= 0);
+            int done = !(rr > st->atol2 && k < maxiter && k >= 0);
             if (k < 0) st->status = WSPM_BREAKDOWN;
-            else if (done && tot[0] > st->atol2) st->status = WSPM_MAXITER;
-            if (!isfinite(tot[0])) { done = 1; st->status = WSPM_NAN; }
+            else if (done && rr > st->atol2) st->status = WSPM_MAXITER;
+            if (!isfinite(rr)) { done = 1; st->status = WSPM_NAN; }
             st->done = done;
             set_cond(cond, use_cond, done ? 0u : 1u);
         }
     }
 }
 
-void bicgstab_enqueue_init(const Sell &A, const double *vals, const double *b, const double *x0, double *x,
-                           const BicgBuffers &w, double tol, double atol, int maxiter,
+template <typename T>
+void bicgstab_enqueue_init(const Sell &A, const T *vals, const T *b, const double *b64, const T *x0, T *x,
+                           const BicgBuffers<T> &w, double tol, double atol, const double *tol_dev, int maxiter,
                            cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
     const int nb = reduction_blocks(A.n_rows);
-    if (x != x0) copy_kernel<double><<<nb, kBlock, 0, st>>>(x0, x, A.n_rows);
+    if (x0 && x != x0) copy_kernel<T><<<nb, kBlock, 0, st>>>(x0, x, A.n_rows);
     WSPM_WIDTH_DISPATCH(A.max_width,
-                        bicg_init_kernel<MW><<<nb, kBlock, 0, st>>>(A, vals, b, x0, w.r, w.rhat, w.p, w.q, w.partials,
-                                                                    w.st, tol, atol, maxiter, cond, use_cond));
+                        bicg_init_kernel<T, MW><<<nb, kBlock, 0, st>>>(A, vals, b, b64, x0, x, w.r, w.rhat, w.p, w.q,
+                                                                       w.partials, w.st, tol, atol, tol_dev, maxiter,
+                                                                       cond, use_cond));
 }
 
-void bicgstab_enqueue_body(const Sell &A, const double *vals, const double *b, double *x, const double *dinv,
-                           const BicgBuffers &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
-                           cudaStream_t st) {
-    (void)b;
+template <typename T>
+void bicgstab_enqueue_body(const Sell &A, const T *vals, T *x, const T *dinv, const BicgBuffers<T> &w, int maxiter,
+                           cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
     const int nb = reduction_blocks(A.n_rows);
-    bicg_p_kernel<<<nb, kBlock, 0, st>>>(A.n_rows, w.r, w.p, w.q, w.phat, dinv, w.st);
+    bicg_p_kernel<T><<<nb, kBlock, 0, st>>>(A.n_rows, w.r, w.p, w.q, w.phat, dinv, w.st);
     WSPM_WIDTH_DISPATCH(A.max_width,
-                        bicg_q_kernel<MW><<<nb, kBlock, 0, st>>>(A, vals, w.phat, w.rhat, w.q, w.partials, w.st));
+                        bicg_q_kernel<T, MW><<<nb, kBlock, 0, st>>>(A, vals, w.phat, w.rhat, w.q, w.partials, w.st));
     WSPM_WIDTH_DISPATCH(A.max_width,
-                        bicg_t_kernel<MW><<<nb, kBlock, 0, st>>>(A, vals, w.r, w.q, dinv, w.t, w.partials, w.st));
-    bicg_x_kernel<<<nb, kBlock, 0, st>>>(A.n_rows, x, w.r, w.rhat, w.p, w.q, w.t, dinv, w.partials, w.st, maxiter,
-                                         cond, use_cond);
+                        bicg_t_kernel<T, MW><<<nb, kBlock, 0, st>>>(A, vals, w.r, w.q, dinv, w.t, w.partials, w.st));
+    bicg_x_kernel<T><<<nb, kBlock, 0, st>>>(A.n_rows, x, w.r, w.rhat, w.p, w.q, w.t, dinv, w.partials, w.st, maxiter,
+                                            cond, use_cond);
 }
 
-// ---------------------------------------------------------------- GMRES(m) (FP64)
+template void bicgstab_enqueue_init<double>(const Sell &, const double *, const double *, const double *,
+                                            const double *, double *, const BicgBuffers<double> &, double, double,
+                                            const double *, int, cudaGraphConditionalHandle, int, cudaStream_t);
+template void bicgstab_enqueue_init<float>(const Sell &, const float *, const float *, const double *, const float *,
+                                           float *, const BicgBuffers<float> &, double, double, const double *, int,
+                                           cudaGraphConditionalHandle, int, cudaStream_t);
+template void bicgstab_enqueue_body<double>(const Sell &, const double *, double *, const double *,
+                                            const BicgBuffers<double> &, int, cudaGraphConditionalHandle, int,
+                                            cudaStream_t);
+template void bicgstab_enqueue_body<float>(const Sell &, const float *, float *, const float *,
+                                           const BicgBuffers<float> &, int, cudaGraphConditionalHandle, int,
+                                           cudaStream_t);
+
+// ---------------------------------------------------------------- GMRES(m)
 constexpr int kMaxRestart = 32;
 constexpr int kMaxDots = kMaxRestart + 2;
 
+// Templated like BiCGSTAB: basis V, w and the reductions in T; the small
+// Hessenberg matrix, the least-squares solve and the scalars in FP64.
+template <typename T>
+__device__ __forceinline__ double type_eps() { return sizeof(T) == 4 ? (double)FLT_EPSILON : DBL_EPSILON; }
+
 // r = M (b - A x) into dst; ||r||^2 (and, at init, ||b||^2, ||M b||^2).
-template <int MW>
-__global__ void __launch_bounds__(kBlock) gm_residual_kernel(Sell A, const double *__restrict__ vals,
-                                                             const double *__restrict__ b, const double *x,
-                                                             const double *__restrict__ dinv, double *dst,
-                                                             double *partials, KrylovState *st, int is_init,
-                                                             double tol, double atol, int maxiter,
+// x == NULL at init: x starts from zero (xz is then cleared).
+template <typename T, int MW>
+__global__ void __launch_bounds__(kBlock) gm_residual_kernel(Sell A, const T *__restrict__ vals,
+                                                             const T *__restrict__ b, const double *__restrict__ b64,
+                                                             const T *x, T *xz, const T *__restrict__ dinv, T *dst,
+                                                             T *partials, KrylovState *st, int is_init, double tol,
+                                                             double atol, const double *tol_dev, int maxiter,
                                                              cudaGraphConditionalHandle cond, int use_cond) {
     if (!is_init && st->done) return;
-    double v[3] = {0.0, 0.0, 0.0};
+    T v[3] = {T(0), T(0), T(0)};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_rows; i += gridDim.x * blockDim.x) {
-        const double d = dinv ? dinv[i] : 1.0;
-        const double ri = d * (b[i] - sell_row<double, MW>(A, vals, i, [&](int c) { return x[c]; }));
+        const T d = dinv ? dinv[i] : T(1);
+        const T bi = rhs_at(b, b64, i);
+        T ri;
+        if (x) {
+            ri = d * (bi - sell_row<T, MW>(A, vals, i, [&](int c) { return x[c]; }));
+        } else {
+            ri = d * bi;
+            xz[i] = T(0);
+        }
         dst[i] = ri;
         v[0] += ri * ri;
-        v[1] += b[i] * b[i];
-        v[2] += (d * b[i]) * (d * b[i]);
+        v[1] += bi * bi;
+        v[2] += (d * bi) * (d * bi);
     }
-    if (publish_partials<double, 3>(v, partials, &st->ticket[2])) {
-        double tot[3];
-        final_sum<double, 3>(partials, tot, &st->ticket[2]);
+    if (publish_partials<T, 3>(v, partials, &st->ticket[2])) {
+        T tot[3];
+        final_sum<T, 3>(partials, tot, &st->ticket[2]);
         if (threadIdx.x == 0) {
-            double rn = sqrt(tot[0]);
-            if (!(rn > DBL_EPSILON)) rn = 0.0;
+            double rn = sqrt((double)tot[0]);
+            if (!(rn > type_eps<T>())) rn = 0.0;
             st->rnorm = rn;
             st->inv_wn = rn > 0.0 ? 1.0 / rn : 0.0;
             if (is_init) {
-                const double bn = sqrt(tot[1]);
+                const double bn = sqrt((double)tot[1]);
+                const double tl = tol_dev ? *tol_dev : tol;
                 st->b_norm = bn;
-                st->mb_norm = sqrt(tot[2]);
-                const double at = fmax(tol * bn, atol);
+                st->mb_norm = sqrt((double)tot[2]);
+                const double at = fmax(tl * bn, atol);
                 // jnp.minimum propagates NaN: with b == 0 the tolerance is NaN and the loop does not run
                 st->ptol = bn > 0.0 ? st->mb_norm * fmin(1.0, at / bn) : __longlong_as_double(0x7ff8000000000000ULL);
                 st->k = 0;
@@ -1643,44 +1686,45 @@ __global__ void __launch_bounds__(kBlock) gm_residual_kernel(Sell A, const doubl
             st->steps = 0;
             int done = !(st->k < maxiter && rn > st->ptol);
             if (done && st->k >= maxiter && rn > st->ptol) st->status = WSPM_MAXITER;
-            if (!isfinite(tot[0])) { done = 1; st->status = WSPM_NAN; }
+            if (!isfinite((double)tot[0])) { done = 1; st->status = WSPM_NAN; }
             st->done = done;
             set_cond(cond, use_cond, done ? 0u : 1u);
         }
     }
 }
 
-__global__ void gm_scale_kernel(int n, double *v, const KrylovState *st) {
+template <typename T>
+__global__ void gm_scale_kernel(int n, T *v, const KrylovState *st) {
     if (st->done || st->broken) return;
-    const double s = st->inv_wn;
+    const T s = (T)st->inv_wn;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] *= s;
 }
 
 // phase 0: w = M A V_j, dots V_k.w (k <= j) and ||w||^2
 // phase 1: w -= V h1 ; dots V_k.w
 // phase 2: w -= V h2 ; ||w||^2, then H column j and breakdown test
-template <int MW>
-__global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(Sell A, const double *__restrict__ vals,
-                                                            const double *__restrict__ dinv, const double *V,
-                                                            double *w, double *H, double *hbuf, double *partials,
-                                                            KrylovState *st, int j, int m, int phase, int64_t ld) {
+template <typename T, int MW>
+__global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(Sell A, const T *__restrict__ vals,
+                                                            const T *__restrict__ dinv, const T *V, T *w, double *H,
+                                                            double *hbuf, T *partials, KrylovState *st, int j, int m,
+                                                            int phase, int64_t ld) {
     if (st->done || st->broken) return;
     const int n = A.n_rows;
     const int nd = j + 1;
-    double v[kMaxDots];
+    T v[kMaxDots];
 #pragma unroll
-    for (int k = 0; k < kMaxDots; ++k) v[k] = 0.0;
-    double h[kMaxRestart + 1];
+    for (int k = 0; k < kMaxDots; ++k) v[k] = T(0);
+    T h[kMaxRestart + 1];
     if (phase > 0) {
         const double *src = hbuf + (phase - 1) * (kMaxRestart + 1);
 #pragma unroll
-        for (int k = 0; k <= kMaxRestart; ++k) h[k] = k < nd ? src[k] : 0.0;
+        for (int k = 0; k <= kMaxRestart; ++k) h[k] = k < nd ? (T)src[k] : T(0);
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double wi;
+        T wi;
         if (phase == 0) {
-            const double *vj = V + (int64_t)j * ld;
-            wi = sell_row<double, MW>(A, vals, i, [&](int c) { return __ldg(vj + c); });
+            const T *vj = V + (int64_t)j * ld;
+            wi = sell_row<T, MW>(A, vals, i, [&](int c) { return __ldg(vj + c); });
             if (dinv) wi *= dinv[i];
         } else {
             wi = w[i];
@@ -1696,20 +1740,20 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(Sell A, const double
         }
         v[kMaxDots - 1] += wi * wi;
     }
-    if (publish_partials<double, kMaxDots>(v, partials, &st->ticket[phase == 2 ? 1 : 0])) {
-        double tot[kMaxDots];
-        final_sum<double, kMaxDots>(partials, tot, &st->ticket[phase == 2 ? 1 : 0]);
+    if (publish_partials<T, kMaxDots>(v, partials, &st->ticket[phase == 2 ? 1 : 0])) {
+        T tot[kMaxDots];
+        final_sum<T, kMaxDots>(partials, tot, &st->ticket[phase == 2 ? 1 : 0]);
         if (threadIdx.x == 0) {
             if (phase == 0) {
-                st->wn0 = sqrt(tot[kMaxDots - 1]);
-                for (int k = 0; k < nd; ++k) hbuf[k] = tot[k];
+                st->wn0 = sqrt((double)tot[kMaxDots - 1]);
+                for (int k = 0; k < nd; ++k) hbuf[k] = (double)tot[k];
             } else if (phase == 1) {
-                for (int k = 0; k < nd; ++k) hbuf[(kMaxRestart + 1) + k] = tot[k];
+                for (int k = 0; k < nd; ++k) hbuf[(kMaxRestart + 1) + k] = (double)tot[k];
             } else {
                 double *col = H + (int64_t)j * (m + 1);
                 for (int k = 0; k < nd; ++k) col[k] = hbuf[k] + hbuf[(kMaxRestart + 1) + k];
-                double wn = sqrt(tot[kMaxDots - 1]);
-                const double thresh = DBL_EPSILON * st->wn0;
+                double wn = sqrt((double)tot[kMaxDots - 1]);
+                const double thresh = type_eps<T>() * st->wn0;
                 if (!(wn > thresh)) wn = 0.0;
                 col[j + 1] = wn;
                 st->wn = wn;
@@ -1722,11 +1766,11 @@ __global__ void __launch_bounds__(kBlock) gm_arnoldi_kernel(Sell A, const double
 }
 
 // V_{j+1} = w / ||w|| (zero after a breakdown); runs even on the breakdown step.
-__global__ void gm_next_kernel(int n, double *V, const double *__restrict__ w, const KrylovState *st, int j,
-                               int64_t ld) {
+template <typename T>
+__global__ void gm_next_kernel(int n, T *V, const T *__restrict__ w, const KrylovState *st, int j, int64_t ld) {
     if (st->done || st->steps != j + 1) return;
-    const double s = st->inv_wn;
-    double *dst = V + (int64_t)(j + 1) * ld;
+    const T s = (T)st->inv_wn;
+    T *dst = V + (int64_t)(j + 1) * ld;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = w[i] * s;
 }
 
@@ -1761,15 +1805,16 @@ __global__ void gm_lsq_kernel(const double *H, double *y, KrylovState *st, int m
     }
 }
 
-__global__ void gm_update_kernel(int n, double *x, const double *V, const double *__restrict__ y,
-                                 const KrylovState *st, int64_t ld) {
+template <typename T>
+__global__ void gm_update_kernel(int n, T *x, const T *V, const double *__restrict__ y, const KrylovState *st,
+                                 int64_t ld) {
     if (st->done) return;
     const int ns = st->steps;
-    double yl[kMaxRestart];
+    T yl[kMaxRestart];
 #pragma unroll
-    for (int k = 0; k < kMaxRestart; ++k) yl[k] = k < ns ? y[k] : 0.0;
+    for (int k = 0; k < kMaxRestart; ++k) yl[k] = k < ns ? (T)y[k] : T(0);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double acc = 0.0;
+        T acc = T(0);
 #pragma unroll
         for (int k = 0; k < kMaxRestart; ++k)
             if (k < ns) acc += yl[k] * V[(int64_t)k * ld + i];
@@ -1777,35 +1822,53 @@ __global__ void gm_update_kernel(int n, double *x, const double *V, const double
     }
 }
 
-void gmres_enqueue_init(const Sell &A, const double *vals, const double *b, const double *x0, double *x,
-                        const double *dinv, const GmresBuffers &w, double tol, double atol, int maxiter,
-                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
+template <typename T>
+void gmres_enqueue_init(const Sell &A, const T *vals, const T *b, const double *b64, const T *x0, T *x,
+                        const T *dinv, const GmresBuffers<T> &w, double tol, double atol, const double *tol_dev,
+                        int maxiter, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
     const int nb = reduction_blocks(A.n_rows);
-    if (x != x0) copy_kernel<double><<<nb, kBlock, 0, st>>>(x0, x, A.n_rows);
+    if (x0 && x != x0) copy_kernel<T><<<nb, kBlock, 0, st>>>(x0, x, A.n_rows);
     WSPM_WIDTH_DISPATCH(A.max_width,
-                        gm_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, vals, b, x0, dinv, w.V, w.partials, w.st, 1,
-                                                                      tol, atol, maxiter, cond, use_cond));
-    gm_scale_kernel<<<nb, kBlock, 0, st>>>(A.n_rows, w.V, w.st);
+                        gm_residual_kernel<T, MW><<<nb, kBlock, 0, st>>>(A, vals, b, b64, x0, x, dinv, w.V,
+                                                                         w.partials, w.st, 1, tol, atol, tol_dev,
+                                                                         maxiter, cond, use_cond));
+    gm_scale_kernel<T><<<nb, kBlock, 0, st>>>(A.n_rows, w.V, w.st);
 }
 
-void gmres_enqueue_body(const Sell &A, const double *vals, const double *b, double *x, const double *dinv,
-                        const GmresBuffers &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
+template <typename T>
+void gmres_enqueue_body(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
+                        const GmresBuffers<T> &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
                         cudaStream_t st) {
     const int nb = reduction_blocks(A.n_rows);
     for (int j = 0; j < w.m; ++j) {
         for (int ph = 0; ph < 3; ++ph)
             WSPM_WIDTH_DISPATCH(A.max_width,
-                                gm_arnoldi_kernel<MW><<<nb, kBlock, 0, st>>>(A, vals, dinv, w.V, w.w, w.H, w.hbuf,
-                                                                             w.partials, w.st, j, w.m, ph, w.ld));
-        gm_next_kernel<<<nb, kBlock, 0, st>>>(A.n_rows, w.V, w.w, w.st, j, w.ld);
+                                gm_arnoldi_kernel<T, MW><<<nb, kBlock, 0, st>>>(A, vals, dinv, w.V, w.w, w.H, w.hbuf,
+                                                                                w.partials, w.st, j, w.m, ph, w.ld));
+        gm_next_kernel<T><<<nb, kBlock, 0, st>>>(A.n_rows, w.V, w.w, w.st, j, w.ld);
     }
     gm_lsq_kernel<<<1, 32, 0, st>>>(w.H, w.y, w.st, w.m);
-    gm_update_kernel<<<nb, kBlock, 0, st>>>(A.n_rows, x, w.V, w.y, w.st, w.ld);
+    gm_update_kernel<T><<<nb, kBlock, 0, st>>>(A.n_rows, x, w.V, w.y, w.st, w.ld);
     WSPM_WIDTH_DISPATCH(A.max_width,
-                        gm_residual_kernel<MW><<<nb, kBlock, 0, st>>>(A, vals, b, x, dinv, w.V, w.partials, w.st, 0,
-                                                                      0.0, 0.0, maxiter, cond, use_cond));
-    gm_scale_kernel<<<nb, kBlock, 0, st>>>(A.n_rows, w.V, w.st);
+                        gm_residual_kernel<T, MW><<<nb, kBlock, 0, st>>>(A, vals, b, b64, x, x, dinv, w.V,
+                                                                         w.partials, w.st, 0, 0.0, 0.0, nullptr,
+                                                                         maxiter, cond, use_cond));
+    gm_scale_kernel<T><<<nb, kBlock, 0, st>>>(A.n_rows, w.V, w.st);
 }
+
+template void gmres_enqueue_init<double>(const Sell &, const double *, const double *, const double *,
+                                         const double *, double *, const double *, const GmresBuffers<double> &,
+                                         double, double, const double *, int, cudaGraphConditionalHandle, int,
+                                         cudaStream_t);
+template void gmres_enqueue_init<float>(const Sell &, const float *, const float *, const double *, const float *,
+                                        float *, const float *, const GmresBuffers<float> &, double, double,
+                                        const double *, int, cudaGraphConditionalHandle, int, cudaStream_t);
+template void gmres_enqueue_body<double>(const Sell &, const double *, const double *, const double *, double *,
+                                         const double *, const GmresBuffers<double> &, int,
+                                         cudaGraphConditionalHandle, int, cudaStream_t);
+template void gmres_enqueue_body<float>(const Sell &, const float *, const float *, const double *, float *,
+                                        const float *, const GmresBuffers<float> &, int, cudaGraphConditionalHandle,
+                                        int, cudaStream_t);
 
 // ---------------------------------------------------------------- workspaces
 static inline int64_t align32(int64_t n) { return (n + 31) & ~int64_t(31); }
@@ -1814,11 +1877,13 @@ int64_t cg_workspace_doubles(int n, int bytes) {
     const int64_t vec = align32(((int64_t)n * bytes + 7) / 8);
     return 5 * vec + align32(4 * kMaxPartials) + align32(sizeof(KrylovState) / 8 + 1);
 }
-int64_t bicgstab_workspace_doubles(int n) {
-    return 6 * align32(n) + align32(4 * kMaxPartials) + align32(sizeof(KrylovState) / 8 + 1);
+int64_t bicgstab_workspace_doubles(int n, int bytes) {
+    const int64_t vec = align32(((int64_t)n * bytes + 7) / 8);
+    return 6 * vec + align32(4 * kMaxPartials) + align32(sizeof(KrylovState) / 8 + 1);
 }
-int64_t gmres_workspace_doubles(int n, int m) {
-    return (m + 2) * align32(n) + align32((int64_t)(m + 1) * m) + align32(m) + align32(2 * (kMaxRestart + 1)) +
+int64_t gmres_workspace_doubles(int n, int m, int bytes) {
+    const int64_t vec = align32(((int64_t)n * bytes + 7) / 8);
+    return (m + 2) * vec + align32((int64_t)(m + 1) * m) + align32(m) + align32(2 * (kMaxRestart + 1)) +
            align32((int64_t)kMaxDots * kMaxPartials) + align32(sizeof(KrylovState) / 8 + 1);
 }
 
@@ -1840,33 +1905,39 @@ CgBuffers<T> carve_cg(double *work, int n, int64_t *used) {
 template CgBuffers<double> carve_cg<double>(double *, int, int64_t *);
 template CgBuffers<float> carve_cg<float>(double *, int, int64_t *);
 
-BicgBuffers carve_bicgstab(double *work, int n, int64_t *used) {
-    const int64_t vec = align32(n);
-    BicgBuffers b;
+template <typename T>
+BicgBuffers<T> carve_bicgstab(double *work, int n, int64_t *used) {
+    const int64_t vec = align32(((int64_t)n * sizeof(T) + 7) / 8);
+    BicgBuffers<T> b;
     double *p = work;
-    b.r = p; p += vec; b.rhat = p; p += vec; b.p = p; p += vec;
-    b.phat = p; p += vec; b.q = p; p += vec; b.t = p; p += vec;
-    b.partials = p; p += align32(4 * kMaxPartials);
+    b.r = (T *)p; p += vec; b.rhat = (T *)p; p += vec; b.p = (T *)p; p += vec;
+    b.phat = (T *)p; p += vec; b.q = (T *)p; p += vec; b.t = (T *)p; p += vec;
+    b.partials = (T *)p; p += align32(4 * kMaxPartials);
     b.st = (KrylovState *)p; p += align32(sizeof(KrylovState) / 8 + 1);
     *used = p - work;
     return b;
 }
+template BicgBuffers<double> carve_bicgstab<double>(double *, int, int64_t *);
+template BicgBuffers<float> carve_bicgstab<float>(double *, int, int64_t *);
 
-GmresBuffers carve_gmres(double *work, int n, int m, int64_t *used) {
-    const int64_t vec = align32(n);
-    GmresBuffers b;
+template <typename T>
+GmresBuffers<T> carve_gmres(double *work, int n, int m, int64_t *used) {
+    const int64_t vec = align32(((int64_t)n * sizeof(T) + 7) / 8);   // in doubles
+    GmresBuffers<T> b;
     double *p = work;
     b.m = m;
-    b.ld = vec;
-    b.V = p; p += (int64_t)(m + 1) * vec;
-    b.w = p; p += vec;
+    b.ld = vec * (int64_t)(8 / sizeof(T));                          // in elements of T
+    b.V = (T *)p; p += (int64_t)(m + 1) * vec;
+    b.w = (T *)p; p += vec;
     b.H = p; p += align32((int64_t)(m + 1) * m);
     b.y = p; p += align32(m);
     b.hbuf = p; p += align32(2 * (kMaxRestart + 1));
-    b.partials = p; p += align32((int64_t)kMaxDots * kMaxPartials);
+    b.partials = (T *)p; p += align32((int64_t)kMaxDots * kMaxPartials);
     b.st = (KrylovState *)p; p += align32(sizeof(KrylovState) / 8 + 1);
     *used = p - work;
     return b;
 }
+template GmresBuffers<double> carve_gmres<double>(double *, int, int, int64_t *);
+template GmresBuffers<float> carve_gmres<float>(double *, int, int, int64_t *);
 
 }  // namespace wspm

@@ -35,9 +35,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Reduction tail of the refinement steps (the start, fused into the assembly or
 // as ir_residual_kernel, and ir_update_kernel): tot = (r.r, b.b); sets
 // the next inner tolerance, the continue flag and the graph condition.
+// inner_launches: kernels the inner solve just finished launched (launch accounting).
 __device__ __forceinline__ void ir_decide(const double (&tot)[2], KrylovState *irs, const KrylovState *inner,
                                           int is_init, double tol, double inner_floor, int maxit,
-                                          cudaGraphConditionalHandle cond, int use_cond) {
+                                          cudaGraphConditionalHandle cond, int use_cond, int inner_launches = 1) {
     if (is_init) {
         irs->bs = tot[1];
         irs->atol2 = tol * tol * tot[1];
@@ -48,8 +49,8 @@ __device__ __forceinline__ void ir_decide(const double (&tot)[2], KrylovState *i
         irs->status = WSPM_OK;
     } else {
         irs->k += 1;
-        irs->steps += inner->k;
-        irs->pad0 += 1;
+        irs->steps += inner->k > 0 ? inner->k : 0;      // a BiCGSTAB breakdown reports k < 0
+        irs->pad0 += inner_launches;
         irs->ns += inner->ns;
     }
     irs->rr = tot[0];
@@ -142,44 +143,55 @@ int pcg_persistent_enqueue(const Sell &A, const T *vals, const T *b, const doubl
 template <typename T>
 bool pcg_eligible(const Sell &A);
 
+// BiCGSTAB and GMRES(m) buffers, templated on the vector type (double for the
+// plain path, float for the mixed path's inner corrections).
+template <typename T>
 struct BicgBuffers {
-    double *r, *rhat, *p, *phat, *q, *t;
-    double *partials;
+    T *r, *rhat, *p, *phat, *q, *t;
+    T *partials;
     KrylovState *st;
 };
-void bicgstab_enqueue_init(const Sell &A, const double *vals, const double *b, const double *x0, double *x,
-                           const BicgBuffers &w, double tol, double atol, int maxiter,
+// b64: optional FP64 right-hand side read in place of b (converted on the fly);
+// x0 == NULL: start from zero; tol_dev: optional device-side relative tolerance.
+template <typename T>
+void bicgstab_enqueue_init(const Sell &A, const T *vals, const T *b, const double *b64, const T *x0, T *x,
+                           const BicgBuffers<T> &w, double tol, double atol, const double *tol_dev, int maxiter,
                            cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
-void bicgstab_enqueue_body(const Sell &A, const double *vals, const double *b, double *x, const double *dinv,
-                           const BicgBuffers &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
-                           cudaStream_t st);
+template <typename T>
+void bicgstab_enqueue_body(const Sell &A, const T *vals, T *x, const T *dinv, const BicgBuffers<T> &w, int maxiter,
+                           cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
 
+template <typename T>
 struct GmresBuffers {
-    double *V;        // [(m+1) * n]
-    double *w;        // [n]
+    T *V;             // [(m+1) * ld]
+    T *w;             // [n]
     double *H;        // [(m+1) * m], column-major by Arnoldi step: H[j*(m+1) + i]
     double *y;        // [m]
     double *hbuf;     // [2 * (m+1)]
-    double *partials; // [(m+2) * kMaxPartials]
+    T *partials;      // [(m+2) * kMaxPartials]
     KrylovState *st;
     int m;
-    int64_t ld;       // leading dimension of V (padded n)
+    int64_t ld;       // leading dimension of V in elements (padded n)
 };
-void gmres_enqueue_init(const Sell &A, const double *vals, const double *b, const double *x0, double *x,
-                        const double *dinv, const GmresBuffers &w, double tol, double atol, int maxiter,
-                        cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
-void gmres_enqueue_body(const Sell &A, const double *vals, const double *b, double *x, const double *dinv,
-                        const GmresBuffers &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
+template <typename T>
+void gmres_enqueue_init(const Sell &A, const T *vals, const T *b, const double *b64, const T *x0, T *x,
+                        const T *dinv, const GmresBuffers<T> &w, double tol, double atol, const double *tol_dev,
+                        int maxiter, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st);
+template <typename T>
+void gmres_enqueue_body(const Sell &A, const T *vals, const T *b, const double *b64, T *x, const T *dinv,
+                        const GmresBuffers<T> &w, int maxiter, cudaGraphConditionalHandle cond, int use_cond,
                         cudaStream_t st);
 
 // Workspace sizing / carving (in doubles).
 int64_t cg_workspace_doubles(int n, int bytes_per_elem);
-int64_t bicgstab_workspace_doubles(int n);
-int64_t gmres_workspace_doubles(int n, int m);
+int64_t bicgstab_workspace_doubles(int n, int bytes_per_elem = 8);
+int64_t gmres_workspace_doubles(int n, int m, int bytes_per_elem = 8);
 template <typename T>
 CgBuffers<T> carve_cg(double *work, int n, int64_t *used);
-BicgBuffers carve_bicgstab(double *work, int n, int64_t *used);
-GmresBuffers carve_gmres(double *work, int n, int m, int64_t *used);
+template <typename T>
+BicgBuffers<T> carve_bicgstab(double *work, int n, int64_t *used);
+template <typename T>
+GmresBuffers<T> carve_gmres(double *work, int n, int m, int64_t *used);
 
 void copy_kernel_d(const double *src, double *dst, int n, cudaStream_t st);
 void spmv_f64(const Sell &A, const double *vals, const double *x, double *y, cudaStream_t st);

@@ -154,9 +154,45 @@ __global__ void step_finish_kernel(int n, const double *__restrict__ h_m, double
     }
 }
 
-// ---- mixed precision: FP32 CG corrections inside FP64 refinement ----------
+// ---- mixed precision: FP32 Krylov corrections inside FP64 refinement --------
 // ir state (KrylovState): bs, atol2, rr, k (refinement iterations), steps (inner
-// iterations summed), status.
+// iterations summed), pad0 (inner-solve kernel launches), status.
+
+// The FP32 inner solver: Jacobi-CG (pipelined or single-reduction resident
+// kernel), BiCGSTAB or GMRES(m), the same method as the FP64 path's solver.
+struct InnerSolver {
+    int solver = WSPM_SOLVER_CG;
+    CgBuffers<float> cg;
+    BicgBuffers<float> bicg;
+    GmresBuffers<float> gm;
+    KrylovState *st() const {
+        return solver == WSPM_SOLVER_BICGSTAB ? bicg.st : solver == WSPM_SOLVER_GMRES ? gm.st : cg.st;
+    }
+};
+
+static int64_t inner_workspace_doubles(int n, int solver, int restart) {
+    if (solver == WSPM_SOLVER_BICGSTAB) return bicgstab_workspace_doubles(n, 4);
+    if (solver == WSPM_SOLVER_GMRES) return gmres_workspace_doubles(n, restart, 4);
+    return cg_workspace_doubles(n, 4);
+}
+
+static InnerSolver carve_inner(double *p, int n, int solver, int restart, int64_t *used) {
+    InnerSolver in;
+    in.solver = solver;
+    if (solver == WSPM_SOLVER_BICGSTAB) in.bicg = carve_bicgstab<float>(p, n, used);
+    else if (solver == WSPM_SOLVER_GMRES) in.gm = carve_gmres<float>(p, n, restart, used);
+    else in.cg = carve_cg<float>(p, n, used);
+    return in;
+}
+
+// Kernels launched by one inner solve of k iterations: CG one resident launch;
+// BiCGSTAB init + 4 per iteration; GMRES(m) 2 + (4m + 4) per restart cycle.
+__device__ __forceinline__ int inner_launches(int solver, int m, int k) {
+    if (k < 0) k = -k;
+    if (solver == WSPM_SOLVER_BICGSTAB) return 1 + 4 * k;
+    if (solver == WSPM_SOLVER_GMRES) return 2 + (4 * m + 4) * k;
+    return 1;
+}
 
 
 // Start of the refinement loop: x = x0, r = b - A x0 (FP64), the FP32 copy of
@@ -193,8 +229,8 @@ template <int MW>
 __global__ void __launch_bounds__(kBlock) ir_update_kernel(Sell A, const double *__restrict__ vals,
                                                            const float *__restrict__ d, double *x, double *r,
                                                            double *partials, KrylovState *irs,
-                                                           const KrylovState *inner, double tol, double inner_floor,
-                                                           int maxit, const int *skip,
+                                                           const KrylovState *inner, int inner_solver, int inner_m,
+                                                           double tol, double inner_floor, int maxit, const int *skip,
                                                            cudaGraphConditionalHandle cond, int use_cond) {
     // every block reads the word before any block can reach the reduction tail that rewrites it
     if (skip && *(volatile const int *)skip) return;
@@ -208,8 +244,52 @@ __global__ void __launch_bounds__(kBlock) ir_update_kernel(Sell A, const double 
     if (publish_partials<double, 2>(v, partials, &irs->ticket[0])) {
         double tot[2];
         final_sum<double, 2>(partials, tot, &irs->ticket[0]);
-        if (threadIdx.x == 0) ir_decide(tot, irs, inner, 0, tol, inner_floor, maxit, cond, use_cond);
+        if (threadIdx.x == 0)
+            ir_decide(tot, irs, inner, 0, tol, inner_floor, maxit, cond, use_cond,
+                      inner_launches(inner_solver, inner_m, inner->k));
     }
+}
+
+static int read_flag(const int *dev_word, cudaStream_t st, int *out, int *pinned);
+
+// One FP32 solve of A d = r64 from d = 0 to the relative tolerance the
+// refinement loop left in *tol_dev.  use_cond = 1 (graph capture): BiCGSTAB and
+// GMRES loop in a nested WHILE node; use_cond = 0 (host-driven mode): bounded
+// chunks of loop bodies between host reads of the solver's done word.  `skip`
+// (CG only): the resident launch returns at once when the word is set.
+static int inner_enqueue(const Sell &A, const float *vals32, const double *r64, float *x32, const float *dv32,
+                         const InnerSolver &in, double inner_tol, int inner_maxiter, const double *tol_dev,
+                         cudaStream_t s, int use_cond, const int *skip, int *pinned) {
+    if (in.solver == WSPM_SOLVER_CG) {
+        const int rc = pcg_persistent_enqueue<float>(A, vals32, nullptr, r64, x32, dv32, in.cg, inner_tol, 0.0,
+                                                     inner_maxiter, true, tol_dev, s, true, skip);
+        if (rc == WSPM_UNSUPPORTED)
+            return cg_persistent_enqueue<float>(A, vals32, nullptr, r64, x32, dv32, in.cg, inner_tol, 0.0,
+                                                inner_maxiter, true, tol_dev, s, skip);
+        return rc;
+    }
+    constexpr int kChunk = 8;
+    cudaGraphConditionalHandle hk = cudaGraphConditionalHandle();
+    if (use_cond && make_cond_handle(s, &hk) != cudaSuccess) return WSPM_CUDA_ERROR;
+    auto body = [&](cudaStream_t b) {
+        if (in.solver == WSPM_SOLVER_BICGSTAB)
+            bicgstab_enqueue_body<float>(A, vals32, x32, dv32, in.bicg, inner_maxiter, hk, use_cond, b);
+        else
+            gmres_enqueue_body<float>(A, vals32, nullptr, r64, x32, dv32, in.gm, inner_maxiter, hk, use_cond, b);
+    };
+    if (in.solver == WSPM_SOLVER_BICGSTAB)
+        bicgstab_enqueue_init<float>(A, vals32, nullptr, r64, nullptr, x32, in.bicg, inner_tol, 0.0, tol_dev,
+                                     inner_maxiter, hk, use_cond, s);
+    else
+        gmres_enqueue_init<float>(A, vals32, nullptr, r64, nullptr, x32, dv32, in.gm, inner_tol, 0.0, tol_dev,
+                                  inner_maxiter, hk, use_cond, s);
+    if (use_cond) return capture_while(s, hk, body) == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+    int flag = 0, rc = WSPM_OK;
+    for (int b = 0; b < inner_maxiter + 1 && rc == WSPM_OK; b += kChunk) {
+        if ((rc = read_flag(&in.st()->done, s, &flag, pinned)) != WSPM_OK || flag) break;
+        for (int c = 0; c < kChunk; ++c) body(s);
+    }
+    return rc;
 }
 
 struct PicardPlan {
@@ -224,9 +304,9 @@ struct PicardPlan {
     PicardState *ps = nullptr;
     double *partials = nullptr;
     CgBuffers<double> cg64;
-    CgBuffers<float> cg32;
-    BicgBuffers bicg;
-    GmresBuffers gm;
+    InnerSolver inner;              // mixed path: the FP32 corrections
+    BicgBuffers<double> bicg;
+    GmresBuffers<double> gm;
     KrylovState *irs = nullptr;
     double *r64 = nullptr;
     float *x32 = nullptr, *dinv32 = nullptr;
@@ -254,7 +334,7 @@ int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
     const int64_t vec = (n + 31) & ~int64_t(31);
     int64_t t = 64 + ((sizeof(PicardState) + 7) / 8) + 2 * kMaxPartials + 64;
     if (mixed) {
-        t += cg_workspace_doubles(n, 4) + 64 + vec /* r64 */ + vec /* x32 + dinv32 as floats */ + 64;
+        t += inner_workspace_doubles(n, solver, restart) + 64 + vec /* r64 */ + vec /* x32 + dinv32 as floats */ + 64;
         t += 64 + ((sizeof(KrylovState) + 7) / 8);
     } else if (solver == WSPM_SOLVER_BICGSTAB) {
         t += bicgstab_workspace_doubles(n);
@@ -264,19 +344,6 @@ int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
         t += cg_workspace_doubles(n, 8);
     }
     return t;
-}
-
-// FP32 inner solve of the refinement loop (correction d of A d = r64, from 0):
-// the pipelined CG where the pattern and the per-block vectors allow it (the
-// outer loop measures the true FP64 residual, so the pipelined recurrences
-// cannot hide an inaccurate inner solve), else the single-reduction form.
-static void inner_cg_enqueue(const Sell &A, const wspm_picard_desc &d, PicardPlan *P, const float *dv32,
-                             cudaStream_t s, const int *skip = nullptr) {
-    const int rc = pcg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol,
-                                                 0.0, d.inner_maxiter, true, &P->irs->inner_tol, s, true, skip);
-    if (rc == WSPM_UNSUPPORTED)
-        cg_persistent_enqueue<float>(A, d.vals32, nullptr, P->r64, P->x32, dv32, P->cg32, d.inner_tol, 0.0,
-                                     d.inner_maxiter, true, &P->irs->inner_tol, s, skip);
 }
 
 static int build_picard_graph(PicardPlan *P) {
@@ -296,7 +363,7 @@ static int build_picard_graph(PicardPlan *P) {
     e = make_cond_handle(cs, &hp);
     state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)P->ps->ticket, 4);
     {
-        KrylovState *sts[4] = {P->cg64.st, P->cg32.st, P->bicg.st, P->gm.st};
+        KrylovState *sts[4] = {P->cg64.st, d.mixed ? P->inner.st() : nullptr, P->bicg.st, P->gm.st};
         for (KrylovState *k : sts)
             if (k) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
         if (P->irs) state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)P->irs, (int)(sizeof(KrylovState) / 4));
@@ -327,41 +394,39 @@ static int build_picard_graph(PicardPlan *P) {
                                                                                   P->partials, P->irs, d.krylov_tol,
                                                                                   d.inner_tol, d.refine_maxiter, hir,
                                                                                   1));
-            // the first correction as plain nodes (both kernels return at once when the start already met
-            // the tolerance), the rest inside the WHILE node: one body launch fewer per Picard iteration
             const float *dv32 = dinv ? P->dinv32 : nullptr;
-            inner_cg_enqueue(A, d, P, dv32, bs, &P->irs->done);
-            WSPM_WIDTH_DISPATCH(A.max_width,
-                                ir_update_kernel<MW><<<nb, kBlock, 0, bs>>>(A, d.vals, P->x32, d.x, P->r64,
-                                                                            P->partials, P->irs, P->cg32.st,
-                                                                            d.krylov_tol, d.inner_tol,
-                                                                            d.refine_maxiter, &P->irs->done, hir,
-                                                                            1));
-            capture_while(bs, hir, [&](cudaStream_t ibs) {
-                inner_cg_enqueue(A, d, P, dv32, ibs);
+            const InnerSolver &in = P->inner;
+            auto correction = [&](cudaStream_t cb, const int *skip) {
+                inner_enqueue(A, d.vals32, P->r64, P->x32, dv32, in, d.inner_tol, d.inner_maxiter,
+                              &P->irs->inner_tol, cb, 1, skip, nullptr);
                 WSPM_WIDTH_DISPATCH(A.max_width,
-                                    ir_update_kernel<MW><<<nb, kBlock, 0, ibs>>>(A, d.vals, P->x32, d.x, P->r64,
-                                                                                 P->partials, P->irs, P->cg32.st,
-                                                                                 d.krylov_tol, d.inner_tol,
-                                                                                 d.refine_maxiter, nullptr, hir, 1));
-            });
+                                    ir_update_kernel<MW><<<nb, kBlock, 0, cb>>>(A, d.vals, P->x32, d.x, P->r64,
+                                                                                P->partials, P->irs, in.st(),
+                                                                                in.solver, in.gm.m, d.krylov_tol,
+                                                                                d.inner_tol, d.refine_maxiter, skip,
+                                                                                hir, 1));
+            };
+            // CG: the first correction as plain nodes (both kernels return at once when the start already met
+            // the tolerance), the rest inside the WHILE node: one body launch fewer per Picard iteration
+            if (in.solver == WSPM_SOLVER_CG) correction(bs, &P->irs->done);
+            capture_while(bs, hir, [&](cudaStream_t ibs) { correction(ibs, nullptr); });
             irs = P->irs;
         } else if (d.solver == WSPM_SOLVER_BICGSTAB) {
             cudaGraphConditionalHandle hk;
             make_cond_handle(bs, &hk);
-            bicgstab_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, P->bicg, d.krylov_tol, 0.0, d.krylov_maxiter, hk, 1,
-                                  bs);
+            bicgstab_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, P->bicg, d.krylov_tol, 0.0, nullptr,
+                                          d.krylov_maxiter, hk, 1, bs);
             capture_while(bs, hk, [&](cudaStream_t kbs) {
-                bicgstab_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->bicg, d.krylov_maxiter, hk, 1, kbs);
+                bicgstab_enqueue_body<double>(A, d.vals, d.x, dinv, P->bicg, d.krylov_maxiter, hk, 1, kbs);
             });
             ks = P->bicg.st;
         } else if (d.solver == WSPM_SOLVER_GMRES) {
             cudaGraphConditionalHandle hk;
             make_cond_handle(bs, &hk);
-            gmres_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, dinv, P->gm, d.krylov_tol, 0.0, d.krylov_maxiter, hk, 1,
-                               bs);
+            gmres_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, dinv, P->gm, d.krylov_tol, 0.0, nullptr,
+                                       d.krylov_maxiter, hk, 1, bs);
             capture_while(bs, hk, [&](cudaStream_t kbs) {
-                gmres_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->gm, d.krylov_maxiter, hk, 1, kbs);
+                gmres_enqueue_body<double>(A, d.vals, d.rhs, nullptr, d.x, dinv, P->gm, d.krylov_maxiter, hk, 1, kbs);
             });
             ks = P->gm.st;
         } else {
@@ -408,7 +473,7 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
     int rc = WSPM_OK, flag = 0;
     constexpr int kChunk = 8;
     state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)P->ps->ticket, 4);
-    KrylovState *sts[5] = {P->cg64.st, P->cg32.st, P->bicg.st, P->gm.st, P->irs};
+    KrylovState *sts[5] = {P->cg64.st, d.mixed ? P->inner.st() : nullptr, P->bicg.st, P->gm.st, P->irs};
     for (KrylovState *k : sts)
         if (k) state_reset_kernel<<<1, 32, 0, st>>>((unsigned int *)k, (int)(sizeof(KrylovState) / 4));
     if (P->Ks_inc) launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, st);
@@ -435,26 +500,29 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                                                                                   d.inner_tol, d.refine_maxiter, none,
                                                                                   0));
             const float *dv32 = dinv ? P->dinv32 : nullptr;
+            const InnerSolver &in = P->inner;
             for (int r = 0; r <= d.refine_maxiter && rc == WSPM_OK; ++r) {
                 if ((rc = read_flag(&P->irs->done, st, &flag, pinned)) != WSPM_OK || flag) break;
-                inner_cg_enqueue(A, d, P, dv32, st);
+                rc = inner_enqueue(A, d.vals32, P->r64, P->x32, dv32, in, d.inner_tol, d.inner_maxiter,
+                                   &P->irs->inner_tol, st, 0, nullptr, pinned);
                 WSPM_WIDTH_DISPATCH(A.max_width,
                                     ir_update_kernel<MW><<<nb, kBlock, 0, st>>>(A, d.vals, P->x32, d.x, P->r64,
-                                                                                P->partials, P->irs, P->cg32.st,
-                                                                                d.krylov_tol, d.inner_tol,
-                                                                                d.refine_maxiter, nullptr, none, 0));
+                                                                                P->partials, P->irs, in.st(),
+                                                                                in.solver, in.gm.m, d.krylov_tol,
+                                                                                d.inner_tol, d.refine_maxiter, nullptr,
+                                                                                none, 0));
             }
             irs = P->irs;
         } else {
             KrylovState *kst = nullptr;
             int max_bodies = d.krylov_maxiter;
             if (d.solver == WSPM_SOLVER_BICGSTAB) {
-                bicgstab_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, P->bicg, d.krylov_tol, 0.0, d.krylov_maxiter, none,
-                                      0, st);
+                bicgstab_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, P->bicg, d.krylov_tol, 0.0,
+                                              nullptr, d.krylov_maxiter, none, 0, st);
                 kst = P->bicg.st;
             } else if (d.solver == WSPM_SOLVER_GMRES) {
-                gmres_enqueue_init(A, d.vals, d.rhs, d.h_m, d.x, dinv, P->gm, d.krylov_tol, 0.0, d.krylov_maxiter,
-                                   none, 0, st);
+                gmres_enqueue_init<double>(A, d.vals, d.rhs, nullptr, d.h_m, d.x, dinv, P->gm, d.krylov_tol, 0.0,
+                                           nullptr, d.krylov_maxiter, none, 0, st);
                 kst = P->gm.st;
             } else {
                 copy_kernel_d(d.h_m, d.x, n, st);
@@ -467,9 +535,10 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
                 if ((rc = read_flag(&kst->done, st, &flag, pinned)) != WSPM_OK || flag) break;
                 for (int c = 0; c < kChunk; ++c) {
                     if (d.solver == WSPM_SOLVER_BICGSTAB)
-                        bicgstab_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->bicg, d.krylov_maxiter, none, 0, st);
+                        bicgstab_enqueue_body<double>(A, d.vals, d.x, dinv, P->bicg, d.krylov_maxiter, none, 0, st);
                     else if (d.solver == WSPM_SOLVER_GMRES)
-                        gmres_enqueue_body(A, d.vals, d.rhs, d.x, dinv, P->gm, d.krylov_maxiter, none, 0, st);
+                        gmres_enqueue_body<double>(A, d.vals, d.rhs, nullptr, d.x, dinv, P->gm, d.krylov_maxiter, none,
+                                                   0, st);
                     else
                         break;
                 }
@@ -498,7 +567,7 @@ extern "C" int wspm_picard_step_host(void *plan, void *stream) {
 
 extern "C" int64_t wspm_picard_workspace_doubles(int32_t n_rows, int32_t mixed) {
     // sized for the largest solver choice so that one buffer fits any plan
-    int64_t a = picard_workspace_doubles(n_rows, mixed, WSPM_SOLVER_GMRES, 32);
+    int64_t a = picard_workspace_doubles(n_rows, mixed, WSPM_SOLVER_GMRES, n_rows < 32 ? n_rows : 32);
     int64_t b = picard_workspace_doubles(n_rows, mixed, WSPM_SOLVER_BICGSTAB, 0);
     int64_t c = picard_workspace_doubles(n_rows, mixed, WSPM_SOLVER_CG, 0);
     return a > b ? (a > c ? a : c) : (b > c ? b : c);
@@ -520,7 +589,6 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
         return WSPM_BAD_ARG;
     if (d.mixed && !d.vals32) return WSPM_BAD_ARG;
     if (d.Ks_elem && !d.Ks_inc) return WSPM_BAD_ARG;
-    if (d.mixed && d.solver != WSPM_SOLVER_CG) return WSPM_UNSUPPORTED;
     if (d.solver == WSPM_SOLVER_GMRES && (d.restart < 1 || d.restart > 32)) return WSPM_UNSUPPORTED;
     if (d.solver < WSPM_SOLVER_CG || d.solver > WSPM_SOLVER_GMRES) return WSPM_BAD_ARG;
     if (d.work_doubles < wspm_picard_workspace_doubles(n, d.mixed)) return WSPM_BAD_ARG;
@@ -544,16 +612,17 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     P->partials = p; p += 2 * kMaxPartials + 64;
     int64_t used = 0;
     if (d.mixed) {
-        P->cg32 = carve_cg<float>(p, n, &used); p += used + 64;
+        const int m = d.restart < n ? d.restart : n;
+        P->inner = carve_inner(p, n, d.solver, m, &used); p += used + 64;
         const int64_t vec = (n + 31) & ~int64_t(31);
         P->r64 = p; p += vec;
         P->x32 = (float *)p; P->dinv32 = (float *)p + vec; p += vec + 64;
         P->irs = (KrylovState *)p; p += 64 + ((sizeof(KrylovState) + 7) / 8);
     } else if (d.solver == WSPM_SOLVER_BICGSTAB) {
-        P->bicg = carve_bicgstab(p, n, &used); p += used;
+        P->bicg = carve_bicgstab<double>(p, n, &used); p += used;
     } else if (d.solver == WSPM_SOLVER_GMRES) {
         const int m = d.restart < n ? d.restart : n;
-        P->gm = carve_gmres(p, n, m, &used); p += used;
+        P->gm = carve_gmres<double>(p, n, m, &used); p += used;
     } else {
         P->cg64 = carve_cg<double>(p, n, &used); p += used;
     }
@@ -601,7 +670,7 @@ __global__ void to_f32_kernel(const double *__restrict__ a, float *b, int64_t n)
 __global__ void mixed_result_kernel(const KrylovState *irs, int32_t *out) {
     if (threadIdx.x == 0) {
         out[0] = irs->status;
-        out[1] = irs->steps;     // FP32 CG iterations, all refinements
+        out[1] = irs->steps;     // FP32 iterations (CG, BiCGSTAB) or restart cycles (GMRES), all refinements
         out[2] = irs->k;         // refinements (FP32 solves)
         out[3] = 0;
     }
@@ -614,7 +683,7 @@ __global__ void mixed_result_kernel(const KrylovState *irs, int32_t *out) {
 struct MixedKey {
     const void *pat_cols, *pat_ptr, *pat_width, *pat_diag_off, *vals, *vals32, *b, *x, *dinv, *work, *result;
     int64_t nnz_padded;
-    int n, n_slices, max_width, n_diags, device, inner_maxiter, refine_maxiter, pad_;
+    int n, n_slices, max_width, n_diags, device, inner_maxiter, refine_maxiter, solver, restart, pad_;
     double tol, inner_tol;
     bool operator==(const MixedKey &o) const { return std::memcmp(this, &o, sizeof(MixedKey)) == 0; }
 };
@@ -630,24 +699,25 @@ constexpr size_t kMixedCacheMax = 8;
 int64_t mixed_vec(int n) { return (n + 31) & ~int64_t(31); }
 
 int build_mixed_graph(const wspm_pattern *pat, const double *vals, const float *vals32, const double *b, double *x,
-                      const double *dinv, double tol, double inner_tol, int inner_maxiter, int refine_maxiter,
-                      double *work, int32_t *result, cudaGraphExec_t *exec_out, cudaGraph_t *graph_out) {
+                      const double *dinv, int solver, int restart, double tol, double inner_tol, int inner_maxiter,
+                      int refine_maxiter, double *work, int32_t *result, cudaGraphExec_t *exec_out,
+                      cudaGraph_t *graph_out) {
     const Sell A = make_sell(pat);
     const int n = pat->n_rows;
     const int nb = reduction_blocks(n);
     const int64_t vec = mixed_vec(n);
-    // workspace: partials | refinement state | FP32 CG buffers | r64 | x32, dinv32 | vals32 (when not given),
+    // workspace: partials | refinement state | FP32 solver buffers | r64 | x32, dinv32 | vals32 (when not given),
     // every part on a 256-byte boundary (the CG kernels move 16-byte row groups)
     auto align = [](double *q) { return (double *)(((uintptr_t)q + 255) & ~(uintptr_t)255); };
     double *p = align(work);
     double *partials = p; p = align(p + 2 * kMaxPartials + 64);
     KrylovState *irs = (KrylovState *)p; p = align(p + 64 + ((sizeof(KrylovState) + 7) / 8));
     int64_t used = 0;
-    CgBuffers<float> cg32 = carve_cg<float>(p, n, &used); p = align(p + used + 64);
+    const InnerSolver in = carve_inner(p, n, solver, restart < n ? restart : n, &used);
+    p = align(p + used + 64);
     double *r64 = p; p = align(p + vec);
     float *x32 = (float *)p, *dinv32 = (float *)p + vec; p = align(p + vec + 64);
     float *v32 = vals32 ? const_cast<float *>(vals32) : (float *)p;
-    const bool pipelined = pcg_eligible<float>(A);
     cudaStream_t cs;
     WSPM_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g;
@@ -655,7 +725,7 @@ int build_mixed_graph(const wspm_pattern *pat, const double *vals, const float *
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
     if (e == cudaSuccess) {
         state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)irs, (int)(sizeof(KrylovState) / 4));
-        state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)cg32.st, (int)(sizeof(KrylovState) / 4));
+        state_reset_kernel<<<1, 32, 0, cs>>>((unsigned int *)in.st(), (int)(sizeof(KrylovState) / 4));
         if (!vals32) to_f32_kernel<<<reduction_blocks(pat->nnz_padded), kBlock, 0, cs>>>(vals, v32, pat->nnz_padded);
         cudaGraphConditionalHandle h;
         e = make_cond_handle(cs, &h);
@@ -663,22 +733,18 @@ int build_mixed_graph(const wspm_pattern *pat, const double *vals, const float *
         WSPM_WIDTH_DISPATCH(A.max_width,
                             ir_residual_kernel<MW><<<nb, kBlock, 0, cs>>>(A, vals, b, x, x, r64, dinv, dv32, partials,
                                                                           irs, tol, inner_tol, refine_maxiter, h, 1));
-        // one correction: the FP32 solve (skipped when `skip` is set at launch) and x += d, r -= A d
+        // one correction: the FP32 solve (CG: skipped when `skip` is set at launch) and x += d, r -= A d
         auto correction = [&](cudaStream_t bs, const int *skip) {
-            int rc = WSPM_UNSUPPORTED;
-            if (pipelined)
-                rc = pcg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0,
-                                                   inner_maxiter, true, &irs->inner_tol, bs, true, skip);
-            if (rc == WSPM_UNSUPPORTED)
-                cg_persistent_enqueue<float>(A, v32, nullptr, r64, x32, dv32, cg32, inner_tol, 0.0, inner_maxiter,
-                                             true, &irs->inner_tol, bs, skip);
+            if (inner_enqueue(A, v32, r64, x32, dv32, in, inner_tol, inner_maxiter, &irs->inner_tol, bs, 1, skip,
+                              nullptr) != WSPM_OK)
+                e = cudaErrorLaunchFailure;
             WSPM_WIDTH_DISPATCH(A.max_width,
                                 ir_update_kernel<MW><<<nb, kBlock, 0, bs>>>(A, vals, x32, x, r64, partials, irs,
-                                                                            cg32.st, tol, inner_tol, refine_maxiter,
-                                                                            skip, h, 1));
+                                                                            in.st(), in.solver, in.gm.m, tol,
+                                                                            inner_tol, refine_maxiter, skip, h, 1));
         };
-        // the first correction as plain nodes, the rest inside the WHILE node
-        if (e == cudaSuccess) correction(cs, &irs->done);
+        // CG: the first correction as plain nodes, the rest inside the WHILE node
+        if (e == cudaSuccess && solver == WSPM_SOLVER_CG) correction(cs, &irs->done);
         if (e == cudaSuccess) e = capture_while(cs, h, [&](cudaStream_t bs) { correction(bs, nullptr); });
         mixed_result_kernel<<<1, 32, 0, cs>>>(irs, result);
         cudaGraph_t out = nullptr;
@@ -695,22 +761,30 @@ int build_mixed_graph(const wspm_pattern *pat, const double *vals, const float *
 
 }  // namespace
 
-extern "C" int64_t wspm_krylov_mixed_workspace_doubles(int32_t n_rows, int64_t nnz_padded) {
-    if (n_rows <= 0 || nnz_padded <= 0) return 0;
+extern "C" int64_t wspm_krylov_mixed_workspace_doubles(int32_t n_rows, int64_t nnz_padded, int32_t solver,
+                                                       int32_t restart) {
+    if (n_rows <= 0 || nnz_padded <= 0 || solver < WSPM_SOLVER_CG || solver > WSPM_SOLVER_GMRES) return 0;
+    if (solver == WSPM_SOLVER_GMRES && (restart < 1 || restart > 32)) return 0;
     const int64_t vec = mixed_vec(n_rows);
-    return 2 * kMaxPartials + 64 + 64 + ((sizeof(KrylovState) + 7) / 8) + cg_workspace_doubles(n_rows, 4) + 64 +
-           vec + vec + 64 + (nnz_padded + 1) / 2 + 64 + 6 * 32;   // + alignment slack of six parts
+    const int m = restart < n_rows ? restart : n_rows;
+    return 2 * kMaxPartials + 64 + 64 + ((sizeof(KrylovState) + 7) / 8) + inner_workspace_doubles(n_rows, solver, m) +
+           64 + vec + vec + 64 + (nnz_padded + 1) / 2 + 64 + 6 * 32;   // + alignment slack of six parts
 }
 
 extern "C" int wspm_krylov_solve_mixed(const wspm_pattern *pat, const double *vals, const float *vals32,
-                                       const double *b, double *x, const double *dinv, double tol, double inner_tol,
-                                       int32_t inner_maxiter, int32_t refine_maxiter, double *work,
-                                       int64_t work_doubles, int32_t *result, void *stream) {
+                                       const double *b, double *x, const double *dinv, int32_t solver,
+                                       int32_t restart, double tol, double inner_tol, int32_t inner_maxiter,
+                                       int32_t refine_maxiter, double *work, int64_t work_doubles, int32_t *result,
+                                       void *stream) {
     if (!pattern_layout_ok(pat)) return WSPM_BAD_ARG;
     if (!vals || !b || !x || !work || !result) return WSPM_BAD_ARG;
+    if (solver < WSPM_SOLVER_CG || solver > WSPM_SOLVER_GMRES) return WSPM_BAD_ARG;
+    if (solver == WSPM_SOLVER_GMRES && (restart < 1 || restart > 32)) return WSPM_UNSUPPORTED;
+    if (solver != WSPM_SOLVER_GMRES) restart = 0;
     if (!(tol > 0.0) || !(inner_tol > 0.0) || inner_tol >= 1.0 || inner_maxiter < 1 || refine_maxiter < 1)
         return WSPM_BAD_ARG;
-    if (work_doubles < wspm_krylov_mixed_workspace_doubles(pat->n_rows, pat->nnz_padded)) return WSPM_BAD_ARG;
+    const int64_t need = wspm_krylov_mixed_workspace_doubles(pat->n_rows, pat->nnz_padded, solver, restart > 0 ? restart : 1);
+    if (need <= 0 || work_doubles < need) return WSPM_BAD_ARG;
     MixedKey key;
     std::memset(&key, 0, sizeof(key));
     key.pat_cols = pat->cols; key.pat_ptr = pat->slice_ptr; key.pat_width = pat->slice_width;
@@ -720,6 +794,7 @@ extern "C" int wspm_krylov_solve_mixed(const wspm_pattern *pat, const double *va
     key.n = pat->n_rows; key.n_slices = pat->n_slices; key.max_width = pat->max_width; key.n_diags = pat->n_diags;
     WSPM_CUDA_TRY(cudaGetDevice(&key.device));
     key.inner_maxiter = inner_maxiter; key.refine_maxiter = refine_maxiter; key.tol = tol;
+    key.solver = solver; key.restart = restart;
     key.inner_tol = inner_tol;
     cudaGraphExec_t exec = nullptr;
     {
@@ -728,8 +803,8 @@ extern "C" int wspm_krylov_solve_mixed(const wspm_pattern *pat, const double *va
             if (en.key == key) { exec = en.exec; break; }
         if (!exec) {
             cudaGraph_t graph = nullptr;
-            const int rc = build_mixed_graph(pat, vals, vals32, b, x, dinv, tol, inner_tol, inner_maxiter,
-                                             refine_maxiter, work, result, &exec, &graph);
+            const int rc = build_mixed_graph(pat, vals, vals32, b, x, dinv, solver, restart, tol, inner_tol,
+                                             inner_maxiter, refine_maxiter, work, result, &exec, &graph);
             if (rc != WSPM_OK) return rc;
             if (g_mixed.size() >= kMixedCacheMax) {
                 cudaGraphExecDestroy(g_mixed.front().exec);

@@ -132,9 +132,10 @@ _SIGS = {
     "wspm_krylov_workspace_doubles": (c_int64, [c_int32, c_int32, c_int32]),
     "wspm_krylov_solve": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_double,
                                     c_double, c_int32, c_int32, c_void_p, c_int64, c_void_p, c_void_p]),
-    "wspm_krylov_mixed_workspace_doubles": (c_int64, [c_int32, c_int64]),
-    "wspm_krylov_solve_mixed": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
-                                          c_double, c_int32, c_int32, c_void_p, c_int64, c_void_p, c_void_p]),
+    "wspm_krylov_mixed_workspace_doubles": (c_int64, [c_int32, c_int64, c_int32, c_int32]),
+    "wspm_krylov_solve_mixed": (c_int32, [P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
+                                          c_int32, c_double, c_double, c_int32, c_int32, c_void_p, c_int64, c_void_p,
+                                          c_void_p]),
     "wspm_cg_iterations": (c_int32, [P(WspmPattern), c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
                                      c_void_p, c_int64, c_void_p, c_void_p]),
     "wspm_read_probe": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_void_p]),

@@ -241,14 +241,21 @@ def krylov_solve(dm, vals, b, x0, solver="cg", dinv=None, tol=1e-10, atol=0.0, m
 
 
 def krylov_solve_mixed(dm, vals, b, x0, dinv=None, tol=1e-8, inner_tol=1e-5, inner_maxiter=20000,
-                       refine_maxiter=20, vals32=None, workspace=None, x_out=None, result=None):
-    """A x = b with FP32 Jacobi-CG corrections inside FP64 iterative refinement (``wspm_krylov_solve_mixed``):
-    the FP64 residual ||b - A x|| reaches tol ||b||.  Returns (x, status tensor[4] on the device: status, FP32 CG
-    iterations, corrections, 0).  ``workspace`` (float64, wspm_krylov_mixed_workspace_doubles entries), ``x_out``
-    and ``result`` (int32[4]) may be kept across calls: the captured graph is cached per argument set, so repeated
-    solves with the same buffers replay it."""
+                       refine_maxiter=20, vals32=None, workspace=None, x_out=None, result=None, solver="cg",
+                       restart=30):
+    """A x = b with FP32 Krylov corrections (``solver``: cg, bicgstab or gmres with ``restart``) inside FP64
+    iterative refinement (``wspm_krylov_solve_mixed``): the FP64 residual ||b - A x|| reaches tol ||b||.  Returns
+    (x, status tensor[4] on the device: status, FP32 iterations (GMRES: restart cycles), corrections, 0).
+    ``workspace`` (float64, wspm_krylov_mixed_workspace_doubles entries), ``x_out`` and ``result`` (int32[4]) may
+    be kept across calls: the captured graph is cached per argument set, so repeated solves with the same buffers
+    replay it."""
+    if solver not in _lib.SOLVERS:
+        raise ValueError(f"Unsupported solver type: {solver}")
     _require_cuda(b, torch.float64, "b", dm.n_nodes)
-    need = int(lib.wspm_krylov_mixed_workspace_doubles(dm.n_nodes, dm.nnz_padded))
+    sid = _lib.SOLVERS[solver]
+    need = int(lib.wspm_krylov_mixed_workspace_doubles(dm.n_nodes, dm.nnz_padded, sid, int(restart)))
+    if need <= 0:
+        raise ValueError(f"unsupported mixed solve ({solver}, restart {restart})")
     work = workspace if workspace is not None else torch.empty(need, dtype=torch.float64, device=b.device)
     if work.numel() < need:
         raise ValueError("workspace too small")
@@ -257,8 +264,9 @@ def krylov_solve_mixed(dm, vals, b, x0, dinv=None, tol=1e-8, inner_tol=1e-5, inn
     x = x_out if x_out is not None else torch.empty_like(b)
     x.copy_(x0)
     check("krylov_solve_mixed", lib.wspm_krylov_solve_mixed(
-        ctypes.byref(dm.c_pat), dptr(vals), dptr(vals32), dptr(b), dptr(x), dptr(dinv), float(tol), float(inner_tol),
-        int(inner_maxiter), int(refine_maxiter), dptr(work), work.numel(), dptr(result), _stream()))
+        ctypes.byref(dm.c_pat), dptr(vals), dptr(vals32), dptr(b), dptr(x), dptr(dinv), sid, int(restart), float(tol),
+        float(inner_tol), int(inner_maxiter), int(refine_maxiter), dptr(work), work.numel(), dptr(result),
+        _stream()))
     return x, result
 
 

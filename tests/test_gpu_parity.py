@@ -199,30 +199,36 @@ def test_krylov_solve_matches_oracle(solver, precond, layout):
     np.testing.assert_allclose(host(x), x_ref, rtol=1e-7, atol=1e-7)
 
 
-@pytest.mark.parametrize("layout,n", [("dia", 30), ("dia", 256), ("sell", 30)])
-def test_krylov_solve_mixed_reaches_fp64_residual(layout, n):
-    """wspm_krylov_solve_mixed: FP32 corrections (pipelined CG on the DIA layout, single-reduction CG on SELL)
-    inside FP64 refinement reach the FP64 residual 1e-8 ||b|| and the FP64 solution; a second call replays the
-    cached graph and gives bitwise the same x."""
+@pytest.mark.parametrize("solver,layout,n", [("cg", "dia", 30), ("cg", "dia", 256), ("cg", "sell", 30),
+                                             ("bicgstab", "dia", 30), ("bicgstab", "dia", 256),
+                                             ("bicgstab", "sell", 30), ("gmres", "dia", 30), ("gmres", "dia", 256),
+                                             ("gmres", "sell", 30)])
+def test_krylov_solve_mixed_reaches_fp64_residual(solver, layout, n):
+    """wspm_krylov_solve_mixed: FP32 corrections (CG: pipelined on the DIA layout, single-reduction on SELL;
+    BiCGSTAB; GMRES(30)) inside FP64 refinement reach the FP64 residual 1e-8 ||b|| and the FP64 solution of the
+    oracle; a second call replays the cached graph and gives bitwise the same x."""
     pts, el, A, b, h = _linear_system(n=n)
     D = dev()
     dm = D.DeviceMesh(pts, el, layout=layout)
     vals = cu(dm.pattern.sell_from_csr_values(A.data))
     dinv = D.jacobi_dinv(dm, vals)
-    ws = torch.empty(int(D.lib.wspm_krylov_mixed_workspace_doubles(dm.n_nodes, dm.nnz_padded)),
+    sid = D._lib.SOLVERS[solver]
+    ws = torch.empty(int(D.lib.wspm_krylov_mixed_workspace_doubles(dm.n_nodes, dm.nnz_padded, sid, 30)),
                      dtype=torch.float64, device="cuda")
     bb, xx = cu(b), torch.empty(dm.n_nodes, dtype=torch.float64, device="cuda")
     res = torch.zeros(4, dtype=torch.int32, device="cuda")
-    x, res = D.krylov_solve_mixed(dm, vals, bb, cu(h), dinv=dinv, tol=1e-8, workspace=ws, x_out=xx, result=res)
+    kw = dict(dinv=dinv, tol=1e-8, workspace=ws, x_out=xx, result=res, solver=solver, restart=30,
+              inner_maxiter=20000 if solver != "gmres" else 2000)
+    x, res = D.krylov_solve_mixed(dm, vals, bb, cu(h), **kw)
     status, inner, corrections = host(res)[:3]
     assert status == 0 and corrections >= 1 and inner > 0
     xh = host(x)
     assert np.linalg.norm(b - A @ xh) <= 1.0001e-8 * np.linalg.norm(b)
-    exact = np.linalg.solve(A.toarray(), b) if n <= 30 else okry.cg(A, b, h, tol=1e-12, maxiter=20000,
-                                                                     dinv=okry.jacobi_inverse_diagonal(A))[0]
+    exact = np.linalg.solve(A.toarray(), b) if n <= 30 else okry.solve_system(A, b, h, solver, "jacobi", tol=1e-12,
+                                                                             maxiter=20000, restart=30)[0]
     np.testing.assert_allclose(xh, exact, rtol=1e-6, atol=1e-6)
     first = x.clone()
-    x2, _ = D.krylov_solve_mixed(dm, vals, bb, cu(h), dinv=dinv, tol=1e-8, workspace=ws, x_out=xx, result=res)
+    x2, _ = D.krylov_solve_mixed(dm, vals, bb, cu(h), **kw)
     assert torch.equal(first, x2)
 
 
@@ -421,6 +427,47 @@ def test_mixed_precision_refinement_reaches_fp64_residual(layout):
         out[mixed] = res
     np.testing.assert_array_equal(out[True]["iterations"], out[False]["iterations"])
     np.testing.assert_allclose(out[True]["pressure_head"], out[False]["pressure_head"], rtol=1e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("solver,dim", [("bicgstab", 3), ("gmres", 2), ("bicgstab", 2)])
+def test_mixed_precision_nonsymmetric_solvers_in_the_picard_step(solver, dim):
+    """FP32 BiCGSTAB / GMRES(30) corrections inside the FP64 refinement of the Picard graph (and in its host-driven
+    mode): the same Picard iterations as the plain FP64 solver, every linear system to the FP64 residual 1e-8, heads
+    agreeing to that accuracy, and the FP64 oracle's step reproduced."""
+    from wspm_b200.device import DeviceMesh, merge_dirichlet, spmv
+    from wspm_b200.engine import PicardEngine
+    if dim == 3:
+        pts, el = mesh.kuhn_tetrahedra(14, 1.0)
+        top = np.where(np.abs(pts[:, 2] - 1.0) < 1e-12)[0]
+        Ks = None
+    else:
+        pts, el = mesh.structured_triangles(64, 1.0)
+        top = np.where(pts[:, 1] == 1.0)[0]
+        Ks = 0.0922 * np.exp(np.random.default_rng(7).standard_normal(len(el)))
+    bc = merge_dirichlet(len(pts), [(top, -0.1)])
+    phi = opic.VG_UNIT_PHI if Ks is None else opic.VG_UNIT_PHI[:5] + (1.0,)
+    dm = DeviceMesh(pts, el)
+    kw = dict(Ks_elem=Ks, bc_val=bc, solver=solver, precond="jacobi", krylov_tol=1e-8, restart=30,
+              krylov_maxiter=2000 if solver == "bicgstab" else 200, inner_maxiter=2000 if solver == "bicgstab" else 200)
+    out = {}
+    for mixed, host_loop in ((False, False), (True, False), (True, True)):
+        eng = PicardEngine(dm, "vg", phi, mixed=mixed, **kw)
+        eng.host_loop = host_loop
+        res = eng.run(-np.ones(len(pts)), 1e-4, 1e-3, fixed_dt=True, max_steps=2)
+        assert np.all(res["status"] == 0), res["status"]
+        r = eng.rhs - spmv(dm, eng.vals, eng.x)
+        assert float(torch.linalg.norm(r) / torch.linalg.norm(eng.rhs)) <= 1.01e-8
+        out[(mixed, host_loop)] = res
+    for key in ((True, False), (True, True)):
+        np.testing.assert_array_equal(out[key]["iterations"], out[(False, False)]["iterations"])
+        np.testing.assert_allclose(out[key]["pressure_head"], out[(False, False)]["pressure_head"], rtol=1e-6,
+                                   atol=1e-7)
+    np.testing.assert_array_equal(out[(True, True)]["pressure_head"], out[(True, False)]["pressure_head"])
+    prob, h0 = opic.vg_dirichlet_case(pts, el, top, Ks_elem=Ks, solver=solver, precond="jacobi", tol=1e-8,
+                                      maxiter=2000 if solver == "bicgstab" else 200, restart=30)
+    ref = opic.run_time_loop(prob, h0, 1e-4, 1e-3, fixed_dt=True, max_steps=2)
+    np.testing.assert_array_equal(out[(True, False)]["iterations"], ref["iterations"])
+    np.testing.assert_allclose(out[(True, False)]["pressure_head"], ref["pressure_head"], rtol=1e-6, atol=1e-7)
 
 
 def test_fused_refinement_start_matches_standalone_residual():
