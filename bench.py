@@ -370,34 +370,35 @@ def cg_probe(args):
     print(f"cg probe {args.cg_probe}: {args.probe_iters} iterations, |x| = {float(torch.linalg.norm(x.double())):.6e}")
 
 
-def ensemble_domains(n_domains, seed, sides=tuple(range(32, 257, 16))):
-    """Config-3 ensemble: side lengths uniform in {32, 48, ..., 256}; VG alpha, n, Ks log-uniform in
-    [1, 10], [1.3, 3], [0.01, 1]; theta_r .05, theta_s .40; h0 -1, top Dirichlet -0.1 (as the unit-square case)."""
+def ensemble_domains(n_domains, seed):
+    """Config-3 ensemble (wspm_b200.mesh.vg_parameter_ensemble): sides uniform in {32, 48, ..., 256}; VG alpha, n,
+    Ks log-uniform in [1, 10], [1.3, 3], [0.01, 1]; theta_r .05, theta_s .40; h0 -1, top Dirichlet -0.1."""
     from wspm_b200 import mesh
-    rng = np.random.default_rng(seed)
-    lu = lambda lo, hi: float(np.exp(rng.uniform(np.log(lo), np.log(hi))))  # noqa: E731
-    cache, doms = {}, []
-    for _ in range(n_domains):
-        s = int(rng.choice(sides))
-        if s not in cache:
-            pts, tri = mesh.structured_triangles(s, 1.0)
-            bc = np.full(len(pts), np.nan)
-            bc[np.abs(pts[:, 1] - 1.0) < 1e-12] = -0.1
-            cache[s] = (pts, tri, bc)
-        pts, tri, bc = cache[s]
-        n = lu(1.3, 3.0)
-        doms.append((pts, tri, (lu(1.0, 10.0), 0.40, 0.05, n, 1.0 - 1.0 / n, lu(0.01, 1.0)), bc, None))
-    return doms
+    return mesh.vg_parameter_ensemble(n_domains, seed)
 
 
 def run_ensemble(args):
     """Batched ensemble (one launch per step for all domains) vs one single-domain engine per domain."""
+    world, rank, _ = dist_setup(args)
+    line = ensemble_measure(args.domains, args.steps, args.warmup, args.seed, world, rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def ensemble_measure(n_domains, steps, warmup, seed, world=1, rank=0):
     import torch
     from wspm_b200.device import DeviceMesh
     from wspm_b200.engine import PicardEngine
     from wspm_b200.ensemble import Ensemble
     from wspm_b200.ensemble import gather_domain_results, partition_domains
-    world, rank, _ = dist_setup(args)
+
+    class _A:
+        pass
+    args = _A()
+    args.domains, args.steps, args.warmup, args.seed = n_domains, steps, warmup, seed
     all_doms = ensemble_domains(args.domains, args.seed)
     # shard the independent domains over the ranks, balancing nnz (7 per node for these meshes); no collective
     # on the data path, one gather of the per-domain iteration counts at the end
@@ -454,11 +455,6 @@ def run_ensemble(args):
     t_seq = allreduce_max(e0.elapsed_time(e1) * 1e-3, world)
     dofits_seq = allreduce_sum(float((sizes * its_s).sum()), world)
     sizes_all = np.array([len(d[0]) for d in all_doms])
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
-    if rank != 0:
-        return
     line = {"metric": "ensemble DOF*Picard-iter/s (batched domains, one launch per step)",
             "value": dofits / t_batch, "unit": "DOF*Picard-iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
@@ -475,7 +471,7 @@ def run_ensemble(args):
                         "autotune_ms": getattr(ens, "timing", {})},
             "sequential": {"seconds": t_seq, "value": dofits_seq / t_seq},
             "speedup_vs_sequential": (dofits / t_batch) / (dofits_seq / t_seq)}
-    print(json.dumps(line))
+    return line
 
 
 def run_adjoint(args):
@@ -543,69 +539,105 @@ def adjoint_measure(n, steps, seed, fd_params):
     return line
 
 
-def run_config2(args):
-    """3D Richards (Kuhn tetrahedra, BiCGSTAB + Jacobi) and a three-species transport chain on a 2D grid."""
+def config2_measure(n3d, steps, warmup, n_transport, host_loop=False):
+    """3D Richards (Kuhn tetrahedra, BiCGSTAB + Jacobi) and the three-species transport chain (GMRES(30) + Jacobi),
+    each in plain FP64 and in mixed precision (FP32 corrections of the same solver inside FP64 refinement)."""
     import torch
     from wspm_b200 import mesh
     from wspm_b200.device import (DeviceMesh, apply_dirichlet, assemble_adr, flux_dispersion, jacobi_dinv,
-                                  krylov_solve, merge_dirichlet)
+                                  krylov_solve, krylov_solve_mixed, merge_dirichlet, spmv)
     from wspm_b200.engine import PicardEngine, default_rule
     torch.cuda.set_device(0)
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = lambda: flush_buf.fill_(1.0)  # noqa: E731
     # ---- 3D Richards: unit cube, n^3 hexahedra split in 6 tets, VG c0 soil, h0 -1, top face Dirichlet -0.1
-    n = args.n3d
+    n = n3d
     pts, tets = mesh.kuhn_tetrahedra(n, 1.0)
     top = np.where(np.abs(pts[:, 2] - 1.0) < 1e-12)[0]
     dm3 = DeviceMesh(pts, tets)
-    eng = PicardEngine(dm3, "vg", VG_PHI_UNIT_KS, bc_val=merge_dirichlet(len(pts), [(top, -0.1)]),
-                       solver="bicgstab", precond="jacobi", krylov_tol=1e-8, krylov_maxiter=1000)
-    eng.host_loop = args.host_loop          # host-driven loops: the same kernels, visible to profilers
     h0 = -np.ones(len(pts))
-    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    t3 = time_path(eng, h0, 1e-4, args.steps3d, args.warmup, 1, lambda: flush_buf.fill_(1.0))
+    r3, fields = {}, {}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        eng = PicardEngine(dm3, "vg", VG_PHI_UNIT_KS, bc_val=merge_dirichlet(len(pts), [(top, -0.1)]),
+                           solver="bicgstab", precond="jacobi", krylov_tol=1e-8, krylov_maxiter=1000, mixed=mixed,
+                           inner_tol=1e-5, inner_maxiter=1000, refine_maxiter=30)
+        eng.host_loop = host_loop          # host-driven loops: the same kernels, visible to profilers
+        t = time_path(eng, h0, 1e-4, steps, warmup, 1, flush)
+        res = eng.rhs - spmv(dm3, eng.vals, eng.x)
+        r3[name] = {"ms_per_step": t["ms"] / steps, "picard_its": t["picard_its"], "krylov_its": t["krylov_its"],
+                    "value": len(pts) * t["picard_its"] / (t["ms"] * 1e-3),
+                    "true_rel_residual": float(torch.linalg.norm(res) / torch.linalg.norm(eng.rhs))}
+        if mixed:
+            r3[name]["refinements"] = t["refinements"]
+        fields[name] = eng.h_n.clone()
+        del eng
+    r3["mixed"]["rel_diff_vs_fp64"] = float(torch.linalg.norm(fields["mixed"] - fields["fp64"]) /
+                                            torch.linalg.norm(fields["fp64"]))
+    r3["mixed"]["speedup_vs_fp64"] = r3["mixed"]["value"] / r3["fp64"]["value"]
     # ---- transport chain on an m x m grid: species 1 -> 2 -> 3, first-order rates k1, k2, sorption on species 2,
     # dispersivities 0.5 / 0.1, Dirichlet 1.0 for species 1 on the top edge, GMRES(30) + Jacobi
-    m = args.n_transport
+    m = n_transport
     p2, tri = mesh.structured_triangles(m, 1.0)
     dm2 = DeviceMesh(p2, tri)
     top2 = np.where(np.abs(p2[:, 1] - 1.0) < 1e-12)[0]
     hh = torch.as_tensor(-0.5 - 0.5 * p2[:, 1], dtype=torch.float64, device="cuda")
     Q, W = default_rule(2)
-    c = [torch.zeros(len(p2), dtype=torch.float64, device="cuda") for _ in range(3)]
     k1, k2, sorption = 0.36, 0.2, 1.5 * 3.5
+    rt, conc = {}, {}
+    for name in ("fp64", "mixed"):
+        c = [torch.zeros(len(p2), dtype=torch.float64, device="cuda") for _ in range(3)]
+        stats = {"krylov": 0, "refinements": 0}
 
-    def transport_step():
-        qx, qz, aq, Dxx, Dxz, Dzz, th = flux_dispersion(dm2, hh, VG_PHI_UNIT_KS, 0.5, 0.1, 0.0)
-        up = None
-        for s_, (mu, sorp, mu_up) in enumerate(((k1, 0.0, 0.0), (k2, sorption, k1), (0.0, 0.0, k2))):
-            vals, rhs, dinv = assemble_adr(dm2, th, qx, qz, Dxx, Dxz, Dzz, c[s_], 1e-3, Q, W, mu=mu, sorption=sorp,
-                                           mu_up=mu_up, c_up=up, lumped=True)
-            if s_ == 0:
-                apply_dirichlet(dm2, top2, np.ones(top2.size), vals, rhs)
-            c[s_], _ = krylov_solve(dm2, vals, rhs, c[s_], "gmres", dinv=jacobi_dinv(dm2, vals), tol=1e-10,
-                                    maxiter=100, restart=30)
-            up = c[s_]
-    for _ in range(args.warmup):
-        transport_step()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(args.steps3d):
-        transport_step()
-    e1.record()
-    torch.cuda.synchronize()
-    t_tr = e0.elapsed_time(e1) / args.steps3d
-    line = {"metric": "3D Richards DOF*Picard-iter/s (FP64, BiCGSTAB + Jacobi) and transport-chain step time",
-            "value": len(pts) * t3["picard_its"] / (t3["ms"] * 1e-3), "unit": "DOF*Picard-iter/s", "n_gpus": 1,
-            "steps": args.steps3d, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": f"{n}^3 unit cube, Kuhn split (6 tets per hexahedron), VG "
-                                                        "c0 soil, h0 -1, top face Dirichlet -0.1, dt 1e-4 fixed",
-                                            "nodes": len(pts), "elements": len(tets), "nnz": int(dm3.pattern.nnz)},
-            "richards3d": {"ms_per_step": t3["ms"] / args.steps3d, "picard_its": t3["picard_its"],
-                           "krylov_its": t3["krylov_its"]},
-            "transport": {"workload": f"{m}^2 triangles, 3 species first-order chain (0.36, 0.2 /day), sorption "
-                                      "rho_b Kd = 5.25 on species 2, dispersivity 0.5 / 0.1, Dirichlet 1.0 inflow of "
-                                      "species 1 on the top edge, lumped mass, GMRES(30) + Jacobi, dt 1e-3",
-                          "nodes": len(p2), "ms_per_step": t_tr}}
+        def transport_step():
+            qx, qz, aq, Dxx, Dxz, Dzz, th = flux_dispersion(dm2, hh, VG_PHI_UNIT_KS, 0.5, 0.1, 0.0)
+            up = None
+            for s_, (mu, sorp, mu_up) in enumerate(((k1, 0.0, 0.0), (k2, sorption, k1), (0.0, 0.0, k2))):
+                vals, rhs, dinv = assemble_adr(dm2, th, qx, qz, Dxx, Dxz, Dzz, c[s_], 1e-3, Q, W, mu=mu,
+                                               sorption=sorp, mu_up=mu_up, c_up=up, lumped=True)
+                if s_ == 0:
+                    apply_dirichlet(dm2, top2, np.ones(top2.size), vals, rhs)
+                dinv = jacobi_dinv(dm2, vals)
+                if name == "fp64":
+                    c[s_], _ = krylov_solve(dm2, vals, rhs, c[s_], "gmres", dinv=dinv, tol=1e-10, maxiter=100,
+                                            restart=30)
+                else:
+                    c[s_], _ = krylov_solve_mixed(dm2, vals, rhs, c[s_], dinv=dinv, tol=1e-10, inner_tol=1e-5,
+                                                  inner_maxiter=100, refine_maxiter=30, solver="gmres", restart=30)
+                up = c[s_]
+        for _ in range(warmup):
+            transport_step()
+        for s_ in range(3):
+            c[s_].zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            transport_step()
+        e1.record()
+        torch.cuda.synchronize()
+        rt[name] = {"ms_per_step": e0.elapsed_time(e1) / steps}
+        conc[name] = torch.cat(c)
+    rt["mixed"]["rel_diff_vs_fp64"] = float(torch.linalg.norm(conc["mixed"] - conc["fp64"]) /
+                                            torch.linalg.norm(conc["fp64"]))
+    rt["mixed"]["speedup_vs_fp64"] = rt["fp64"]["ms_per_step"] / rt["mixed"]["ms_per_step"]
+    return {"richards3d": dict(workload=f"{n}^3 unit cube, Kuhn split (6 tets per hexahedron), VG c0 soil, h0 -1, "
+                                        f"top face Dirichlet -0.1, dt 1e-4 fixed, BiCGSTAB + Jacobi to 1e-8, "
+                                        f"{steps} steps", nodes=len(pts), elements=len(tets),
+                               nnz=int(dm3.pattern.nnz), **r3),
+            "transport": dict(workload=f"{m}^2 triangles, 3 species first-order chain (0.36, 0.2 /day), sorption "
+                                       "rho_b Kd = 5.25 on species 2, dispersivity 0.5 / 0.1, Dirichlet 1.0 inflow "
+                                       "of species 1 on the top edge, lumped mass, GMRES(30) + Jacobi to 1e-10 "
+                                       f"(mixed: true FP64 residual), dt 1e-3, {steps} steps", nodes=len(p2), **rt)}
+
+
+def run_config2(args):
+    """3D Richards on Kuhn tetrahedra and a three-species transport chain, FP64 and mixed; own JSON line."""
+    r = config2_measure(args.n3d, args.steps3d, args.warmup, args.n_transport, args.host_loop)
+    line = {"metric": "3D Richards DOF*Picard-iter/s (BiCGSTAB + Jacobi; FP64 and mixed) and transport-chain "
+                      "step time (GMRES(30); FP64 and mixed)",
+            "value": r["richards3d"]["mixed"]["value"], "unit": "DOF*Picard-iter/s", "n_gpus": 1,
+            "steps": args.steps3d, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64 / f32+f64",
+            "data": "synthetic", "config": {"workload": r["richards3d"]["workload"]}, **r}
     print(json.dumps(line))
 
 
@@ -635,6 +667,10 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--fd-params", type=int, default=32)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement of the main line")
+    ap.add_argument("--fd-params-main", type=int, default=8,
+                    help="parameters checked by central differences in the main line's adjoint measurement")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the config-2 (3D, transport) and ensemble measurements of the main line")
     ap.add_argument("--config2", action="store_true",
                     help="3D Richards on Kuhn tetrahedra and a three-species transport chain; own JSON line")
     ap.add_argument("--n3d", type=int, default=96)
@@ -773,11 +809,21 @@ def main():
                           "measure": "max over steps of ||x_gpu - x_oracle|| / ||x_oracle||", **parity}
         line["cpu_baseline"] = cpu_baseline_from(ref, args.n, args.steps)
     if world == 1 and not args.no_adjoint:
-        # second part of the metric: adjoint / forward time of the per-element-parameter run
-        a = adjoint_measure(args.adjoint_n, args.adjoint_steps, args.seed, 0)
+        # second part of the metric: adjoint / forward time of the per-element-parameter run, with a
+        # central-difference check of the gradient on a sample of the parameters
+        a = adjoint_measure(args.adjoint_n, args.adjoint_steps, args.seed, args.fd_params_main)
         line["adjoint"] = {"adjoint_over_forward": a["value"], "forward_s": a["forward_s"],
                            "backward_s": a["backward_s"], "workload": a["config"]["workload"],
-                           "parameters": a["config"]["parameters"]}
+                           "parameters": a["config"]["parameters"], "fd_check": a["fd_check"]}
+    if world == 1 and not args.no_extras:
+        # the other configurations, bounded: 3D Richards and the transport chain in both precisions, and the
+        # batched ensemble against sequential single-domain solves
+        line["config2"] = config2_measure(args.n3d, 3, 2, args.n_transport)
+        e = ensemble_measure(args.domains, 3, 2, args.seed)
+        line["ensemble"] = {"workload": e["config"]["workload"], "domains": e["config"]["domains"],
+                            "nodes_total": e["config"]["nodes_total"], "steps": 3,
+                            "batched": e["batched"], "sequential": e["sequential"],
+                            "batched_value": e["value"], "speedup_vs_sequential": e["speedup_vs_sequential"]}
     print(json.dumps(line))
     barrier(world)
     if world > 1:

@@ -109,3 +109,25 @@ def lognormal_ks_square(n, seed, sigma_lnk=1.0, ks_mean=KS_MEAN):
     Ks = np.exp(np.log(ks_mean) + sigma_lnk * rng.standard_normal(len(tri)))
     top = np.where(pts[:, 1] == 1.0)[0]
     return pts, tri, Ks, top
+
+
+def vg_parameter_ensemble(n_domains, seed, sides=tuple(range(32, 257, 16))):
+    """Independent unit-square Richards domains of uneven size for the batched ensemble: side lengths drawn
+    uniformly from {32, 48, ..., 256}; van Genuchten alpha, n, Ks log-uniform in [1, 10] 1/m, [1.3, 3],
+    [0.01, 1] m/day, m = 1 - 1/n, theta_r .05, theta_s .40; Dirichlet -0.1 on the top edge (NaN = free).
+    Returns [(points, triangles, phi, bc_val, None)] (the Ensemble's domain tuples); meshes of equal side are
+    shared."""
+    rng = np.random.default_rng(seed)
+    lu = lambda lo, hi: float(np.exp(rng.uniform(np.log(lo), np.log(hi))))  # noqa: E731
+    cache, doms = {}, []
+    for _ in range(n_domains):
+        s = int(rng.choice(sides))
+        if s not in cache:
+            pts, tri = structured_triangles(s, 1.0)
+            bc = np.full(len(pts), np.nan)
+            bc[np.abs(pts[:, 1] - 1.0) < 1e-12] = -0.1
+            cache[s] = (pts, tri, bc)
+        pts, tri, bc = cache[s]
+        n = lu(1.3, 3.0)
+        doms.append((pts, tri, (lu(1.0, 10.0), 0.40, 0.05, n, 1.0 - 1.0 / n, lu(0.01, 1.0)), bc, None))
+    return doms

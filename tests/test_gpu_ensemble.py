@@ -81,3 +81,36 @@ def test_ensemble_masks_finished_domains_and_autotunes():
     torch.cuda.synchronize()
     assert torch.equal(h, ens.h_n) and np.array_equal(t, ens.t.cpu().numpy())
     assert out["active"].shape[1] == 3 and out["active"][0].all()
+
+
+def test_ensemble_config3_domains_match_oracle():
+    """The 256-domain ensemble of the benchmark (sides 32 ... 256, log-uniform alpha, n, Ks; 6.26 M nodes) advanced
+    3 steps from dt0 1e-4 with each domain's own dt rule; a sample of domains of the smallest and largest sides is
+    compared with the FP64 oracle (the C restatement, one step at a time with the oracle's own dt rule): the same
+    Picard iterations every step, the same dt, heads within 1e-9 relative."""
+    from oracle import picard as opic, richards2d_c
+    from wspm_b200.ensemble import Ensemble
+    richards2d_c.build()
+    doms = mesh.vg_parameter_ensemble(256, 2024)
+    steps, dt0 = 3, 1e-4
+    ens = Ensemble(doms, dt0=dt0, tmax=1.0, krylov_tol=1e-10, krylov_maxiter=2000, picard_tol=1e-6,
+                   picard_maxiter=100)
+    ens.set_state(-1.0)
+    recs = [ens.step() for _ in range(steps)]
+    sides = np.array([len(d[0]) for d in doms])
+    sample = [int(np.where(sides == 33 * 33)[0][0]), int(np.where(sides == 257 * 257)[0][0]),
+              int(np.where(sides == 257 * 257)[0][1]), int(np.argsort(sides)[len(sides) // 2])]
+    for d in sample:
+        pts, tri, phi, bc, _ = doms[d]
+        top = np.where(~np.isnan(bc))[0]
+        nodes, vals = opic.dirichlet_arrays(len(pts), [(top, -0.1)])
+        h, dt = -np.ones(len(pts)), dt0
+        for s in range(steps):
+            out = richards2d_c.run_vg_fixed_dt(pts, tri, phi, nodes, vals, h, dt, 1, picard_tol=1e-6, picard_max=100,
+                                               cg_tol=1e-10, cg_maxiter=2000)
+            assert int(recs[s]["iterations"][d]) == int(out["picard_its"][0]), (d, s)
+            assert int(recs[s]["status"][d]) == 0
+            h, dt = out["h"], opic.adapt_dt(dt, int(out["picard_its"][0]))
+        got = ens.domain(d).cpu().numpy()
+        assert np.linalg.norm(got - h) / np.linalg.norm(h) <= 1e-9, d
+        assert ens.dt[d].item() == dt, d
