@@ -388,6 +388,14 @@ int wspm_picard_step(void *plan, void *stream);
  * cannot follow conditional graph nodes, and as a fallback.               */
 int wspm_picard_step_host(void *plan, void *stream);
 int wspm_picard_destroy(void *plan);
+/* Structural zeros of a DIA plan: bit k set = diagonal k can hold nonzeros.  At
+ * plan creation the element geometry is scanned once (the stiffness factor
+ * (G^T G)[i][j] of every element pair, computed as the assembly computes it);
+ * a diagonal on which every factor is exactly zero is exactly zero in every
+ * assembly (the lumped mass and the Dirichlet rows touch only the main
+ * diagonal), and the step's sparse kernels skip its loads -- fma(0, x, acc) ==
+ * acc, so no result changes.  -1 for SELL patterns (nothing skipped).       */
+int64_t wspm_picard_dia_live(void *plan);
 
 /* ---- batched ensemble of independent domains -------------------------------
  * No single reference function: the reference solves one domain per

@@ -154,6 +154,87 @@ __device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM],
     }
 }
 
+// Structural zeros of a DIA Richards matrix.  Off the main diagonal the row
+// kernel adds, per element, Kbar detJ (G^T G)[li][j]; the lumped mass and the
+// Dirichlet rows touch only the main diagonal or write zeros.  Bit k of *mask is
+// set when some element puts a nonzero factor (G^T G)[li][j] -- evaluated with
+// exactly the operations of richards_rows_kernel -- on diagonal k, and for the
+// main diagonal; a clear bit is a diagonal that is exactly zero in every
+// assembly, whatever K, C and dt are (e.g. the edges opposite the right angles of
+// a split-square grid whose coordinates are exact binary fractions).  An
+// element pair whose offset is on no diagonal sets every bit (no skipping).
+template <int DIM>
+__global__ void dia_live_kernel(int n_elems, const int32_t *__restrict__ conn, const double *__restrict__ coords,
+                                int nd, const int32_t *__restrict__ diag_off, unsigned long long *mask) {
+    constexpr int NV = DIM + 1;
+    __shared__ unsigned long long s_mask;
+    if (threadIdx.x == 0) s_mask = 0ull;
+    __syncthreads();
+    unsigned long long m = 0ull;
+    if (blockIdx.x == 0 && threadIdx.x < nd && diag_off[threadIdx.x] == 0) m |= 1ull << threadIdx.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_elems; e += gridDim.x * blockDim.x) {
+        int nodes[NV];
+        double X[NV][DIM];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            nodes[j] = conn[(int64_t)NV * e + j];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) X[j][d] = coords[(int64_t)DIM * nodes[j] + d];
+        }
+        double G[DIM][NV], detJ;
+        p1_geometry_xyz<DIM>(X, G, detJ);
+#pragma unroll
+        for (int li = 0; li < NV; ++li) {
+            double gli[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                double g = G[d][0];
+#pragma unroll
+                for (int j = 1; j < NV; ++j) g = li == j ? G[d][j] : g;
+                gli[d] = g;
+            }
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                if (j == li) continue;
+                double gg = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) gg = fma(gli[d], G[d][j], gg);
+                if (gg == 0.0) continue;
+                const int off = nodes[j] - nodes[li];
+                int k = 0;
+                while (k < nd && diag_off[k] != off) ++k;
+                m |= k < nd ? 1ull << k : ~0ull;
+            }
+        }
+    }
+    if (m) atomicOr(&s_mask, m);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_mask) atomicOr(mask, s_mask);
+}
+
+// Live-diagonal mask of a DIA Richards pattern (all ones for SELL patterns or on
+// any failure, which only disables the skipping).  `word`: one device word of
+// scratch; synchronous (plan creation only).
+unsigned long long richards_dia_live_mask(const wspm_mesh *mesh, const wspm_pattern *pat,
+                                          unsigned long long *word) {
+    const unsigned long long all = ~0ull;
+    if (!mesh || !pat || pat->n_diags <= 0 || pat->n_diags > 63 || !pat->diag_offsets || !word) return all;
+    if (mesh->dim != 2 && mesh->dim != 3) return all;
+    if (cudaMemset(word, 0, sizeof(unsigned long long)) != cudaSuccess) return all;
+    const int blocks = (int)((mesh->n_elems + 255) / 256 < 148 * 8 ? (mesh->n_elems + 255) / 256 : 148 * 8);
+    if (mesh->dim == 2)
+        dia_live_kernel<2><<<blocks > 0 ? blocks : 1, 256>>>(mesh->n_elems, mesh->conn, mesh->coords, pat->n_diags,
+                                                             pat->diag_offsets, word);
+    else
+        dia_live_kernel<3><<<blocks > 0 ? blocks : 1, 256>>>(mesh->n_elems, mesh->conn, mesh->coords, pat->n_diags,
+                                                             pat->diag_offsets, word);
+    unsigned long long m = 0ull;
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpy(&m, word, sizeof(m), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return all;
+    return m;
+}
+
 // Incidence-ordered per-element values: slot o of the incidence layout gets
 // elem[inc_elem[o]]; padding slots get kIncPad, a NaN bit pattern that the
 // row kernel tests for (so it needs no element id per slot).

@@ -138,7 +138,14 @@ struct Sell {
     int n_diags;
     const int32_t *diag_off;
     int64_t ld;
+    // DIA: bit k clear = diagonal k holds exact zeros in every row (a structural
+    // zero of the discretisation, e.g. the edge opposite a right angle of P1
+    // triangles); the sparse kernels then skip its loads.  fma(0, x, acc) == acc
+    // for finite x, so skipping changes no result bit.  All ones by default.
+    unsigned long long live;
 };
+
+__host__ __device__ __forceinline__ bool dia_live(const Sell &A, int k) { return (A.live >> k) & 1ull; }
 
 __device__ __forceinline__ int64_t entry_pos(const Sell &A, int i, int k) {
     return A.n_diags > 0 ? (int64_t)k * A.ld + i : __ldg(A.slice_ptr + (i >> 5)) + (int64_t)kSlice * k + (i & 31);
@@ -168,7 +175,7 @@ __device__ __forceinline__ T sell_row_dot(const Sell &A, const T *__restrict__ v
 #pragma unroll
                 for (int g = 0; g < G; ++g) {
                     const int k = k0 + g;
-                    if (k < nd) {
+                    if (k < nd && dia_live(A, k)) {
                         v[g] = __ldg(vals + (int64_t)k * A.ld + i);
                         const int cc = i + __ldg(A.diag_off + k);
                         c[g] = cc < 0 ? 0 : (cc > last ? last : cc);
@@ -176,10 +183,11 @@ __device__ __forceinline__ T sell_row_dot(const Sell &A, const T *__restrict__ v
                 }
 #pragma unroll
                 for (int g = 0; g < G; ++g)
-                    if (k0 + g < nd) acc = fma(v[g], xf(c[g]), acc);
+                    if (k0 + g < nd && dia_live(A, k0 + g)) acc = fma(v[g], xf(c[g]), acc);
             }
         } else {
             for (int k = 0; k < nd; ++k) {
+                if (!dia_live(A, k)) continue;
                 int cc = i + __ldg(A.diag_off + k);
                 cc = cc < 0 ? 0 : (cc > last ? last : cc);
                 acc = fma(__ldg(vals + (int64_t)k * A.ld + i), xf(cc), acc);

@@ -402,8 +402,13 @@ template <> struct Vec16<double> {
 // loads: inside a phase no block writes z, and the acquire that ends the
 // preceding wait (flag or barrier) followed by the block barrier orders every
 // earlier z store before these loads.
+//
+// The resident kernels keep only the diagonals that can hold nonzeros: entry k
+// of their lists has column offset s_off[k] and its values at s_vo[k] + row
+// (s_vo[k] = (index of the diagonal) * ld).  A skipped diagonal is exactly zero,
+// and fma(0, x, acc) == acc, so the products are those of the full row.
 template <typename T, int MW>
-__device__ __forceinline__ T dia_row_z(const T *__restrict__ vals, int64_t ld, int i, int last, int nd,
+__device__ __forceinline__ T dia_row_z(const T *__restrict__ vals, const int64_t *s_vo, int i, int last, int nd,
                                        const int *s_off, const T *z) {
     T acc = T(0);
 #pragma unroll
@@ -411,7 +416,7 @@ __device__ __forceinline__ T dia_row_z(const T *__restrict__ vals, int64_t ld, i
         if (k < nd) {
             int c = i + s_off[k];
             c = c < 0 ? 0 : (c > last ? last : c);
-            acc = fma(__ldg(vals + (int64_t)k * ld + i), z[c], acc);
+            acc = fma(__ldg(vals + s_vo[k] + i), z[c], acc);
         }
     }
     return acc;
@@ -421,7 +426,7 @@ __device__ __forceinline__ T dia_row_z(const T *__restrict__ vals, int64_t ld, i
 // per diagonal, issued G diagonals at a time before their first use, then the
 // gathers diagonal by diagonal.  Each row accumulates in diagonal order.
 template <typename T, int MW>
-__device__ __forceinline__ void dia_group_z(const T *__restrict__ vals, int64_t ld, int i, int last, int nd,
+__device__ __forceinline__ void dia_group_z(const T *__restrict__ vals, const int64_t *s_vo, int i, int last, int nd,
                                             const int *s_off, const T *z, T (&w)[Vec16<T>::N]) {
     using VT = Vec16<T>;
     constexpr int N = VT::N;
@@ -434,7 +439,7 @@ __device__ __forceinline__ void dia_group_z(const T *__restrict__ vals, int64_t 
         typename VT::V vv[G];
 #pragma unroll
         for (int g = 0; g < G; ++g)
-            if (k0 + g < nd) vv[g] = __ldg(reinterpret_cast<const typename VT::V *>(vals + (int64_t)(k0 + g) * ld + i));
+            if (k0 + g < nd) vv[g] = __ldg(reinterpret_cast<const typename VT::V *>(vals + s_vo[k0 + g] + i));
 #pragma unroll
         for (int g = 0; g < G; ++g) {
             if (k0 + g < nd) {
@@ -474,7 +479,7 @@ __device__ __forceinline__ void rcg_spmv_rows(int l0, int l1, T &acc, const Sell
 // Returns false when that wait gave up.
 template <typename T, int MW>
 __device__ __forceinline__ bool rcg_spmv_dia(int nl, int lo_i, int hi_i, T &acc, const T *__restrict__ vals,
-                                             int64_t ld, int r0, int last, int nd, const int *s_off, const T *z,
+                                             const int64_t *s_vo, int r0, int last, int nd, const int *s_off, const T *z,
                                              T *wbase, const unsigned int *zflag, int nbr_lo, int nbr_hi,
                                              unsigned int epoch, bool poll, GridBarrier *bar) {
     using VT = Vec16<T>;
@@ -498,7 +503,7 @@ __device__ __forceinline__ bool rcg_spmv_dia(int nl, int lo_i, int hi_i, T &acc,
         const int l = g * N, i = r0 + l;
         if (l + N <= nl) {
             T w[N];
-            dia_group_z<T, MW>(vals, ld, i, last, nd, s_off, z, w);
+            dia_group_z<T, MW>(vals, s_vo, i, last, nd, s_off, z, w);
             *reinterpret_cast<typename VT::V *>(wbase + l) = VT::join(w);
             T zo[N];
             VT::split(*reinterpret_cast<const typename VT::V *>(z + i), zo);
@@ -506,7 +511,7 @@ __device__ __forceinline__ bool rcg_spmv_dia(int nl, int lo_i, int hi_i, T &acc,
             for (int q = 0; q < N; ++q) acc = fma(w[q], zo[q], acc);
         } else {
             for (int q = 0; l + q < nl; ++q) {
-                const T wi = dia_row_z<T, MW>(vals, ld, i + q, last, nd, s_off, z);
+                const T wi = dia_row_z<T, MW>(vals, s_vo, i + q, last, nd, s_off, z);
                 wbase[l + q] = wi;
                 acc = fma(wi, z[i + q], acc);
             }
@@ -547,6 +552,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     constexpr int N = VT::N;
     extern __shared__ __align__(16) unsigned char rcg_smem[];
     __shared__ int s_off[MW > 0 ? MW : 1];
+    __shared__ int64_t s_vo[MW > 0 ? MW : 1];
     T *const sm = reinterpret_cast<T *>(rcg_smem);
     if (resident_skip(a.skip, a.st)) return;
     const unsigned long long t_entry = (blockIdx.x == 0 && threadIdx.x == 0) ? global_ns() : 0ull;
@@ -577,14 +583,19 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
 #define RCG_G(v) ((v) == kVR ? gvR : (v) == kVP ? gvP : (v) == kVS ? gvS : gvW)
 #define RCG_P(v, l) ((v) < NS ? (sm + (v) * chunk + (l)) : (RCG_G(v) + (l)))
 #define RCG(v, l) (*RCG_P(v, l))
-    const int nd = A.n_diags;
-    const bool dia = MW > 0 && nd > 0 && nd <= MW;
+    const bool dia = MW > 0 && A.n_diags > 0 && A.n_diags <= MW;
+    int nd = 0;                // diagonals that can hold nonzeros (A.live)
     int lo_i = 0, hi_i = 0, nbr_lo = 0, nbr_hi = nb - 1;
     if (dia) {
         int mn = 0, mx = 0;
-        for (int k = 0; k < nd; ++k) {
+        for (int k = 0; k < A.n_diags; ++k) {
+            if (!dia_live(A, k)) continue;
             const int o = __ldg(A.diag_off + k);
-            if (threadIdx.x == 0) s_off[k] = o;
+            if (threadIdx.x == 0) {
+                s_off[nd] = o;
+                s_vo[nd] = (int64_t)k * A.ld;
+            }
+            ++nd;
             mn = min(mn, o);
             mx = max(mx, o);
         }
@@ -597,7 +608,6 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
         if (nl == 0) { nbr_lo = 1; nbr_hi = 0; }
     }
     const int last = n - 1;
-    const int64_t ld = A.ld;
     T *const wbase = kVW < NS ? sm + kVW * chunk : gvW;
     // ---- init: x, M into place; r = b - A x0 ; z = M r.  On DIA patterns A x0
     // comes from the same row-group SpMV as the iterations (into w, which is
@@ -610,7 +620,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
         if (ax_dia) {
             __syncthreads();       // s_off (written by thread 0 above) is read by every thread
             T unused = T(0);
-            rcg_spmv_dia<T, (MW > 0 ? MW : 1)>(nl, lo_i, hi_i, unused, vals, ld, r0, last, nd, s_off, xg, wbase,
+            rcg_spmv_dia<T, (MW > 0 ? MW : 1)>(nl, lo_i, hi_i, unused, vals, s_vo, r0, last, nd, s_off, xg, wbase,
                                                 zflag, nbr_lo, nbr_hi, 0u, false, bar);
             __syncthreads();
         }
@@ -679,7 +689,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) cg_resident_kernel(RcgArgs<T> a)
     if (!isfinite(rs)) { done = true; status = WSPM_NAN; }
     unsigned int red = 0;      // counting barriers passed
 #define RCG_SPMV_DIA(acc, epoch, poll)                                                                       \
-    rcg_spmv_dia<T, (MW > 0 ? MW : 1)>(nl, lo_i, hi_i, (acc), vals, ld, r0, last, nd, s_off, z, wbase, zflag, \
+    rcg_spmv_dia<T, (MW > 0 ? MW : 1)>(nl, lo_i, hi_i, (acc), vals, s_vo, r0, last, nd, s_off, z, wbase, zflag, \
                                        nbr_lo, nbr_hi, (epoch), (poll), bar)
     // w0 = A z0 and d0 = (w0, z0) when iterating
     if (!done && ok) {
@@ -1017,8 +1027,9 @@ __device__ __forceinline__ void warp_partials(const T *partials, int nb, T (&out
 // first, the wait for the neighbours' flags before the first round with a
 // halo group).  Returns false when that wait gave up.
 template <typename T, int MW>
-__device__ __forceinline__ bool pcg_spmv_dia(int nl, int lo_i, int hi_i, const T *__restrict__ vals, int64_t ld,
-                                             int r0, int last, int nd, const int *s_off, const T *src, T *dst,
+__device__ __forceinline__ bool pcg_spmv_dia(int nl, int lo_i, int hi_i, const T *__restrict__ vals,
+                                             const int64_t *s_vo, int r0, int last, int nd, const int *s_off,
+                                             const T *src, T *dst,
                                              const unsigned int *flag, int nbr_lo, int nbr_hi, unsigned int epoch,
                                              bool poll, GridBarrier *bar, int tid, int nthr, bool named) {
     using VT = Vec16<T>;
@@ -1041,10 +1052,10 @@ __device__ __forceinline__ bool pcg_spmv_dia(int nl, int lo_i, int hi_i, const T
         const int l = g * N, i = r0 + l;
         if (l + N <= nl) {
             T w[N];
-            dia_group_z<T, MW>(vals, ld, i, last, nd, s_off, src, w);
+            dia_group_z<T, MW>(vals, s_vo, i, last, nd, s_off, src, w);
             *reinterpret_cast<typename VT::V *>(dst + l) = VT::join(w);
         } else {
-            for (int q = 0; l + q < nl; ++q) dst[l + q] = dia_row_z<T, MW>(vals, ld, i + q, last, nd, s_off, src);
+            for (int q = 0; l + q < nl; ++q) dst[l + q] = dia_row_z<T, MW>(vals, s_vo, i + q, last, nd, s_off, src);
         }
     }
     if (m_wait >= rounds && poll && !wait_flags_group(flag, nbr_lo, nbr_hi, epoch, bar, tid, nthr, named))
@@ -1061,6 +1072,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
     constexpr int N = VT::N;
     extern __shared__ __align__(16) unsigned char rcg_smem[];
     __shared__ int s_off[MW];
+    __shared__ int64_t s_vo[MW];
     __shared__ T s_scal[3];
     __shared__ int s_ok;
     T *const sm = reinterpret_cast<T *>(rcg_smem);
@@ -1090,13 +1102,17 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
     T *const vR = sm + kPR * chunk, *const vW = sm + kPW * chunk, *const vS = sm + kPS * chunk;
     T *const vP = sm + kPP * chunk, *const vZ = sm + kPZ * chunk, *const vN = sm + kPN * chunk;
     T *const vX = XS ? sm + kPX * chunk : xg + r0;   // x: on chip when it fits, else the caller's array
-    const int nd = a.A.n_diags;
-    const int64_t ld = a.A.ld;
     const int last = n - 1;
+    int nd = 0;                // diagonals that can hold nonzeros (A.live)
     int mn = 0, mx = 0;
-    for (int k = 0; k < nd; ++k) {
+    for (int k = 0; k < a.A.n_diags; ++k) {
+        if (!dia_live(a.A, k)) continue;
         const int o = __ldg(a.A.diag_off + k);
-        if (tid == 0) s_off[k] = o;
+        if (tid == 0) {
+            s_off[nd] = o;
+            s_vo[nd] = (int64_t)k * a.A.ld;
+        }
+        ++nd;
         mn = min(mn, o);
         mx = max(mx, o);
     }
@@ -1144,7 +1160,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
                 const int i = r0 + l;
                 const T bi = a.b64 ? (T)a.b64[i] : a.b[i];
                 if (XS) vX[l] = xg[i];
-                const T ri = bi - dia_row_z<T, MW>(vals, ld, i, last, nd, s_off, xg);
+                const T ri = bi - dia_row_z<T, MW>(vals, s_vo, i, last, nd, s_off, xg);
                 const T di = dg ? dg[i] : T(1);
                 vR[l] = ri;
                 vS[l] = T(0);
@@ -1177,7 +1193,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
     };
     // w0 = A u0 (the grid barrier published u0), then m0 = M w0 and reduction 0
     if (ok) {
-        ok = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, ld, r0, last, nd, s_off, ex0, vW, flag, nbr_lo, nbr_hi, 0u,
+        ok = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, s_vo, r0, last, nd, s_off, ex0, vW, flag, nbr_lo, nbr_hi, 0u,
                                  false, bar, tid, TB, false);
         __syncthreads();
         T v[3] = {T(0), T(0), T(0)};
@@ -1214,7 +1230,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
         const unsigned int target = (unsigned)(k + 1) * (unsigned)nb;
         if (WS) {
             if (!red_warp) {
-                const bool o = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, ld, r0, last, nd, s_off, msrc, vN, flag,
+                const bool o = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, s_vo, r0, last, nd, s_off, msrc, vN, flag,
                                                    nbr_lo, nbr_hi, (unsigned)(k + 2), true, bar, tid, nthr, true);
                 if (tid == 0) s_ok = o ? 1 : 0;
             } else {
@@ -1235,7 +1251,7 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
             ok = s_ok != 0 && (*(volatile int *)&bar->error) == 0;
             __syncthreads();       // every thread has read s_ok before it is written again
         } else {
-            ok = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, ld, r0, last, nd, s_off, msrc, vN, flag, nbr_lo, nbr_hi,
+            ok = pcg_spmv_dia<T, MW>(nl, lo_i, hi_i, vals, s_vo, r0, last, nd, s_off, msrc, vN, flag, nbr_lo, nbr_hi,
                                      (unsigned)(k + 2), true, bar, tid, TB, false);
             if (tid == 0) s_ok = count_wait(bar, target) ? 1 : 0;
             __syncthreads();

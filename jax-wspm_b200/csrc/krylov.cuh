@@ -10,6 +10,7 @@ inline Sell make_sell(const wspm_pattern *p) {
     s.n_rows = p->n_rows; s.n_slices = p->n_slices; s.max_width = p->max_width;
     s.slice_ptr = p->slice_ptr; s.slice_width = p->slice_width; s.cols = p->cols;
     s.n_diags = p->n_diags; s.diag_off = p->diag_offsets; s.ld = (int64_t)p->n_slices * kSlice;
+    s.live = ~0ull;
     return s;
 }
 

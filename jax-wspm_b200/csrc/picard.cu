@@ -35,6 +35,7 @@ int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *p
                                     float *vals32, double *rhs, double *dinv, const RefineStart *res,
                                     cudaStream_t st);
 int richards_assembly_blocks(const wspm_mesh *mesh, const wspm_pattern *pat);
+unsigned long long richards_dia_live_mask(const wspm_mesh *mesh, const wspm_pattern *pat, unsigned long long *word);
 int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st);
 
 struct PicardState {
@@ -311,7 +312,15 @@ struct PicardPlan {
     double *r64 = nullptr;
     float *x32 = nullptr, *dinv32 = nullptr;
     double *Ks_inc = nullptr;   // Ks_elem in incidence order (caller's buffer), refreshed at every step start
+    unsigned long long live = ~0ull;   // DIA diagonals that can hold nonzeros (structural zeros skipped)
 };
+
+// The plan's matrix descriptor: the pattern with its structural-zero diagonals marked.
+static Sell plan_sell(const PicardPlan *P) {
+    Sell A = make_sell(&P->pat);
+    A.live = P->live;
+    return A;
+}
 
 // The mixed path starts each refinement loop inside the assembly launch (r = b - A h_m
 // from the rows just built) when nothing is added to the rows after it (no Neumann or
@@ -349,7 +358,7 @@ int64_t picard_workspace_doubles(int n, int mixed, int solver, int restart) {
 static int build_picard_graph(PicardPlan *P) {
     const wspm_picard_desc &d = P->d;
     const int n = P->mesh.n_nodes;
-    const Sell A = make_sell(&P->pat);
+    const Sell A = plan_sell(P);
     const int nb = reduction_blocks(n);
     const double *dinv = d.precond == WSPM_PRECOND_JACOBI ? d.dinv : nullptr;
     cudaStream_t cs;
@@ -464,7 +473,7 @@ static int read_flag(const int *dev_word, cudaStream_t st, int *out, int *pinned
 static int picard_step_host(PicardPlan *P, cudaStream_t st) {
     const wspm_picard_desc &d = P->d;
     const int n = P->mesh.n_nodes;
-    const Sell A = make_sell(&P->pat);
+    const Sell A = plan_sell(P);
     const int nb = reduction_blocks(n);
     const double *dinv = d.precond == WSPM_PRECOND_JACOBI ? d.dinv : nullptr;
     const cudaGraphConditionalHandle none = cudaGraphConditionalHandle();
@@ -627,6 +636,9 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
         P->cg64 = carve_cg<double>(p, n, &used); p += used;
     }
     P->Ks_inc = d.Ks_elem ? d.Ks_inc : nullptr;
+    // structural zeros of the DIA layout, found once from the geometry (the first
+    // partial-sum slot of the workspace serves as the scratch word)
+    P->live = richards_dia_live_mask(&P->mesh, &P->pat, reinterpret_cast<unsigned long long *>(P->partials));
     int rc = build_picard_graph(P);
     if (rc != WSPM_OK) {
         delete P;
@@ -634,6 +646,12 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     }
     *plan_out = P;
     return WSPM_OK;
+}
+
+extern "C" int64_t wspm_picard_dia_live(void *plan) {
+    if (!plan) return -1;
+    const PicardPlan *P = (const PicardPlan *)plan;
+    return P->pat.n_diags > 0 ? (int64_t)(P->live & ((1ull << P->pat.n_diags) - 1ull)) : -1;
 }
 
 extern "C" int wspm_picard_step(void *plan, void *stream) {

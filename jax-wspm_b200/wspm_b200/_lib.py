@@ -147,6 +147,7 @@ _SIGS = {
     "wspm_picard_step": (c_int32, [c_void_p, c_void_p]),
     "wspm_picard_step_host": (c_int32, [c_void_p, c_void_p]),
     "wspm_picard_destroy": (c_int32, [c_void_p]),
+    "wspm_picard_dia_live": (c_int64, [c_void_p]),
     "wspm_pattern_build": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_int64, c_int32,
                                      P(P(WspmPatternHost))]),
     "wspm_pattern_free": (None, [P(WspmPatternHost)]),

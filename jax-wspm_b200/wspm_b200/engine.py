@@ -126,6 +126,13 @@ class PicardEngine:
                 pass
             self.plan = None
 
+    @property
+    def live_diagonals(self):
+        """DIA plans: bit mask of the diagonals that can hold nonzeros (the others are structural zeros whose
+        loads the step skips); None for SELL patterns."""
+        m = int(lib.wspm_picard_dia_live(self.plan))
+        return None if m < 0 else m
+
     # -- device-side step -----------------------------------------------------
     def set_state(self, h):
         self.h_n.copy_(torch.as_tensor(h, dtype=torch.float64).to(self.dm.device).reshape(-1))

@@ -516,3 +516,40 @@ def test_host_loop_mode_matches_device_loop(solver, precond, mixed):
     np.testing.assert_array_equal(a["iterations"], b["iterations"])
     np.testing.assert_array_equal(a["krylov_iterations"], b["krylov_iterations"])
     np.testing.assert_array_equal(a["pressure_head"], b["pressure_head"])
+
+
+@pytest.mark.parametrize("kind,n", [("tri", 64), ("tri", 50), ("tet", 8)])
+def test_structural_zero_diagonals_are_exactly_zero(kind, n):
+    """A Picard plan on a DIA pattern marks the diagonals whose element stiffness factors are all exactly zero; the
+    step's CG and refinement kernels skip them.  Every diagonal it marks must hold exact zeros after assembly (at
+    the last Picard iterate, both precisions).  On the split-square grid with exact binary coordinates (n = 64) the
+    two diagonals of the edges opposite the right angles (offsets +-(n+2)) are such zeros."""
+    from wspm_b200.device import DeviceMesh, merge_dirichlet
+    from wspm_b200.engine import PicardEngine
+    if kind == "tri":
+        pts, el = mesh.structured_triangles(n, 1.0)
+        top = np.where(pts[:, 1] == 1.0)[0]
+    else:
+        pts, el = mesh.kuhn_tetrahedra(n, 1.0)
+        top = np.where(np.abs(pts[:, 2] - 1.0) < 1e-12)[0]
+    dm = DeviceMesh(pts, el)
+    offs = dm.pattern.diag_offsets
+    assert dm.pattern.n_diags > 0
+    bc = merge_dirichlet(len(pts), [(top, -0.1)])
+    for mixed in (False, True):
+        eng = PicardEngine(dm, "vg", opic.VG_UNIT_PHI, bc_val=bc, solver="cg", precond="jacobi", krylov_tol=1e-8,
+                           krylov_maxiter=5000, mixed=mixed)
+        live = eng.live_diagonals
+        res = eng.run(-np.ones(len(pts)), 1e-4, 1e-3, fixed_dt=True, max_steps=2)
+        assert np.all(res["status"] == 0)
+        ld = 32 * dm.pattern.n_slices
+        vals = host(eng.vals).reshape(len(offs), ld)
+        for k, o in enumerate(offs):
+            if not (live >> k) & 1:
+                assert o != 0 and np.all(vals[k] == 0.0), (k, o)
+        if mixed:
+            v32 = host(eng.vals32).reshape(len(offs), ld)
+            assert all(np.all(v32[k] == 0.0) for k in range(len(offs)) if not (live >> k) & 1)
+        if kind == "tri" and n == 64:
+            dead = {int(o) for k, o in enumerate(offs) if not (live >> k) & 1}
+            assert dead == {n + 2, -(n + 2)}, dead
