@@ -732,8 +732,11 @@ def main():
     t_it64 = r64["krylov_kernel_s"] / max(1, r64["krylov_its"])
     # L2 bytes one iteration must move: pipelined FP32 = the matrix (nd diagonals of ld rows) + 1/diag read +
     # m = M w written and read by the SpMV; FP64 = the matrix + z written and read, x read and written, 1/diag
-    l2_32 = nd * ld * 4 + 3 * N * 4
-    l2_64 = nd * ld * 8 + 5 * N * 8
+    # (only the diagonals the plan reads: structural-zero diagonals are skipped)
+    live = engmx.live_diagonals
+    nd_read = bin(live).count("1") if live is not None else nd
+    l2_32 = nd_read * ld * 4 + 3 * N * 4
+    l2_64 = nd_read * ld * 8 + 5 * N * 8
     l2_peak32 = l2_read_bandwidth(nd * ld * 4)
     l2_peak64 = l2_read_bandwidth(nd * ld * 8)
     b32 = algorithmic_bytes_cg(N, nnz, 4)
@@ -784,6 +787,7 @@ def main():
                      "peak_kind": "measured in this run: wspm_read_probe, 16-byte L1-bypassing reads over a "
                                   "buffer the size of the FP32 matrix, CUDA events",
                      "l2_bytes_per_iteration": l2_32, "seconds_per_iteration": t_it32,
+                     "diagonals_read": f"{nd_read} of {nd} (the others are structural zeros, skipped)",
                      "timing": "the kernel's own %globaltimer entry-to-exit durations summed over the timed "
                                "steps / inner iterations",
                      "traffic": load_traffic("cg_iteration_f32"),
