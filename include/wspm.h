@@ -444,6 +444,18 @@ int64_t wspm_ensemble_workspace_doubles(int32_t n_rows, int64_t nnz_padded);
  * (one thread-block cluster) share each domain.                                */
 int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
                        int32_t block_threads, void *stream);
+/* The time loop of the ensemble on the device (RichardsSolver.solve's loop,
+ * richards_solver_v2.py:272-352, for every domain at once): one CUDA graph
+ * whose WHILE node launches wspm_ensemble_step's kernel until every domain has
+ * reached tmax or max_steps steps ran; no host round trip between steps.
+ * Scratch/outputs (device): active[n_domains] (int32, domains below tmax
+ * after the last step), its_total[n_domains] (int64, Picard iterations summed
+ * over the steps each domain took), run[2] (int32: steps launched, domains
+ * still active).  The graph is captured on every call and released when the
+ * launch completes; `stream` orders it like any other call.                 */
+int wspm_ensemble_run(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
+                      int32_t block_threads, int32_t max_steps, int32_t *active, int64_t *its_total,
+                      int32_t *run, void *stream);
 
 /* ---- per-element soil parameters and the discrete adjoint --------------------
  * No reference counterpart: the reference evaluates one van Genuchten

@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "soil.cuh"
 #include "krylov.cuh"
+#include "graph.cuh"
 
 namespace wspm {
 
@@ -363,8 +364,106 @@ extern "C" int64_t wspm_ensemble_workspace_doubles(int32_t n_rows, int64_t nnz_p
     return 12 * (int64_t)n_rows + nnz_padded + 64;
 }
 
+static int ensemble_enqueue(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
+                            int32_t block_threads, cudaStream_t st);
+
 extern "C" int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
                                   int32_t block_threads, void *stream) {
+    return ensemble_enqueue(mesh, pat, ens, block_threads, (cudaStream_t)stream);
+}
+
+// ---- several steps on the device: WHILE(any domain below tmax && steps < max){ step; tail }
+namespace {
+
+// active[d] = t[d] < tmax; its_total = 0; run[0] = steps = 0, run[1] = active domains.
+__global__ void ens_run_init_kernel(int D, const double *t, double tmax, int32_t *active, int64_t *its_total,
+                                    int32_t *run, int max_steps, cudaGraphConditionalHandle cond) {
+    __shared__ int s_n;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    int n = 0;
+    for (int d = threadIdx.x; d < D; d += blockDim.x) {
+        const int a = t[d] < tmax;
+        active[d] = a;
+        its_total[d] = 0;
+        n += a;
+    }
+    atomicAdd(&s_n, n);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        run[0] = 0;
+        run[1] = s_n;
+        cudaGraphSetConditional(cond, (s_n > 0 && max_steps > 0) ? 1u : 0u);
+    }
+}
+
+// After a step: the Picard iterations of the domains that were active are added up, the
+// step is counted, the active set is recomputed and the loop continues while a domain is
+// below tmax and fewer than max_steps steps ran.
+__global__ void ens_run_tail_kernel(int D, const double *t, double tmax, const int32_t *its, int32_t *active,
+                                    int64_t *its_total, int32_t *run, int max_steps,
+                                    cudaGraphConditionalHandle cond) {
+    __shared__ int s_n;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    int n = 0;
+    for (int d = threadIdx.x; d < D; d += blockDim.x) {
+        if (active[d]) its_total[d] += its[d];
+        const int a = t[d] < tmax;
+        active[d] = a;
+        n += a;
+    }
+    atomicAdd(&s_n, n);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int steps = run[0] + 1;
+        run[0] = steps;
+        run[1] = s_n;
+        cudaGraphSetConditional(cond, (s_n > 0 && steps < max_steps) ? 1u : 0u);
+    }
+}
+
+}  // namespace
+
+extern "C" int wspm_ensemble_run(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
+                                 int32_t block_threads, int32_t max_steps, int32_t *active, int64_t *its_total,
+                                 int32_t *run, void *stream) {
+    if (!ens || !active || !its_total || !run || max_steps < 0) return WSPM_BAD_ARG;
+    cudaStream_t cs;
+    WSPM_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) { cudaStreamDestroy(cs); return WSPM_CUDA_ERROR; }
+    int rc = WSPM_OK;
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+        cudaGraphConditionalHandle h;
+        e = make_cond_handle(cs, &h);
+        const int D = ens->n_domains;
+        if (e == cudaSuccess) {
+            ens_run_init_kernel<<<1, 256, 0, cs>>>(D, ens->t, ens->tmax, active, its_total, run, max_steps, h);
+            e = capture_while(cs, h, [&](cudaStream_t bs) {
+                rc = ensemble_enqueue(mesh, pat, ens, block_threads, bs);
+                ens_run_tail_kernel<<<1, 256, 0, bs>>>(D, ens->t, ens->tmax, ens->its, active, its_total, run,
+                                                       max_steps, h);
+            });
+        }
+        cudaGraph_t out = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(cs, &out);
+        if (e == cudaSuccess) e = e2;
+    }
+    cudaStreamDestroy(cs);
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess && rc == WSPM_OK) e = cudaGraphInstantiate(&exec, g, 0);
+    if (e == cudaSuccess && rc == WSPM_OK) e = cudaGraphLaunch(exec, (cudaStream_t)stream);
+    // the executable graph is released once the launch completes (freed asynchronously)
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(g);
+    if (rc != WSPM_OK) return rc;
+    return e == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+}
+
+static int ensemble_enqueue(const wspm_mesh *mesh, const wspm_pattern *pat, const wspm_ensemble *ens,
+                            int32_t block_threads, cudaStream_t st) {
     if (!mesh || !pat || !ens || mesh->dim != 2 || !ens->node_off || !ens->order || !ens->phi || !ens->h_n ||
         !ens->work || !ens->dt || !ens->t || !ens->its || !ens->kits || !ens->status || !ens->err || !ens->queue ||
         ens->n_domains <= 0 || ens->nq <= 0 || ens->nq > 16 || pat->n_rows != mesh->n_nodes)
@@ -377,7 +476,6 @@ extern "C" int wspm_ensemble_step(const wspm_mesh *mesh, const wspm_pattern *pat
     if (ens->cluster_size != 0 && ens->cluster_size != 1 && ens->cluster_size != 2 && ens->cluster_size != 4 &&
         ens->cluster_size != 8 && ens->cluster_size != 16)
         return WSPM_BAD_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
     EnsArgs a;
     a.A = make_sell(pat);
     a.diag_pos = pat->diag_pos;

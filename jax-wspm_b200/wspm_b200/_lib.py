@@ -111,6 +111,8 @@ _SIGS = {
                                        P(c_double), c_int32, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
                                        c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_ensemble_step": (c_int32, [P(WspmMesh), P(WspmPattern), P(WspmEnsemble), c_int32, c_void_p]),
+    "wspm_ensemble_run": (c_int32, [P(WspmMesh), P(WspmPattern), P(WspmEnsemble), c_int32, c_int32, c_void_p,
+                                    c_void_p, c_void_p, c_void_p]),
     "wspm_soil_van_genuchten": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_soil_exponential": (c_int32, [c_void_p, c_int64, P(c_double), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_assemble_richards": (c_int32, [P(WspmMesh), P(WspmPattern), c_void_p, c_void_p, c_void_p, c_void_p,

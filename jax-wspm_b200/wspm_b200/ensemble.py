@@ -11,7 +11,9 @@ Picard loop with its own soil parameters, Dirichlet values and dt, and adapts
 that dt.  Domains that reached ``tmax`` are masked out of later launches.
 
 ``autotune()`` times one step at each (CTA size, cluster size) the kernel
-supports on a copy of the state and keeps the fastest.
+supports on a copy of the state and keeps the fastest.  ``run_device()`` runs
+the time loop itself on the device: one CUDA graph whose WHILE node repeats the
+step launch until every domain reached ``tmax`` (or a step cap).
 """
 import ctypes
 import time
@@ -150,6 +152,23 @@ class Ensemble:
         check("ensemble_step", lib.wspm_ensemble_step(ctypes.byref(self.dm.c_mesh), ctypes.byref(self.dm.c_pat),
                                                        ctypes.byref(self.c), int(self.block_threads),
                                                        ctypes.c_void_p(st.cuda_stream)))
+
+    def run_device(self, max_steps, stream=None):
+        """Up to ``max_steps`` steps of every active domain in one CUDA graph (``wspm_ensemble_run``: the time
+        loop runs on the device, no host round trip between steps).  Returns device tensors (Picard iterations
+        summed per domain, int32[2] = steps launched, domains still active); nothing is synchronised."""
+        st = stream if stream is not None else torch.cuda.current_stream()
+        dev = self.h_n.device
+        if not hasattr(self, "_run_bufs"):
+            self._run_bufs = (torch.zeros(self.n_domains, dtype=torch.int32, device=dev),
+                              torch.zeros(self.n_domains, dtype=torch.int64, device=dev),
+                              torch.zeros(2, dtype=torch.int32, device=dev))
+        act, its, run = self._run_bufs
+        self.c.cluster_size = int(self.cluster_size)
+        check("ensemble_run", lib.wspm_ensemble_run(ctypes.byref(self.dm.c_mesh), ctypes.byref(self.dm.c_pat),
+                                                     ctypes.byref(self.c), int(self.block_threads), int(max_steps),
+                                                     dptr(act), dptr(its), dptr(run), ctypes.c_void_p(st.cuda_stream)))
+        return its, run
 
     def active(self):
         return int((self.t < self.tmax).sum().item())

@@ -114,3 +114,30 @@ def test_ensemble_config3_domains_match_oracle():
         got = ens.domain(d).cpu().numpy()
         assert np.linalg.norm(got - h) / np.linalg.norm(h) <= 1e-9, d
         assert ens.dt[d].item() == dt, d
+
+
+def test_ensemble_device_time_loop_matches_host_steps():
+    """wspm_ensemble_run (the time loop in one CUDA graph) gives bit for bit the heads, dt and times of the same
+    number of host-launched steps, sums the Picard iterations of the steps each domain took, and stops by itself
+    when every domain has reached tmax."""
+    from wspm_b200.ensemble import Ensemble
+    doms = _domains([8, 12, 16, 10, 20, 6], seed=4)
+    kw = dict(dt0=1e-3, tmax=2.5e-2, krylov_tol=1e-10, krylov_maxiter=1000)
+    host, dev = Ensemble(doms, **kw), Ensemble(doms, **kw)
+    for e in (host, dev):
+        e.set_state(-1.0)
+        e.cluster_size = 2
+    total = np.zeros(len(doms), dtype=np.int64)
+    for _ in range(4):
+        r = host.step()
+        total += np.where(r["active"], r["iterations"], 0)
+    its, run = dev.run_device(4)
+    torch.cuda.synchronize()
+    assert run.cpu().tolist()[0] == 4
+    np.testing.assert_array_equal(its.cpu().numpy(), total)
+    assert torch.equal(host.h_n, dev.h_n) and torch.equal(host.dt, dev.dt) and torch.equal(host.t, dev.t)
+    host.run()                                       # to tmax from the host
+    its2, run2 = dev.run_device(1000)                # to tmax on the device
+    torch.cuda.synchronize()
+    assert run2.cpu().tolist()[1] == 0 and dev.active() == 0
+    assert torch.equal(host.h_n, dev.h_n) and torch.equal(host.t, dev.t)
