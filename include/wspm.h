@@ -50,6 +50,7 @@ extern "C" {
 #define WSPM_PRECOND_ILU      2   /* the reference's create_ilu0 (symmetric Gauss-Seidel form) */
 #define WSPM_PRECOND_SSOR     3   /* the reference's create_ssor: omega (D/omega + L)^-1        */
 #define WSPM_PRECOND_BLOCK_JACOBI 4
+#define WSPM_PRECOND_ILU0     5   /* true ILU(0) on A's pattern (wspm_ilu0_factor), not the reference's ilu */
 #define WSPM_SOIL_VAN_GENUCHTEN 0
 #define WSPM_SOIL_EXPONENTIAL   1
 
@@ -511,6 +512,16 @@ typedef struct wspm_levels {
 int wspm_precond_apply(const wspm_pattern *pat, const double *vals, int32_t kind, double omega,
                        int32_t block_size, const wspm_levels *lower, const wspm_levels *upper, const double *x,
                        double *y, double *tmp, void *stream);
+/* True ILU(0): incomplete LU with zero fill on A's own pattern (IKJ form; the
+ * rows of one level of the lower sweep's schedule factor in parallel).  No
+ * reference counterpart: the reference's `ilu` never updates a pivot (see
+ * WSPM_PRECOND_ILU); this is the factorization that name stands for.  lu: a
+ * values array in the pattern's layout receiving L (strict lower part, unit
+ * diagonal implied) and U; apply with wspm_precond_apply(kind =
+ * WSPM_PRECOND_ILU0, vals = lu, lower and upper schedules).  Zero pivots are
+ * taken as 1.                                                               */
+int wspm_ilu0_factor(const wspm_pattern *pat, const double *vals, const wspm_levels *lower, double *lu,
+                     void *stream);
 
 /* ---- mass balance and transport stability numbers (2D) ---------------------
  * integrate_2d_domain, src/solvers/.ipynb_checkpoints/richards_mass_balance-checkpoint.py:25-69

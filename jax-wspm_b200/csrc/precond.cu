@@ -68,6 +68,91 @@ __global__ void __launch_bounds__(1024) tri_sweep_kernel(Sell A, const double *_
     }
 }
 
+// ---- true ILU(0) -------------------------------------------------------------
+// Incomplete LU with zero fill on A's own pattern (Saad, Iterative Methods for
+// Sparse Linear Systems, 2nd ed., Alg. 10.4, IKJ form): for each row i, for its
+// entries k < i in ascending column order, l_ik = a_ik / u_kk, then
+// a_ij -= l_ik u_kj for every later entry j of row i that row k also holds.  Row i
+// reads only rows k < i, all of earlier levels of the lower sweep's schedule, so
+// the rows of one level factor in parallel.  Result in `lu` (same layout as
+// `vals`): the strict lower part holds L (unit diagonal implied), the rest U.  A
+// zero pivot u_kk is taken as 1 (the reference's convention for zero diagonals).
+// Not the reference's `ilu` (which never updates a pivot, see create_ilu0
+// above): this is the factorization SURVEY-style "true ILU(0)" names.
+
+// position q of column j in row i, -1 when the row does not hold it
+__device__ __forceinline__ int entry_index(const Sell &A, int i, int j) {
+    const int w = row_width(A, i);
+    for (int q = 0; q < w; ++q)
+        if (entry_col(A, i, q) == j) return q;
+    return -1;
+}
+
+__global__ void __launch_bounds__(1024) ilu0_factor_kernel(Sell A, const int32_t *__restrict__ diag_pos,
+                                                           const int32_t *__restrict__ level_ptr,
+                                                           const int32_t *__restrict__ rows, int n_levels,
+                                                           double *lu) {
+    const int n = A.n_rows;
+    for (int lv = 0; lv < n_levels; ++lv) {
+        const int k1 = level_ptr[lv + 1];
+        for (int kk = level_ptr[lv] + threadIdx.x; kk < k1; kk += blockDim.x) {
+            const int i = rows[kk];
+            const int w = row_width(A, i);
+            // entries in ascending column order: SELL rows are sorted; DIA offsets ascend
+            for (int q = 0; q < w; ++q) {
+                const int k = entry_col(A, i, q);
+                if (k < 0 || k >= n || k >= i) continue;
+                const int64_t pik = entry_pos(A, i, q);
+                const double aik = lu[pik];
+                if (aik == 0.0) continue;
+                const double ukk = lu[entry_pos(A, k, diag_pos[k])];
+                const double l = aik / (ukk != 0.0 ? ukk : 1.0);
+                lu[pik] = l;
+                for (int q2 = q + 1; q2 < w; ++q2) {
+                    const int j = entry_col(A, i, q2);
+                    if (j <= k || j < 0 || j >= n) continue;
+                    const int qk = entry_index(A, k, j);
+                    if (qk < 0) continue;
+                    lu[entry_pos(A, i, q2)] -= l * lu[entry_pos(A, k, qk)];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// y = (LU)^-1 x with the factors above: forward sweep with unit-lower L, backward with U.
+template <int MODE>
+__global__ void __launch_bounds__(1024) ilu0_sweep_kernel(Sell A, const double *__restrict__ lu,
+                                                          const int32_t *__restrict__ diag_pos,
+                                                          const int32_t *__restrict__ level_ptr,
+                                                          const int32_t *__restrict__ rows, int n_levels,
+                                                          const double *__restrict__ x, double *y) {
+    const int n = A.n_rows;
+    for (int lv = 0; lv < n_levels; ++lv) {
+        const int k1 = level_ptr[lv + 1];
+        for (int kk = level_ptr[lv] + threadIdx.x; kk < k1; kk += blockDim.x) {
+            const int i = rows[kk];
+            const int w = row_width(A, i);
+            double s = x[i];
+            for (int q = 0; q < w; ++q) {
+                const int j = entry_col(A, i, q);
+                if (j < 0 || j >= n) continue;
+                if (MODE == 1 ? !(j > i) : !(j < i)) continue;
+                const double a = lu[entry_pos(A, i, q)];
+                if (a != 0.0) s -= a * y[j];
+            }
+            if (MODE == 0) {
+                y[i] = s;
+            } else {
+                const double d = lu[entry_pos(A, i, diag_pos[i])];
+                y[i] = s / (d != 0.0 ? d : 1.0);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // value of A(i, j) in row i (0 when absent)
 __device__ __forceinline__ double entry_value(const Sell &A, const double *vals, int i, int j) {
     const int w = row_width(A, i);
@@ -115,6 +200,14 @@ extern "C" int wspm_precond_apply(const wspm_pattern *pat, const double *vals, i
                                                 lower->n_levels, x, tmp, omega);
         tri_sweep_kernel<1><<<1, 1024, 0, st>>>(A, vals, pat->diag_pos, upper->level_ptr, upper->rows,
                                                 upper->n_levels, tmp, y, omega);
+    } else if (kind == WSPM_PRECOND_ILU0) {
+        // vals holds the factors of wspm_ilu0_factor
+        if (!lower || !upper || !tmp || !lower->level_ptr || !lower->rows || !upper->level_ptr || !upper->rows)
+            return WSPM_BAD_ARG;
+        ilu0_sweep_kernel<0><<<1, 1024, 0, st>>>(A, vals, pat->diag_pos, lower->level_ptr, lower->rows,
+                                                 lower->n_levels, x, tmp);
+        ilu0_sweep_kernel<1><<<1, 1024, 0, st>>>(A, vals, pat->diag_pos, upper->level_ptr, upper->rows,
+                                                 upper->n_levels, tmp, y);
     } else if (kind == WSPM_PRECOND_SSOR) {
         if (!lower || !lower->level_ptr || !lower->rows || !(omega != 0.0)) return WSPM_BAD_ARG;
         tri_sweep_kernel<2><<<1, 1024, 0, st>>>(A, vals, pat->diag_pos, lower->level_ptr, lower->rows,
@@ -122,5 +215,16 @@ extern "C" int wspm_precond_apply(const wspm_pattern *pat, const double *vals, i
     } else {
         return WSPM_UNSUPPORTED;
     }
+    return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
+}
+
+extern "C" int wspm_ilu0_factor(const wspm_pattern *pat, const double *vals, const wspm_levels *lower, double *lu,
+                                void *stream) {
+    if (!pat || !vals || !lu || !lower || !lower->level_ptr || !lower->rows || pat->n_rows <= 0 || !pat->diag_pos)
+        return WSPM_BAD_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    WSPM_CUDA_TRY(cudaMemcpyAsync(lu, vals, (size_t)pat->nnz_padded * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    ilu0_factor_kernel<<<1, 1024, 0, st>>>(make_sell(pat), pat->diag_pos, lower->level_ptr, lower->rows,
+                                           lower->n_levels, lu);
     return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
 }

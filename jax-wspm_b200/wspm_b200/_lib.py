@@ -86,13 +86,14 @@ class WspmLevels(ctypes.Structure):
     _fields_ = [("n_levels", c_int32), ("level_ptr", c_void_p), ("rows", c_void_p)]
 
 
-PRECOND_KIND = {"ilu": 2, "ssor": 3, "block_jacobi": 4}
+PRECOND_KIND = {"ilu": 2, "ssor": 3, "block_jacobi": 4, "ilu0": 5}
 P = ctypes.POINTER
 _SIGS = {
     "wspm_balance_workspace_doubles": (c_int64, []),
     "wspm_integrate_2d": (c_int32, [P(WspmMesh), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_peclet_courant": (c_int32, [P(WspmMesh), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
                                       c_void_p, c_void_p, c_void_p]),
+    "wspm_ilu0_factor": (c_int32, [P(WspmPattern), c_void_p, P(WspmLevels), c_void_p, c_void_p]),
     "wspm_precond_apply": (c_int32, [P(WspmPattern), c_void_p, c_int32, c_double, c_int32, P(WspmLevels),
                                      P(WspmLevels), c_void_p, c_void_p, c_void_p, c_void_p]),
     "wspm_ensemble_workspace_doubles": (c_int64, [c_int32, c_int64]),

@@ -2,7 +2,9 @@
 
 ``ReferencePreconditioner`` applies create_ilu0 / create_ssor / create_block_jacobi
 (src/solvers/jax_linear_solver.py:38-252) as their code computes them, on the
-device (``wspm_precond_apply``; triangular sweeps level scheduled).  The
+device (``wspm_precond_apply``; triangular sweeps level scheduled); kind
+``"ilu0"`` is a true ILU(0) on A's pattern (``wspm_ilu0_factor``), which the
+reference's ``ilu`` is not.  The
 solvers below follow jax.scipy.sparse.linalg's cg / bicgstab / gmres with a
 general preconditioner -- the same recurrences and stopping rules as the
 device-resident Jacobi path (JAX: with a preconditioner CG tests r.r; GMRES is
@@ -28,11 +30,17 @@ class ReferencePreconditioner:
         if kind == "block_jacobi" and self.block_size not in (1, 2):
             raise NotImplementedError("block_jacobi: block_size 1 or 2 on the device path")
         self.lower = self.upper = None
-        if kind in ("ilu", "ssor"):
+        if kind in ("ilu", "ssor", "ilu0"):
             self.lower = self._levels(True)
-        if kind == "ilu":
+        if kind in ("ilu", "ilu0"):
             self.upper = self._levels(False)
         self.tmp = dm.vec()
+        if kind == "ilu0":
+            # true ILU(0): factor once on the device, then apply the two sweeps with the factors
+            self.vals = dm.empty_vals()
+            check("ilu0_factor", lib.wspm_ilu0_factor(ctypes.byref(dm.c_pat), dptr(vals), ctypes.byref(self.lower),
+                                                      dptr(self.vals),
+                                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
 
     def _levels(self, lower):
         cache = self.dm.__dict__.setdefault("_tri_levels", {})
@@ -163,8 +171,15 @@ def gmres(A, b, x0, M, tol=1e-10, atol=0.0, restart=30, maxiter=100):
 
 
 def solve(dm, vals, b, x0, solver, precond, tol=1e-10, atol=0.0, maxiter=100, restart=30, omega=1.0, block_size=2):
-    """(x, iterations) of A x = b with the reference's preconditioner ``precond`` (ilu / ssor / block_jacobi)."""
-    M = ReferencePreconditioner(dm, vals, precond, omega=omega, block_size=block_size)
+    """(x, iterations) of A x = b with the preconditioner ``precond``: the reference's ilu / ssor / block_jacobi,
+    the true ILU(0) (``"ilu0"``) or Jacobi (host-driven loop; the device-resident Jacobi solvers are
+    ``device.krylov_solve``)."""
+    if precond == "jacobi":
+        from .device import jacobi_dinv
+        dinv = jacobi_dinv(dm, vals)
+        M = lambda v: dinv * v  # noqa: E731
+    else:
+        M = ReferencePreconditioner(dm, vals, precond, omega=omega, block_size=block_size)
     A = lambda v: spmv(dm, vals, v)  # noqa: E731
     if solver == "cg":
         return cg(A, b, x0, M, tol, atol, maxiter)

@@ -277,3 +277,59 @@ def solve_system(A, b, x0, solver_type="gmres", precond_type="none", tol=1e-10,
         import scipy.sparse.linalg as spla
         return spla.spsolve(A.tocsc(), b), 0
     raise ValueError(f"Unsupported solver type: {solver_type}")
+
+
+def true_ilu0(A):
+    """Incomplete LU with zero fill on A's own pattern (Saad, Iterative Methods for Sparse Linear Systems,
+    Alg. 10.4, IKJ form) -- not a reference function (the reference's `ilu` is `reference_preconditioner`'s
+    symmetric Gauss-Seidel form); the factorization the device's wspm_ilu0_factor computes.  Returns a CSR matrix
+    holding L (strict lower part, unit diagonal implied) and U; zero pivots are taken as 1."""
+    import scipy.sparse as sp
+    LU = sp.csr_matrix(A, dtype=np.float64, copy=True)
+    LU.sort_indices()
+    ip, ix, d = LU.indptr, LU.indices, LU.data
+    n = LU.shape[0]
+    diag = np.full(n, -1, dtype=np.int64)
+    for i in range(n):
+        for q in range(ip[i], ip[i + 1]):
+            if ix[q] == i:
+                diag[i] = q
+    for i in range(n):
+        pos = {int(ix[q]): q for q in range(ip[i], ip[i + 1])}
+        for q in range(ip[i], ip[i + 1]):
+            k = int(ix[q])
+            if k >= i:
+                break
+            if d[q] == 0.0:
+                continue
+            ukk = d[diag[k]] if diag[k] >= 0 else 0.0
+            lik = d[q] / (ukk if ukk != 0.0 else 1.0)
+            d[q] = lik
+            for q2 in range(ip[k], ip[k + 1]):
+                j = int(ix[q2])
+                if j > k and j in pos and pos[j] > q:
+                    d[pos[j]] -= lik * d[q2]
+    return LU
+
+
+def true_ilu0_apply(LU, x):
+    """y = (L U)^-1 x with the factors of true_ilu0 (forward sweep with unit L, backward with U)."""
+    ip, ix, d = LU.indptr, LU.indices, LU.data
+    n = LU.shape[0]
+    y = np.array(x, dtype=np.float64, copy=True)
+    for i in range(n):
+        s = y[i]
+        for q in range(ip[i], ip[i + 1]):
+            if ix[q] < i:
+                s -= d[q] * y[ix[q]]
+        y[i] = s
+    z = np.zeros(n)
+    for i in range(n - 1, -1, -1):
+        s, di = y[i], 0.0
+        for q in range(ip[i], ip[i + 1]):
+            if ix[q] > i:
+                s -= d[q] * z[ix[q]]
+            elif ix[q] == i:
+                di = d[q]
+        z[i] = s / (di if di != 0.0 else 1.0)
+    return z

@@ -93,3 +93,28 @@ def test_oracle_pipelined_cg_converges_like_cg():
     # a cap stops the run with exactly maxiter updates
     _, k3 = krylov.pipelined_cg(A, b, np.zeros(n), tol=0.0, maxiter=7, dinv=d)
     assert k3 == 7
+
+
+def test_oracle_true_ilu0_reproduces_a_on_its_pattern():
+    """The defining property of ILU(0): (L U)_ij = A_ij on every position of A's pattern (here a 2D P1 Richards
+    matrix with Dirichlet rows), and the factorization is exact for a tridiagonal matrix."""
+    import scipy.sparse as sp
+    from oracle import assembly as oasm, krylov as okry, soil as osoil
+    from wspm_b200 import mesh
+    pts, tri = mesh.structured_triangles(12, 1.0)
+    h = -np.linspace(0.1, 2.0, len(pts))
+    C, K, th = osoil.van_genuchten_model(h, (3.35, 0.368, 0.102, 2.0, 0.5, 0.0922))
+    A, b = oasm.assemble_richards(tri, len(pts), pts, th, th - 1e-3, h, K, C, 1e-3)
+    top = np.where(pts[:, 1] == 1.0)[0]
+    A, b = oasm.apply_dirichlet_rows(A, b, top, -0.1 * np.ones(top.size))
+    LU = okry.true_ilu0(A)
+    L = sp.tril(LU, -1) + sp.eye(A.shape[0])
+    U = sp.triu(LU)
+    prod = (L @ U).tocsr()
+    Ac = A.tocoo()
+    np.testing.assert_allclose(np.asarray(prod[Ac.row, Ac.col]).ravel(), Ac.data, rtol=1e-12,
+                               atol=1e-12 * np.abs(Ac.data).max())
+    n = 25
+    T = sp.diags([-np.ones(n - 1), 3 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1]).tocsr()
+    x = np.random.default_rng(1).standard_normal(n)
+    np.testing.assert_allclose(T @ okry.true_ilu0_apply(okry.true_ilu0(T), x), x, atol=1e-12)
