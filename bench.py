@@ -405,6 +405,19 @@ def ensemble_measure(n_domains, steps, warmup, seed, world=1, rank=0):
     mine = partition_domains([7 * len(d[0]) for d in all_doms], world)[rank]
     doms = [all_doms[int(i)] for i in mine]
     sizes = np.array([len(d[0]) for d in doms])
+    # start-up: the pattern of the block-diagonal union mesh, host builder vs device builder
+    from wspm_b200.pattern import Pattern
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    union = np.concatenate([d[1] + off[i] for i, d in enumerate(doms)])
+    t0 = time.perf_counter()
+    Pattern(union, int(off[-1]), layout="sell", builder="native")
+    t_host = time.perf_counter() - t0
+    Pattern(union, int(off[-1]), layout="sell", builder="device")      # warm (module load, first allocations)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Pattern(union, int(off[-1]), layout="sell", builder="device")
+    torch.cuda.synchronize()
+    t_dev = time.perf_counter() - t0
     dt0, tmax = 1e-4, 1.0
     kw = dict(krylov_tol=1e-10, krylov_maxiter=2000, picard_tol=1e-6, picard_maxiter=100)
     ens = Ensemble(doms, dt0=dt0, tmax=tmax, **kw)
@@ -468,7 +481,10 @@ def ensemble_measure(n_domains, steps, warmup, seed, world=1, rank=0):
                         "cluster_size": ens.cluster_size,
                         "autotune_ms": getattr(ens, "timing", {})},
             "sequential": {"seconds": t_seq, "value": dofits_seq / t_seq},
-            "speedup_vs_sequential": (dofits / t_batch) / (dofits_seq / t_seq)}
+            "speedup_vs_sequential": (dofits / t_batch) / (dofits_seq / t_seq),
+            "startup_pattern": {"nodes": int(off[-1]), "elements": int(len(union)), "host_builder_s": t_host,
+                                "device_builder_s": t_dev, "note": "device time includes copying the arrays back "
+                                                                   "to host NumPy (the Pattern object keeps both)"}}
     return line
 
 
@@ -825,7 +841,8 @@ def main():
         line["ensemble"] = {"workload": e["config"]["workload"], "domains": e["config"]["domains"],
                             "nodes_total": e["config"]["nodes_total"], "steps": 3,
                             "batched": e["batched"], "sequential": e["sequential"],
-                            "batched_value": e["value"], "speedup_vs_sequential": e["speedup_vs_sequential"]}
+                            "batched_value": e["value"], "speedup_vs_sequential": e["speedup_vs_sequential"],
+                            "startup_pattern": e["startup_pattern"]}
     print(json.dumps(line))
     barrier(world)
     if world > 1:

@@ -128,6 +128,35 @@ typedef struct wspm_pattern_host {
 int wspm_pattern_build(const int64_t *elements, int64_t n_elems, int32_t nv, int32_t n_nodes,
                        const int64_t *extra_pairs, int64_t n_extra, int32_t layout, wspm_pattern_host **out);
 void wspm_pattern_free(wspm_pattern_host *p);
+/* Device-side pattern builder: the arrays of wspm_pattern_build (no extra
+ * pairs), element for element, built on the GPU from the connectivity already
+ * there (conn: int32 [n_elems * nv], device).  Same reference function as the
+ * host builder.  Two phases, because the library allocates nothing:
+ *   wspm_pattern_device_count: fills *sizes (host struct) and leaves its work in
+ *     `scratch` (device, wspm_pattern_device_scratch_bytes bytes); synchronises
+ *     with the host once to read the sizes;
+ *   wspm_pattern_device_fill: writes the device arrays, sized from *sizes
+ *     (csr_indptr [n_rows+1], csr_indices / sell_index [nnz], slice_ptr /
+ *     inc_ptr [n_slices+1], slice_width / inc_width [n_slices], cols
+ *     [nnz_padded], diag_pos [n_rows], diag_offsets [n_diags], inc_elem /
+ *     inc_slots [n_inc]); the scratch must be the one count filled.
+ * WSPM_BAD_ARG for ids out of range or a node in no element; WSPM_UNSUPPORTED
+ * where the host builder returns it, for a row that gathers more than 128
+ * element vertices, and beyond 2^33 rows (use the host builder then).       */
+typedef struct wspm_pattern_sizes {
+    int32_t n_rows, n_slices, max_width, max_inc, n_diags, layout;
+    int64_t nnz, nnz_padded, n_inc, ld;
+    int32_t diag_offsets[64];
+} wspm_pattern_sizes;
+int64_t wspm_pattern_device_scratch_bytes(int64_t n_elems, int32_t nv, int32_t n_nodes);
+int wspm_pattern_device_count(const int32_t *conn, int64_t n_elems, int32_t nv, int32_t n_nodes, int32_t layout,
+                              void *scratch, int64_t scratch_bytes, wspm_pattern_sizes *sizes, void *stream);
+int wspm_pattern_device_fill(const int32_t *conn, int64_t n_elems, int32_t nv, int32_t n_nodes,
+                             const wspm_pattern_sizes *sizes, void *scratch, int64_t scratch_bytes,
+                             int64_t *csr_indptr, int32_t *csr_indices, int64_t *sell_index, int64_t *slice_ptr,
+                             int32_t *slice_width, int32_t *cols, int32_t *diag_pos, int32_t *diag_offsets,
+                             int64_t *inc_ptr, int32_t *inc_width, int32_t *inc_elem, uint32_t *inc_slots,
+                             void *stream);
 /* Level schedule of a triangular sweep over a CSR pattern (host): level[i] =
  * 1 + the highest level among the rows row i depends on (columns j < i when
  * lower != 0, j > i otherwise), 0 without dependencies; *n_levels = max + 1.

@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(1024) ilu0_factor_kernel(Sell A, const int32_t
         for (int kk = level_ptr[lv] + threadIdx.x; kk < k1; kk += blockDim.x) {
             const int i = rows[kk];
             const int w = row_width(A, i);
+            const int dpi = diag_pos[i];     // SELL padding slots also name column i: only this one is the diagonal
             // entries in ascending column order: SELL rows are sorted; DIA offsets ascend
             for (int q = 0; q < w; ++q) {
                 const int k = entry_col(A, i, q);
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(1024) ilu0_factor_kernel(Sell A, const int32_t
                 lu[pik] = l;
                 for (int q2 = q + 1; q2 < w; ++q2) {
                     const int j = entry_col(A, i, q2);
-                    if (j <= k || j < 0 || j >= n) continue;
+                    if (j <= k || j < 0 || j >= n || (j == i && q2 != dpi)) continue;
                     const int qk = entry_index(A, k, j);
                     if (qk < 0) continue;
                     lu[entry_pos(A, i, q2)] -= l * lu[entry_pos(A, k, qk)];

@@ -38,6 +38,12 @@ class WspmEdges(ctypes.Structure):
                 ("e_local", c_void_p), ("e_other", c_void_p), ("e_kother", c_void_p), ("e_jac", c_void_p)]
 
 
+class WspmPatternSizes(ctypes.Structure):
+    _fields_ = [("n_rows", c_int32), ("n_slices", c_int32), ("max_width", c_int32), ("max_inc", c_int32),
+                ("n_diags", c_int32), ("layout", c_int32), ("nnz", c_int64), ("nnz_padded", c_int64),
+                ("n_inc", c_int64), ("ld", c_int64), ("diag_offsets", c_int32 * 64)]
+
+
 class WspmPicardDesc(ctypes.Structure):
     _fields_ = [("mesh", ctypes.POINTER(WspmMesh)), ("pat", ctypes.POINTER(WspmPattern)),
                 ("soil_model", c_int32), ("phi", c_double * 6), ("Ks_elem", c_void_p), ("bc_val", c_void_p),
@@ -154,6 +160,11 @@ _SIGS = {
     "wspm_pattern_build": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_int64, c_int32,
                                      P(P(WspmPatternHost))]),
     "wspm_pattern_free": (None, [P(WspmPatternHost)]),
+    "wspm_pattern_device_scratch_bytes": (c_int64, [c_int64, c_int32, c_int32]),
+    "wspm_pattern_device_count": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_int32, c_void_p, c_int64,
+                                            P(WspmPatternSizes), c_void_p]),
+    "wspm_pattern_device_fill": (c_int32, [c_void_p, c_int64, c_int32, c_int32, P(WspmPatternSizes), c_void_p,
+                                           c_int64] + [c_void_p] * 12 + [c_void_p]),
     "wspm_pattern_levels": (c_int32, [c_void_p, c_void_p, c_int32, c_int32, c_void_p, P(c_int32)]),
     "wspm_version": (ctypes.c_char_p, []),
     "wspm_status_string": (ctypes.c_char_p, [c_int32]),

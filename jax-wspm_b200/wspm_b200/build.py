@@ -14,7 +14,7 @@ PKG_ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(PKG_ROOT, "csrc")
 INCLUDE = os.path.join(os.path.dirname(PKG_ROOT), "include")
 LIB = os.path.join(HERE, "libwspm.so")
-SOURCES = ["assembly.cu", "krylov.cu", "picard.cu", "capi.cu", "transport.cu", "noalloc.cu", "ensemble.cu", "adjoint.cu", "precond.cu", "balance.cu", "pattern.cu", "measure.cu"]
+SOURCES = ["assembly.cu", "krylov.cu", "picard.cu", "capi.cu", "transport.cu", "noalloc.cu", "ensemble.cu", "adjoint.cu", "precond.cu", "balance.cu", "pattern.cu", "measure.cu", "pattern_dev.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]

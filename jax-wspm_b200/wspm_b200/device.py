@@ -35,7 +35,8 @@ def _require_cuda(t, dtype, name, numel=None):
 class DeviceMesh:
     """Mesh + pattern on the GPU.  ``points`` (N, dim) float64, ``elements`` (E, dim+1)."""
 
-    def __init__(self, points, elements, device=None, pattern=None, layout="auto", extra_pairs=None):
+    def __init__(self, points, elements, device=None, pattern=None, layout="auto", extra_pairs=None,
+                 builder="native"):
         points = np.ascontiguousarray(points, dtype=np.float64)
         elements = np.ascontiguousarray(elements, dtype=np.int64)
         if elements.ndim != 2 or elements.shape[1] != points.shape[1] + 1:
@@ -47,21 +48,28 @@ class DeviceMesh:
         self.n_nodes, self.dim = points.shape
         self.n_elems, self.nv = elements.shape
         self.pattern = pattern if pattern is not None else Pattern(elements, self.n_nodes, layout=layout,
-                                                                   extra_pairs=extra_pairs)
+                                                                   extra_pairs=extra_pairs, builder=builder)
         pat = self.pattern
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self.conn = t(elements.astype(np.int32))
         self.coords = t(points)
-        self.slice_ptr = t(pat.slice_ptr)
-        self.slice_width = t(pat.slice_width)
-        self.cols = t(pat.cols)
-        self.diag_pos = t(pat.diag_pos)
-        self.inc_ptr = t(pat.inc_ptr)
-        self.inc_width = t(pat.inc_width)
-        self.inc_elem = t(pat.inc_elem)
-        self.inc_slots = t(pat.inc_slots.view(np.int32))
-        self.sell_index = t(pat.sell_index)
-        self.diag_offsets = t(pat.diag_offsets if pat.n_diags else np.zeros(1, dtype=np.int32))
+        dev_arrays = getattr(pat, "device_arrays", None)
+        if dev_arrays is not None and dev_arrays["cols"].device == self.device:
+            # built on this GPU (Pattern(builder="device")): use the arrays where they are
+            for k in ("slice_ptr", "slice_width", "cols", "diag_pos", "inc_ptr", "inc_width", "inc_elem",
+                      "inc_slots", "sell_index", "diag_offsets"):
+                setattr(self, k, dev_arrays[k])
+        else:
+            self.slice_ptr = t(pat.slice_ptr)
+            self.slice_width = t(pat.slice_width)
+            self.cols = t(pat.cols)
+            self.diag_pos = t(pat.diag_pos)
+            self.inc_ptr = t(pat.inc_ptr)
+            self.inc_width = t(pat.inc_width)
+            self.inc_elem = t(pat.inc_elem)
+            self.inc_slots = t(pat.inc_slots.view(np.int32))
+            self.sell_index = t(pat.sell_index)
+            self.diag_offsets = t(pat.diag_offsets if pat.n_diags else np.zeros(1, dtype=np.int32))
         self.c_mesh = _lib.WspmMesh(self.n_nodes, self.n_elems, self.dim, self.nv, self.conn.data_ptr(),
                                     self.coords.data_ptr())
         self.c_pat = _lib.WspmPattern(pat.n_rows, pat.n_slices, pat.max_width, pat.max_inc, pat.nnz_padded,

@@ -31,12 +31,18 @@ class Pattern:
     def __init__(self, elements, n_nodes, layout="auto", extra_pairs=None, builder="native"):
         """``extra_pairs`` (k, 2): node pairs that must have matrix slots although no element
         contains both (boundary edges whose end points are not an element edge); both (i, j) and
-        (j, i) are added.  ``builder``: "native" (``wspm_pattern_build`` in libwspm) or "numpy" (the same
-        arrays built with NumPy; kept as the restatement the native builder is tested against)."""
+        (j, i) are added.  ``builder``: "native" (``wspm_pattern_build`` in libwspm, host), "device" (the same
+        arrays built on the GPU by ``wspm_pattern_device_count`` / ``_fill``; no ``extra_pairs``; the device
+        arrays are kept in ``device_arrays`` for DeviceMesh) or "numpy" (the same arrays built with NumPy; kept as
+        the restatement the native builders are tested against)."""
         if layout not in ("auto", "sell", "dia"):
             raise ValueError(f"unknown layout {layout!r}")
         if builder == "native":
             self._build_native(elements, n_nodes, layout, extra_pairs)
+        elif builder == "device":
+            if extra_pairs is not None and len(extra_pairs):
+                raise ValueError("the device builder takes no extra pairs (use builder='native')")
+            self._build_device(elements, n_nodes, layout)
         elif builder == "numpy":
             self._build_numpy(elements, n_nodes, layout, extra_pairs)
         else:
@@ -88,6 +94,59 @@ class Pattern:
             self.inc_slots = arr(h.inc_slots, h.n_inc)
         finally:
             _lib.lib.wspm_pattern_free(out)
+
+    def _build_device(self, elements, n_nodes, layout, device=None):
+        import ctypes
+        import torch
+        from . import _lib
+        el = elements if isinstance(elements, torch.Tensor) else torch.as_tensor(np.asarray(elements))
+        dev = torch.device(device or (el.device if el.is_cuda else "cuda"))
+        conn = el.to(device=dev, dtype=torch.int32).contiguous()
+        if conn.ndim != 2:
+            raise ValueError("elements must be a 2D array")
+        E, nv = conn.shape
+        N = int(n_nodes)
+        lib = _lib.lib
+        nbytes = int(lib.wspm_pattern_device_scratch_bytes(E, nv, N))
+        if nbytes <= 0:
+            raise ValueError("invalid mesh sizes")
+        scratch = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        sz = _lib.WspmPatternSizes()
+        st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        code = {"auto": 0, "sell": 1, "dia": 2}[layout]
+        rc = lib.wspm_pattern_device_count(conn.data_ptr(), E, nv, N, code, scratch.data_ptr(), nbytes,
+                                           ctypes.byref(sz), st)
+        if rc == _lib.WSPM_UNSUPPORTED:
+            raise ValueError("pattern not representable (too many diagonals for DIA, rows longer than 63, or rows "
+                             "that gather more than 128 element vertices: use builder='native')")
+        if rc != _lib.WSPM_OK:
+            raise ValueError("invalid mesh: element ids out of bounds or nodes that belong to no element")
+        ns = int(sz.n_slices)
+        i64 = dict(dtype=torch.int64, device=dev)
+        i32 = dict(dtype=torch.int32, device=dev)
+        d = {"csr_indptr": torch.empty(N + 1, **i64), "csr_indices": torch.empty(int(sz.nnz), **i32),
+             "sell_index": torch.empty(int(sz.nnz), **i64), "slice_ptr": torch.empty(ns + 1, **i64),
+             "slice_width": torch.empty(ns, **i32), "cols": torch.empty(int(sz.nnz_padded), **i32),
+             "diag_pos": torch.empty(N, **i32), "diag_offsets": torch.zeros(max(1, int(sz.n_diags)), **i32),
+             "inc_ptr": torch.empty(ns + 1, **i64), "inc_width": torch.empty(ns, **i32),
+             "inc_elem": torch.empty(int(sz.n_inc), **i32), "inc_slots": torch.empty(int(sz.n_inc), **i32)}
+        order = ("csr_indptr", "csr_indices", "sell_index", "slice_ptr", "slice_width", "cols", "diag_pos",
+                 "diag_offsets", "inc_ptr", "inc_width", "inc_elem", "inc_slots")
+        rc = lib.wspm_pattern_device_fill(conn.data_ptr(), E, nv, N, ctypes.byref(sz), scratch.data_ptr(), nbytes,
+                                          *[d[k].data_ptr() for k in order], st)
+        _lib.check("pattern_device_fill", rc)
+        self.n_rows, self.n_elems, self.nv = N, E, nv
+        self.nnz, self.n_slices, self.nnz_padded = int(sz.nnz), ns, int(sz.nnz_padded)
+        self.layout = "dia" if sz.layout == 2 else "sell"
+        self.ld = int(sz.ld)
+        self.max_width, self.max_inc, self.n_diags = int(sz.max_width), int(sz.max_inc), int(sz.n_diags)
+        host = {k: v.cpu().numpy() for k, v in d.items()}
+        for k in order:
+            setattr(self, k, host[k])
+        self.inc_slots = host["inc_slots"].view(np.uint32)
+        if not self.n_diags:
+            self.diag_offsets = np.zeros(0, dtype=np.int32)
+        self.device_arrays = d
 
     def _slot(self, rows, cols_):
         if self.layout == "dia":

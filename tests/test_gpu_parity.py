@@ -553,3 +553,66 @@ def test_structural_zero_diagonals_are_exactly_zero(kind, n):
         if kind == "tri" and n == 64:
             dead = {int(o) for k, o in enumerate(offs) if not (live >> k) & 1}
             assert dead == {n + 2, -(n + 2)}, dead
+
+
+def _device_pattern_cases():
+    from wspm_b200 import mesh as m
+    pts, tri = m.structured_triangles(40, 1.0)
+    rng = np.random.default_rng(11)
+    perm = rng.permutation(len(pts))
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(pts))
+    p3, tets = m.kuhn_tetrahedra(6, 1.0)
+    doms = m.vg_parameter_ensemble(12, 3, sides=(32, 48, 64))
+    sizes = np.array([len(d[0]) for d in doms])
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    union = np.concatenate([d[1] + off[i] for i, d in enumerate(doms)])
+    z = np.load(os.path.join(GOLD, "solute_pinns25.npz"))
+    return [("tri_auto", tri, len(pts), "auto"), ("tri_sell", tri, len(pts), "sell"),
+            ("tri_permuted", inv[tri], len(pts), "auto"), ("tet_auto", tets, len(p3), "auto"),
+            ("ensemble_union", union, int(off[-1]), "sell"), ("solute_unstructured", z["triangles"], len(z["points"]),
+                                                               "auto")]
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_device_pattern_builder_matches_host_builder(case):
+    """wspm_pattern_device_count / _fill build, on the GPU, exactly the arrays of the host builder (CSR, storage
+    layout, diagonal positions, incidence with packed row positions) -- structured DIA and SELL, a randomly
+    renumbered mesh, tetrahedra, an ensemble's block-diagonal union and the reference's unstructured SoluteTest
+    mesh."""
+    from wspm_b200.pattern import Pattern
+    name, el, n, layout = _device_pattern_cases()[case]
+    host = Pattern(el, n, layout=layout, builder="native")
+    dev = Pattern(el, n, layout=layout, builder="device")
+    assert (dev.layout, dev.n_diags, dev.nnz, dev.nnz_padded, dev.max_width, dev.max_inc) == \
+           (host.layout, host.n_diags, host.nnz, host.nnz_padded, host.max_width, host.max_inc), name
+    for k in ("csr_indptr", "csr_indices", "sell_index", "slice_ptr", "slice_width", "cols", "diag_pos",
+              "diag_offsets", "inc_ptr", "inc_width", "inc_elem", "inc_slots"):
+        np.testing.assert_array_equal(getattr(dev, k), getattr(host, k), err_msg=f"{name}: {k}")
+
+
+def test_device_pattern_builder_rejects_bad_meshes():
+    from wspm_b200.pattern import Pattern
+    pts, tri = mesh.structured_triangles(4, 1.0)
+    bad = tri.copy()
+    bad[0, 0] = len(pts)
+    with pytest.raises(ValueError):
+        Pattern(bad, len(pts), builder="device")
+    with pytest.raises(ValueError):
+        Pattern(tri, len(pts) + 3, builder="device")          # nodes that belong to no element
+
+
+def test_engine_on_a_device_built_pattern_matches_host_built():
+    """A Picard run on the device-built pattern (DeviceMesh reuses its device arrays) equals the run on the host
+    pattern bit for bit."""
+    from wspm_b200.device import DeviceMesh, merge_dirichlet
+    from wspm_b200.engine import PicardEngine
+    pts, tri = mesh.structured_triangles(48, 1.0)
+    top = np.where(pts[:, 1] == 1.0)[0]
+    bc = merge_dirichlet(len(pts), [(top, -0.1)])
+    out = []
+    for builder in ("native", "device"):
+        eng = PicardEngine(DeviceMesh(pts, tri, builder=builder), "vg", opic.VG_UNIT_PHI, bc_val=bc, solver="cg",
+                           precond="jacobi", krylov_tol=1e-8, krylov_maxiter=5000, mixed=True)
+        out.append(eng.run(-np.ones(len(pts)), 1e-4, 1e-3, fixed_dt=True, max_steps=2)["pressure_head"])
+    np.testing.assert_array_equal(out[0], out[1])
