@@ -309,6 +309,10 @@ constexpr int kRcgBlock = 512;    // 128 registers: the 2D instances run without
 __device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void st_relaxed_u32(unsigned int *p, unsigned int v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // Counting barrier: every block adds one arrival; a block passes once the count
 // reaches `target` (= gridDim * barriers passed so far).  One atomic per block
@@ -1186,9 +1190,11 @@ __global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a
             pp[blockIdx.x] = v[0];
             pp[nb + blockIdx.x] = v[1];
             pp[2 * nb + blockIdx.x] = v[2];
-            __threadfence();
+            // one release fence orders the partials and (after the block barrier) every m store of
+            // the block before both the arrival and the flag, which readers load with acquire
+            fence_acq_rel_gpu();
             atomicAdd(&bar->mono, 1u);
-            st_release_u32(flag + blockIdx.x, epoch);
+            st_relaxed_u32(flag + blockIdx.x, epoch);
         }
     };
     // w0 = A u0 (the grid barrier published u0), then m0 = M w0 and reduction 0
