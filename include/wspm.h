@@ -404,12 +404,23 @@ typedef struct wspm_picard_desc {
     double *Ks_inc;            /* with Ks_elem: wspm_picard_ks_inc_doubles(pat)
                                   doubles, Ks_elem gathered in incidence order
                                   at every step start; NULL without Ks_elem */
+    void *shapes;              /* optional, wspm_picard_shape_bytes(mesh, pat)
+                                  bytes of device memory: the plan records the
+                                  mesh's distinct element Jacobians (bitwise)
+                                  there at creation, and when they are few
+                                  (<= 256 triangle / 64 tetrahedron shapes) its
+                                  assembly reads each element-row's geometric
+                                  factors from a per-shape table instead of
+                                  recomputing them (same values bit for bit);
+                                  NULL: always recompute                     */
 } wspm_picard_desc;
 
 int64_t wspm_picard_workspace_doubles(int32_t n_rows, int32_t mixed);
 /* Size of wspm_picard_desc.Ks_inc: one double per incidence slot
  * (n_slices * 32 * max_inc).                                               */
 int64_t wspm_picard_ks_inc_doubles(const wspm_pattern *pat);
+/* Size in bytes of wspm_picard_desc.shapes for this mesh and pattern.      */
+int64_t wspm_picard_shape_bytes(const wspm_mesh *mesh, const wspm_pattern *pat);
 int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out);
 int wspm_picard_step(void *plan, void *stream);
 /* The same step with the loops driven from the host (identical kernels; the
@@ -426,6 +437,17 @@ int wspm_picard_destroy(void *plan);
  * diagonal), and the step's sparse kernels skip its loads -- fma(0, x, acc) ==
  * acc, so no result changes.  -1 for SELL patterns (nothing skipped).       */
 int64_t wspm_picard_dia_live(void *plan);
+/* Element shapes of a plan: the number of distinct element Jacobians its
+ * assembly takes from the shape table (0: the assembly recomputes every
+ * element's geometry -- no shape buffer, or too many shapes).  No
+ * counterpart in the reference: an assembly-time lookup, results unchanged. */
+int32_t wspm_picard_shapes(void *plan);
+/* One assembly of the plan's system at its current state (theta_m, h_m, K, C
+ * and dt as the step left them; Dirichlet rows, 1/diag, the FP32 copy on a
+ * mixed plan) with the kernel the step runs, the shape path included.
+ * Replaces assemble_global_matrices_sparse_re (src/numerics/
+ * assembly_re_v2.py:62-166) for a caller that holds a plan.               */
+int wspm_picard_assemble(void *plan, void *stream);
 
 /* ---- batched ensemble of independent domains -------------------------------
  * No single reference function: the reference solves one domain per

@@ -59,7 +59,19 @@ struct RichardsAsmArgs {
     float *vals32;
     double *rhs, *dinv;
     RefineStart res;           // used by the RES instantiations only
+    const double *shape_tab;   // CLS: per element shape, kShapeStride<DIM> doubles (shape_table_kernel)
+    int n_shapes;
 };
+
+// Element shapes: elements whose Jacobians are bitwise equal have bitwise equal
+// geometry, so a mesh with few distinct Jacobians (a grid whose coordinates are
+// exact binary fractions has two triangle shapes, six Kuhn tetrahedra) can take
+// the geometric factors of every element-row from a small table instead of
+// recomputing them.  Entry of a shape: detJ, then gg[li][j] = G[:,li] . G[:,j]
+// (NV x NV, the fma chain of the row kernel), then G[DIM-1][li] (NV values).
+template <int DIM> constexpr int kShapeStride = 1 + (DIM + 1) * (DIM + 1) + (DIM + 1);
+template <int DIM> constexpr int kShapeShift = 2 + 6 * (DIM + 1);   // shape id above the incidence word's fields
+template <int DIM> constexpr int kMaxShapes = DIM == 2 ? 256 : 64;
 
 template <int DIM>
 __device__ __forceinline__ void p1_geometry(const double *__restrict__ coords, const int (&nd)[DIM + 1],
@@ -110,13 +122,12 @@ __device__ __forceinline__ void p1_geometry(const double *__restrict__ coords, c
     }
 }
 
-// Same as p1_geometry, from vertex coordinates already in registers.
+// G and detJ from the Jacobian's columns J[r][c] = X[r+1][c] - X[0][c]: the
+// arithmetic of p1_geometry after its differences.
 template <int DIM>
-__device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM], double (&G)[DIM][DIM + 1],
-                                                double &detJ) {
+__device__ __forceinline__ void p1_geometry_j(const double (&J)[DIM][DIM], double (&G)[DIM][DIM + 1], double &detJ) {
     if constexpr (DIM == 2) {
-        const double J00 = X[1][0] - X[0][0], J01 = X[1][1] - X[0][1];
-        const double J10 = X[2][0] - X[0][0], J11 = X[2][1] - X[0][1];
+        const double J00 = J[0][0], J01 = J[0][1], J10 = J[1][0], J11 = J[1][1];
         detJ = J00 * J11 - J01 * J10;
         const double id = 1.0 / detJ;
         G[0][1] = J11 * id;  G[1][1] = -J10 * id;
@@ -124,11 +135,6 @@ __device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM],
         G[0][0] = -(G[0][1] + G[0][2]);
         G[1][0] = -(G[1][1] + G[1][2]);
     } else {
-        double J[3][3];
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) J[r][c] = X[r + 1][c] - X[0][c];
         const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
         const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
         const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
@@ -152,6 +158,23 @@ __device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM],
             G[d][0] = -((inv[d][0] + inv[d][1]) + inv[d][2]);
         }
     }
+}
+
+template <int DIM>
+__device__ __forceinline__ void p1_jacobian(const double (&X)[DIM + 1][DIM], double (&J)[DIM][DIM]) {
+#pragma unroll
+    for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) J[r][c] = X[r + 1][c] - X[0][c];
+}
+
+// Same as p1_geometry, from vertex coordinates already in registers.
+template <int DIM>
+__device__ __forceinline__ void p1_geometry_xyz(const double (&X)[DIM + 1][DIM], double (&G)[DIM][DIM + 1],
+                                                double &detJ) {
+    double J[DIM][DIM];
+    p1_jacobian<DIM>(X, J);
+    p1_geometry_j<DIM>(J, G, detJ);
 }
 
 // Structural zeros of a DIA Richards matrix.  Off the main diagonal the row
@@ -277,17 +300,26 @@ __global__ void incidence_gather_kernel(int n_slices, const int64_t *__restrict_
 //
 // The element-local row index li selects a column of G by selects: an indexed
 // register array would live in local memory.
-template <int DIM, int MW, int KSM, bool STAGE, int TB, int MINB, bool RES>
+//
+// CLS: the incidence words carry the element's shape id (kShapeShift) and the
+// geometric factors come from the shape table, copied into shared memory once
+// per block; the column stage then holds K only.  Every value and every
+// accumulation order are those of the geometry-computing form.
+template <int DIM, int MW, int KSM, bool STAGE, int TB, int MINB, bool RES, bool CLS>
 __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs a) {
     constexpr int NV = DIM + 1;
     constexpr int CH = STAGE ? 4 : 1;   // incidences whose loads are issued together
-    extern __shared__ double acc_sm[];  // [MW][TB] accumulators, then [MW][NV][TB] column data (STAGE)
+    constexpr int CV = CLS ? 1 : NV;    // staged values per column (K; or coordinates and K)
+    extern __shared__ double acc_sm[];  // [MW][TB] accumulators, [MW][CV][TB] column data (STAGE), shapes (CLS)
     __shared__ int s_off[MW];
     const int i = blockIdx.x * TB + threadIdx.x;
     const int s = i >> 5, lane = i & 31;
     const bool dia = a.n_diags > 0;
     if (dia)
         for (int k = threadIdx.x; k < a.n_diags; k += TB) s_off[k] = a.diag_off[k];
+    double *const s_shape = acc_sm + MW * TB * (STAGE ? 1 + CV : 1);
+    if constexpr (CLS)
+        for (int k = threadIdx.x; k < a.n_shapes * kShapeStride<DIM>; k += TB) s_shape[k] = a.shape_tab[k];
     __syncthreads();
     double res_v[2] = {0.0, 0.0};   // RES: this row's (r.r, b.b)
     do {   // one pass; break = this thread has no row (every thread reaches the RES reduction)
@@ -305,7 +337,7 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
         break;
     }
     double *acc = acc_sm + threadIdx.x;
-    double *colv = acc_sm + MW * TB + threadIdx.x;   // column k, component c at colv[(k * NV + c) * TB]
+    double *colv = acc_sm + MW * TB + threadIdx.x;   // column k, component c at colv[(k * CV + c) * TB]
     for (int k = 0; k < width; ++k) acc[k * TB] = 0.0;
     const int dpos = a.diag_pos[i];
 
@@ -336,8 +368,10 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
                     if (k < width) {
                         int c = dia ? i + s_off[k] : __ldg(a.cols + vb + kstride * k);
                         c = c < 0 ? 0 : (c > last ? last : c);
+                        if constexpr (!CLS) {
 #pragma unroll
-                        for (int d = 0; d < DIM; ++d) xv[g][d] = __ldg(a.coords + (int64_t)DIM * c + d);
+                            for (int d = 0; d < DIM; ++d) xv[g][d] = __ldg(a.coords + (int64_t)DIM * c + d);
+                        }
                         kv[g] = __ldg(a.K + c);
                     }
                 }
@@ -345,9 +379,11 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
                 for (int g = 0; g < CG; ++g) {
                     const int k = k0 + g;
                     if (k < width) {
+                        if constexpr (!CLS) {
 #pragma unroll
-                        for (int d = 0; d < DIM; ++d) colv[(k * NV + d) * TB] = xv[g][d];
-                        colv[(k * NV + DIM) * TB] = kv[g];
+                            for (int d = 0; d < DIM; ++d) colv[(k * CV + d) * TB] = xv[g][d];
+                        }
+                        colv[(k * CV + CV - 1) * TB] = kv[g];
                     }
                 }
             }
@@ -386,43 +422,63 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
                 for (int j = 0; j < NV; ++j) {
                     const int kp = (packed >> (2 + 6 * j)) & 63;
                     if constexpr (STAGE) {
+                        if constexpr (!CLS) {
 #pragma unroll
-                        for (int d = 0; d < DIM; ++d) X[j][d] = colv[(kp * NV + d) * TB];
-                        Kv[j] = colv[(kp * NV + DIM) * TB];
+                            for (int d = 0; d < DIM; ++d) X[j][d] = colv[(kp * CV + d) * TB];
+                        }
+                        Kv[j] = colv[(kp * CV + CV - 1) * TB];
                     } else {
                         const int col = i + s_off[kp];
+                        if constexpr (!CLS) {
 #pragma unroll
-                        for (int d = 0; d < DIM; ++d) X[j][d] = __ldg(a.coords + (int64_t)DIM * col + d);
+                            for (int d = 0; d < DIM; ++d) X[j][d] = __ldg(a.coords + (int64_t)DIM * col + d);
+                        }
                         Kv[j] = __ldg(a.K + col);
                     }
                 }
-                double G[DIM][NV], detJ;
-                p1_geometry_xyz<DIM>(X, G, detJ);
                 double Kbar = 0.0;
 #pragma unroll
                 for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], Kv[j], Kbar);
                 if constexpr (KSM != 0) Kbar *= kse[c];
-                const double kd = Kbar * detJ;
-                const double Ml = a.mcoef[li] * detJ;
-                double gli[DIM];
+                if constexpr (CLS) {
+                    const double *sh = s_shape + (packed >> kShapeShift<DIM>) * kShapeStride<DIM>;
+                    const double detJ = sh[0];
+                    const double kd = Kbar * detJ;
+                    const double Ml = a.mcoef[li] * detJ;
+                    const double *ggl = sh + 1 + li * NV;
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    double g = G[d][0];
+                    for (int j = 0; j < NV; ++j) {
+                        double v = kd * ggl[j];
+                        if (j == li) v += inv_dt * (Ml * Ci);
+                        const int kpos = (packed >> (2 + 6 * j)) & 63;
+                        acc[kpos * TB] += v;
+                    }
+                    bsum += -kd * sh[1 + NV * NV + li] - inv_dt * (Ml * storage);
+                } else {
+                    double G[DIM][NV], detJ;
+                    p1_geometry_xyz<DIM>(X, G, detJ);
+                    const double kd = Kbar * detJ;
+                    const double Ml = a.mcoef[li] * detJ;
+                    double gli[DIM];
 #pragma unroll
-                    for (int j = 1; j < NV; ++j) g = li == j ? G[d][j] : g;
-                    gli[d] = g;
+                    for (int d = 0; d < DIM; ++d) {
+                        double g = G[d][0];
+#pragma unroll
+                        for (int j = 1; j < NV; ++j) g = li == j ? G[d][j] : g;
+                        gli[d] = g;
+                    }
+#pragma unroll
+                    for (int j = 0; j < NV; ++j) {
+                        double gg = 0.0;
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) gg = fma(gli[d], G[d][j], gg);
+                        double v = kd * gg;
+                        if (j == li) v += inv_dt * (Ml * Ci);
+                        const int kpos = (packed >> (2 + 6 * j)) & 63;
+                        acc[kpos * TB] += v;
+                    }
+                    bsum += -kd * gli[DIM - 1] - inv_dt * (Ml * storage);
                 }
-#pragma unroll
-                for (int j = 0; j < NV; ++j) {
-                    double gg = 0.0;
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) gg = fma(gli[d], G[d][j], gg);
-                    double v = kd * gg;
-                    if (j == li) v += inv_dt * (Ml * Ci);
-                    const int kpos = (packed >> (2 + 6 * j)) & 63;
-                    acc[kpos * TB] += v;
-                }
-                bsum += -kd * gli[DIM - 1] - inv_dt * (Ml * storage);
             }
         }
         rhs_i = bsum;
@@ -508,22 +564,24 @@ void quadrature_constants(int dim, const double *Q, const double *W, int nq, dou
     }
 }
 
-template <int DIM, int MW, bool STAGE, int TB, int MINB>
+template <int DIM, int MW, bool STAGE, int TB, int MINB, bool CLS>
 static void launch_rows(const RichardsAsmArgs &a, int ksm, int n_slices, bool res, cudaStream_t st) {
     const int blocks = (n_slices * kSlice + TB - 1) / TB;
-    const size_t smem = (size_t)MW * TB * sizeof(double) * (STAGE ? 1 + (DIM + 1) : 1);
+    const int cv = CLS ? 1 : DIM + 1;
+    const size_t smem = (size_t)MW * TB * sizeof(double) * (STAGE ? 1 + cv : 1) +
+                        (CLS ? (size_t)a.n_shapes * kShapeStride<DIM> * sizeof(double) : 0);
     auto run = [&](auto kfn) {
         if (smem > 48 * 1024) cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kfn<<<blocks, TB, smem, st>>>(a);
     };
     if (res) {
-        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, true>);
-        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, true>);
-        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, true>);
+        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, true, CLS>);
+        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, true, CLS>);
+        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, true, CLS>);
     } else {
-        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, false>);
-        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, false>);
-        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, false>);
+        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, false, CLS>);
+        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, false, CLS>);
+        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, false, CLS>);
     }
 }
 
@@ -537,12 +595,212 @@ int richards_assembly_blocks(const wspm_mesh *mesh, const wspm_pattern *pat) {
     return (rows + tb - 1) / tb;
 }
 
+// ---- element shapes (plan time) -------------------------------------------------
+// Distinct Jacobians by their bits, in an open-addressing table of kShapeSlots
+// slots (state 0 free, 1 being written, 2 ready; keys are the Jacobian's bits).
+// Every wait and probe sequence is bounded; a table that overflows, or a wait that
+// gives up, sets the overflow word and the shape path is not used.
+constexpr int kShapeSlots = 2048;
+
+__device__ __forceinline__ unsigned int shape_ld_acquire(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long shape_mix(unsigned long long h) {
+    h ^= h >> 33; h *= 0xff51afd7ed558ccdULL; h ^= h >> 33; h *= 0xc4ceb9fe1a85ec53ULL; h ^= h >> 33;
+    return h;
+}
+
+template <int DIM>
+__global__ void shape_insert_kernel(wspm_mesh mesh, unsigned int *state, unsigned long long *keys,
+                                    uint16_t *elem_slot, int *meta) {
+    constexpr int NV = DIM + 1, NK = DIM * DIM;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < mesh.n_elems; e += gridDim.x * blockDim.x) {
+        double X[NV][DIM];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            const int v = mesh.conn[(int64_t)NV * e + j];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) X[j][d] = mesh.coords[(int64_t)DIM * v + d];
+        }
+        double J[DIM][DIM];
+        p1_jacobian<DIM>(X, J);
+        unsigned long long kb[NK], h = 0x9e3779b97f4a7c15ULL;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) {
+                kb[r * DIM + c] = (unsigned long long)__double_as_longlong(J[r][c]);
+                h = shape_mix(h ^ kb[r * DIM + c]);
+            }
+        int found = -1;
+        for (int probe = 0; probe < kShapeSlots && found < 0; ++probe) {
+            const int sl = (int)((h + (unsigned long long)probe) & (kShapeSlots - 1));
+            unsigned int stv = shape_ld_acquire(state + sl);
+            if (stv == 0u && atomicCAS(state + sl, 0u, 1u) == 0u) {
+#pragma unroll
+                for (int q = 0; q < NK; ++q) keys[(int64_t)sl * NK + q] = kb[q];
+                __threadfence();
+                atomicExch(state + sl, 2u);
+                found = sl;
+                break;
+            }
+            long long spins = 0;
+            while ((stv = shape_ld_acquire(state + sl)) != 2u) {
+                if (++spins > 4000000LL) { atomicExch(meta + 1, 1); return; }
+                __nanosleep(32);
+            }
+            bool eq = true;
+#pragma unroll
+            for (int q = 0; q < NK; ++q) eq = eq && __ldcg(keys + (int64_t)sl * NK + q) == kb[q];
+            if (eq) found = sl;
+        }
+        if (found < 0) { atomicExch(meta + 1, 1); return; }
+        elem_slot[e] = (uint16_t)found;
+    }
+}
+
+// One block: shape ids in slot order, and each shape's entry of the table.
+template <int DIM>
+__global__ void shape_table_kernel(const unsigned int *state, const unsigned long long *keys, int *slot_shape,
+                                   int *meta, double *table, int max_shapes) {
+    constexpr int NV = DIM + 1, NK = DIM * DIM;
+    __shared__ int s_count;
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int sl = 0; sl < kShapeSlots; ++sl) {
+            if (state[sl] == 2u) slot_shape[sl] = c++;
+            else slot_shape[sl] = -1;
+        }
+        meta[0] = c;
+        if (c > max_shapes) meta[1] = 1;
+        s_count = c;
+    }
+    __syncthreads();
+    if (s_count > max_shapes) return;
+    for (int sl = threadIdx.x; sl < kShapeSlots; sl += blockDim.x) {
+        const int id = slot_shape[sl];
+        if (id < 0) continue;
+        double J[DIM][DIM];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) J[r][c] = __longlong_as_double((long long)keys[(int64_t)sl * NK + r * DIM + c]);
+        double G[DIM][NV], detJ;
+        p1_geometry_j<DIM>(J, G, detJ);
+        double *t = table + (int64_t)id * kShapeStride<DIM>;
+        t[0] = detJ;
+#pragma unroll
+        for (int li = 0; li < NV; ++li) {
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+                double gg = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) gg = fma(G[d][li], G[d][j], gg);
+                t[1 + li * NV + j] = gg;
+            }
+            t[1 + NV * NV + li] = G[DIM - 1][li];
+        }
+    }
+}
+
+// Incidence words with the element's shape id above the position fields.
+template <int DIM>
+__global__ void shape_words_kernel(int n_slices, const int64_t *__restrict__ inc_ptr,
+                                   const int32_t *__restrict__ inc_width, const int32_t *__restrict__ inc_elem,
+                                   const uint32_t *__restrict__ inc_slots, const uint16_t *__restrict__ elem_slot,
+                                   const int *__restrict__ slot_shape, uint32_t *words) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = i >> 5, lane = i & 31;
+    if (s >= n_slices) return;
+    const int64_t ib = inc_ptr[s] + lane;
+    const int w = inc_width[s];
+    for (int k = 0; k < w; ++k) {
+        const int64_t o = ib + (int64_t)kSlice * k;
+        const int e = inc_elem[o];
+        uint32_t word = inc_slots[o];
+        if (e >= 0) word |= (uint32_t)slot_shape[elem_slot[e]] << kShapeShift<DIM>;
+        words[o] = word;
+    }
+}
+
+// Layout of the caller's shape buffer (bytes, 256-aligned parts): words
+// [n_slices*32*max_inc] u32, element slots [n_elems] u16, slot states
+// [kShapeSlots] u32, keys [kShapeSlots * dim^2] u64, slot shapes [kShapeSlots]
+// i32, meta [64] i32, table [kMaxShapes * stride] f64.
+struct ShapeBuffer {
+    uint32_t *words; uint16_t *elem_slot; unsigned int *state; unsigned long long *keys; int *slot_shape;
+    int *meta; double *table; int64_t bytes;
+};
+static int64_t align256(int64_t b) { return (b + 255) & ~int64_t(255); }
+static ShapeBuffer carve_shapes(void *base, const wspm_mesh *mesh, const wspm_pattern *pat) {
+    ShapeBuffer sb;
+    char *p = (char *)base;
+    int64_t off = 0;
+    const int dim = mesh->dim;
+    auto take = [&](int64_t bytes) { char *q = p ? p + off : nullptr; off += align256(bytes); return q; };
+    sb.words = (uint32_t *)take((int64_t)pat->n_slices * kSlice * (pat->max_inc > 0 ? pat->max_inc : 1) * 4);
+    sb.elem_slot = (uint16_t *)take((int64_t)mesh->n_elems * 2);
+    sb.state = (unsigned int *)take((int64_t)kShapeSlots * 4);
+    sb.keys = (unsigned long long *)take((int64_t)kShapeSlots * dim * dim * 8);
+    sb.slot_shape = (int *)take((int64_t)kShapeSlots * 4);
+    sb.meta = (int *)take(64 * 4);
+    sb.table = (double *)take((int64_t)(dim == 2 ? kMaxShapes<2> * kShapeStride<2> : kMaxShapes<3> * kShapeStride<3>) * 8);
+    sb.bytes = off;
+    return sb;
+}
+
+int64_t richards_shape_bytes(const wspm_mesh *mesh, const wspm_pattern *pat) {
+    if (!mesh || !pat || (mesh->dim != 2 && mesh->dim != 3)) return -1;
+    return carve_shapes(nullptr, mesh, pat).bytes;
+}
+
+// Builds the shape words and table in `buf` (synchronous, plan creation).  Returns
+// the number of shapes, or 0 when the mesh has too many (the caller then uses the
+// geometry-computing kernel) or anything failed.
+int richards_build_shapes(const wspm_mesh *mesh, const wspm_pattern *pat, void *buf, const uint32_t **words,
+                          const double **table) {
+    if (!mesh || !pat || !buf || mesh->n_elems <= 0 || pat->n_slices <= 0 || !pat->inc_slots || !pat->inc_elem)
+        return 0;
+    if (mesh->dim != 2 && mesh->dim != 3) return 0;
+    if (pat->max_width > 63) return 0;
+    const ShapeBuffer sb = carve_shapes(buf, mesh, pat);
+    if (cudaMemset(sb.state, 0, (size_t)kShapeSlots * 4) != cudaSuccess) return 0;
+    if (cudaMemset(sb.meta, 0, 64 * 4) != cudaSuccess) return 0;
+    const int blocks = (int)((mesh->n_elems + 255) / 256 < 148 * 8 ? (mesh->n_elems + 255) / 256 : 148 * 8);
+    const int nsw = (pat->n_slices * kSlice + 255) / 256;
+    if (mesh->dim == 2) {
+        shape_insert_kernel<2><<<blocks, 256>>>(*mesh, sb.state, sb.keys, sb.elem_slot, sb.meta);
+        shape_table_kernel<2><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table, kMaxShapes<2>);
+    } else {
+        shape_insert_kernel<3><<<blocks, 256>>>(*mesh, sb.state, sb.keys, sb.elem_slot, sb.meta);
+        shape_table_kernel<3><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table, kMaxShapes<3>);
+    }
+    int meta[2] = {0, 1};
+    if (cudaGetLastError() != cudaSuccess || cudaMemcpy(meta, sb.meta, sizeof(meta), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return 0;
+    if (meta[1] != 0 || meta[0] <= 0) return 0;
+    if (mesh->dim == 2)
+        shape_words_kernel<2><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
+                                            pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
+    else
+        shape_words_kernel<3><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
+                                            pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return 0;
+    *words = sb.words;
+    *table = sb.table;
+    return meta[0];
+}
+
 static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_pattern *pat,
                                          const double *theta_m, const double *theta_n, const double *h_m,
                                          const double *K, const double *C, const double *Ks_elem,
                                          const double *Ks_inc, const double s[4], const double mc[4], double dt,
                                          const double *dt_dev, const double *bc_val, double *vals, float *vals32,
-                                         double *rhs, double *dinv, const RefineStart *res, cudaStream_t st) {
+                                         double *rhs, double *dinv, const RefineStart *res, const uint32_t *shape_words,
+                                         const double *shape_tab, int n_shapes, cudaStream_t st) {
     RichardsAsmArgs a;
     const bool fused = res != nullptr;
     if (fused) a.res = *res;
@@ -560,22 +818,41 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     a.vals = vals; a.vals32 = vals32; a.rhs = rhs; a.dinv = dinv;
     a.diag_off = pat->diag_offsets;
     a.cols = pat->cols;
+    a.shape_tab = nullptr;
+    a.n_shapes = 0;
     if (pat->max_width > 63) return WSPM_UNSUPPORTED;      // the incidence word holds 6-bit row positions
     const int ksm = Ks_inc ? 2 : (Ks_elem ? 1 : 0);
     const int ns = pat->n_slices;
     const int mw = pat->max_width;
+    // the shape path where the plan found few element shapes (its words carry the shape ids)
+    const bool cls = shape_words && shape_tab && n_shapes > 0 && mw <= 16;
+    if (cls) {
+        a.inc_slots = shape_words;
+        a.shape_tab = shape_tab;
+        a.n_shapes = n_shapes;
+    }
     // launch shapes measured on the 1024^2 triangle and 96^3 Kuhn-tetrahedron grids (B200)
     if (mesh->dim == 2) {
-        if (mw <= 8) launch_rows<2, 8, true, 256, 3>(a, ksm, ns, fused, st);
-        else if (mw <= 16) launch_rows<2, 16, true, 128, 1>(a, ksm, ns, fused, st);
-        else if (mw <= 32) launch_rows<2, 32, true, 64, 1>(a, ksm, ns, fused, st);
-        else launch_rows<2, 64, true, 32, 1>(a, ksm, ns, fused, st);
+        if (mw <= 8) {
+            if (cls) launch_rows<2, 8, true, 256, 5, true>(a, ksm, ns, fused, st);
+            else launch_rows<2, 8, true, 256, 3, false>(a, ksm, ns, fused, st);
+        } else if (mw <= 16) {
+            if (cls) launch_rows<2, 16, true, 128, 2, true>(a, ksm, ns, fused, st);
+            else launch_rows<2, 16, true, 128, 1, false>(a, ksm, ns, fused, st);
+        } else if (mw <= 32) launch_rows<2, 32, true, 64, 1, false>(a, ksm, ns, fused, st);
+        else launch_rows<2, 64, true, 32, 1, false>(a, ksm, ns, fused, st);
     } else {
-        if (pat->n_diags > 0 && mw <= 16) launch_rows<3, 16, false, 128, 8>(a, ksm, ns, fused, st);
-        else if (mw <= 8) launch_rows<3, 8, true, 128, 1>(a, ksm, ns, fused, st);
-        else if (mw <= 16) launch_rows<3, 16, true, 128, 1>(a, ksm, ns, fused, st);
-        else if (mw <= 32) launch_rows<3, 32, true, 64, 1>(a, ksm, ns, fused, st);
-        else launch_rows<3, 64, true, 32, 1>(a, ksm, ns, fused, st);
+        if (pat->n_diags > 0 && mw <= 16) {
+            if (cls) launch_rows<3, 16, false, 128, 8, true>(a, ksm, ns, fused, st);
+            else launch_rows<3, 16, false, 128, 8, false>(a, ksm, ns, fused, st);
+        } else if (mw <= 8) {
+            if (cls) launch_rows<3, 8, true, 128, 2, true>(a, ksm, ns, fused, st);
+            else launch_rows<3, 8, true, 128, 1, false>(a, ksm, ns, fused, st);
+        } else if (mw <= 16) {
+            if (cls) launch_rows<3, 16, true, 128, 2, true>(a, ksm, ns, fused, st);
+            else launch_rows<3, 16, true, 128, 1, false>(a, ksm, ns, fused, st);
+        } else if (mw <= 32) launch_rows<3, 32, true, 64, 1, false>(a, ksm, ns, fused, st);
+        else launch_rows<3, 64, true, 32, 1, false>(a, ksm, ns, fused, st);
     }
     if (fused) refine_start_kernel<<<1, 1024, 0, st>>>(*res, richards_assembly_blocks(mesh, pat));
     return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
@@ -587,7 +864,7 @@ int launch_richards_assembly(const wspm_mesh *mesh, const wspm_pattern *pat, con
                              const double *bc_val, double *vals, float *vals32, double *rhs, double *dinv,
                              cudaStream_t st) {
     return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, nullptr, s, mc, dt,
-                                         nullptr, bc_val, vals, vals32, rhs, dinv, nullptr, st);
+                                         nullptr, bc_val, vals, vals32, rhs, dinv, nullptr, nullptr, nullptr, 0, st);
 }
 
 int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
@@ -595,9 +872,11 @@ int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *p
                                     const double *Ks_elem, const double *Ks_inc, const double s[4],
                                     const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
                                     float *vals32, double *rhs, double *dinv, const RefineStart *res,
+                                    const uint32_t *shape_words, const double *shape_tab, int n_shapes,
                                     cudaStream_t st) {
     return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, Ks_inc, s, mc, 1.0,
-                                         dt_dev, bc_val, vals, vals32, rhs, dinv, res, st);
+                                         dt_dev, bc_val, vals, vals32, rhs, dinv, res, shape_words, shape_tab,
+                                         n_shapes, st);
 }
 
 int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st) {

@@ -33,8 +33,12 @@ int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *p
                                     const double *Ks_elem, const double *Ks_inc, const double s[4],
                                     const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
                                     float *vals32, double *rhs, double *dinv, const RefineStart *res,
+                                    const uint32_t *shape_words, const double *shape_tab, int n_shapes,
                                     cudaStream_t st);
 int richards_assembly_blocks(const wspm_mesh *mesh, const wspm_pattern *pat);
+int64_t richards_shape_bytes(const wspm_mesh *mesh, const wspm_pattern *pat);
+int richards_build_shapes(const wspm_mesh *mesh, const wspm_pattern *pat, void *buf, const uint32_t **words,
+                          const double **table);
 unsigned long long richards_dia_live_mask(const wspm_mesh *mesh, const wspm_pattern *pat, unsigned long long *word);
 int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st);
 
@@ -313,6 +317,11 @@ struct PicardPlan {
     float *x32 = nullptr, *dinv32 = nullptr;
     double *Ks_inc = nullptr;   // Ks_elem in incidence order (caller's buffer), refreshed at every step start
     unsigned long long live = ~0ull;   // DIA diagonals that can hold nonzeros (structural zeros skipped)
+    // element shapes (caller's buffer): incidence words tagged with shape ids and the shapes' geometric
+    // factors; n_shapes == 0 when the mesh has too many distinct Jacobians or no buffer was given
+    const uint32_t *shape_words = nullptr;
+    const double *shape_tab = nullptr;
+    int n_shapes = 0;
 };
 
 // The plan's matrix descriptor: the pattern with its structural-zero diagonals marked.
@@ -388,7 +397,8 @@ static int build_picard_graph(PicardPlan *P) {
         const bool fused = fuse_refine_start(P);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                         P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
-                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr, bs);
+                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr,
+                                        P->shape_words, P->shape_tab, P->n_shapes, bs);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           bs);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
@@ -494,7 +504,8 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
         const bool fused = fuse_refine_start(P);
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                         P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
-                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr, st);
+                                        d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr,
+                                        P->shape_words, P->shape_tab, P->n_shapes, st);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           st);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
@@ -582,6 +593,10 @@ extern "C" int64_t wspm_picard_workspace_doubles(int32_t n_rows, int32_t mixed) 
     return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
 
+extern "C" int64_t wspm_picard_shape_bytes(const wspm_mesh *mesh, const wspm_pattern *pat) {
+    return richards_shape_bytes(mesh, pat);
+}
+
 extern "C" int64_t wspm_picard_ks_inc_doubles(const wspm_pattern *pat) {
     if (!pat || pat->n_slices <= 0) return -1;
     return (int64_t)pat->n_slices * kSlice * (int64_t)(pat->max_inc > 0 ? pat->max_inc : 1);
@@ -639,6 +654,8 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     // structural zeros of the DIA layout, found once from the geometry (the first
     // partial-sum slot of the workspace serves as the scratch word)
     P->live = richards_dia_live_mask(&P->mesh, &P->pat, reinterpret_cast<unsigned long long *>(P->partials));
+    // element shapes, found once from the geometry (synchronous)
+    if (d.shapes) P->n_shapes = richards_build_shapes(&P->mesh, &P->pat, d.shapes, &P->shape_words, &P->shape_tab);
     int rc = build_picard_graph(P);
     if (rc != WSPM_OK) {
         delete P;
@@ -646,6 +663,25 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     }
     *plan_out = P;
     return WSPM_OK;
+}
+
+extern "C" int wspm_picard_assemble(void *plan, void *stream) {
+    if (!plan) return WSPM_BAD_ARG;
+    PicardPlan *P = (PicardPlan *)plan;
+    const wspm_picard_desc &d = P->d;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (P->Ks_inc) {
+        const int rc = launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, st);
+        if (rc != WSPM_OK) return rc;
+    }
+    return launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
+                                           P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
+                                           d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, nullptr, P->shape_words,
+                                           P->shape_tab, P->n_shapes, st);
+}
+
+extern "C" int32_t wspm_picard_shapes(void *plan) {
+    return plan ? ((const PicardPlan *)plan)->n_shapes : -1;
 }
 
 extern "C" int64_t wspm_picard_dia_live(void *plan) {

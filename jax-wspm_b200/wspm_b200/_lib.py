@@ -58,7 +58,7 @@ class WspmPicardDesc(ctypes.Structure):
                 ("K", c_void_p), ("C", c_void_p), ("theta_m", c_void_p),
                 ("vals", c_void_p), ("vals32", c_void_p), ("rhs", c_void_p), ("dinv", c_void_p),
                 ("work", c_void_p), ("work_doubles", c_int64), ("dt_dev", c_void_p),
-                ("result", c_void_p), ("result_f64", c_void_p), ("Ks_inc", c_void_p)]
+                ("result", c_void_p), ("result_f64", c_void_p), ("Ks_inc", c_void_p), ("shapes", c_void_p)]
 
 
 class WspmEnsemble(ctypes.Structure):
@@ -152,11 +152,14 @@ _SIGS = {
                                         c_int32, c_void_p, c_void_p]),
     "wspm_picard_workspace_doubles": (c_int64, [c_int32, c_int32]),
     "wspm_picard_ks_inc_doubles": (c_int64, [P(WspmPattern)]),
+    "wspm_picard_shape_bytes": (c_int64, [P(WspmMesh), P(WspmPattern)]),
     "wspm_picard_create": (c_int32, [P(WspmPicardDesc), P(c_void_p)]),
     "wspm_picard_step": (c_int32, [c_void_p, c_void_p]),
     "wspm_picard_step_host": (c_int32, [c_void_p, c_void_p]),
     "wspm_picard_destroy": (c_int32, [c_void_p]),
     "wspm_picard_dia_live": (c_int64, [c_void_p]),
+    "wspm_picard_shapes": (c_int32, [c_void_p]),
+    "wspm_picard_assemble": (c_int32, [c_void_p, c_void_p]),
     "wspm_pattern_build": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_int64, c_int32,
                                      P(P(WspmPatternHost))]),
     "wspm_pattern_free": (None, [P(WspmPatternHost)]),

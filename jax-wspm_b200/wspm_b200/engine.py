@@ -45,7 +45,10 @@ class PicardEngine:
     def __init__(self, dmesh, soil_model="vg", phi=(), Ks_elem=None, bc_val=None, solver="cg", precond="jacobi",
                  krylov_tol=1e-10, krylov_maxiter=100, restart=30, mixed=False, inner_tol=1e-4,
                  inner_maxiter=2000, refine_maxiter=20, picard_tol=1e-6, picard_maxiter=100, picard_relative=True,
-                 quad=None, neumann_nodes=None, neumann_flux=0.0, drainage_nodes=None):
+                 quad=None, neumann_nodes=None, neumann_flux=0.0, drainage_nodes=None, element_shapes=True):
+        """``element_shapes``: give the plan a buffer in which it records the mesh's distinct element Jacobians;
+        with few of them (structured grids) the assembly reads each element-row's geometric factors from a table
+        instead of recomputing them, with bitwise identical results."""
         if not isinstance(dmesh, DeviceMesh):
             raise TypeError("dmesh must be a DeviceMesh")
         self.dm = dm = dmesh
@@ -102,6 +105,13 @@ class PicardEngine:
         if self.Ks_elem is not None:        # Ks_elem in incidence order, refreshed by the step graph
             self.Ks_inc = torch.empty(int(lib.wspm_picard_ks_inc_doubles(ctypes.byref(dm.c_pat))), **f64)
             d.Ks_inc = self.Ks_inc.data_ptr()
+        # element shapes: the plan tags the incidence words with them when the mesh has few distinct Jacobians
+        self.shape_buf = None
+        if element_shapes:
+            nbytes = int(lib.wspm_picard_shape_bytes(ctypes.byref(dm.c_mesh), ctypes.byref(dm.c_pat)))
+            if nbytes > 0:
+                self.shape_buf = torch.empty(nbytes, dtype=torch.uint8, device=dm.device)
+                d.shapes = self.shape_buf.data_ptr()
         # boundary-edge rhs terms (Neumann flux, free drainage of water), applied after assembly
         self.neumann = BoundaryEdges(dm, neumann_nodes) if neumann_nodes is not None else None
         self.drainage = BoundaryEdges(dm, drainage_nodes) if drainage_nodes is not None else None
@@ -125,6 +135,16 @@ class PicardEngine:
             except Exception:
                 pass
             self.plan = None
+
+    def assemble(self):
+        """One assembly of the current system (vals, rhs, dinv; vals32 on a mixed plan) with the step's kernel."""
+        st = torch.cuda.current_stream()
+        check("picard_assemble", lib.wspm_picard_assemble(self.plan, ctypes.c_void_p(st.cuda_stream)))
+
+    def element_shape_count(self):
+        """Distinct element Jacobians the plan's assembly takes from its shape table (0: it recomputes every
+        element's geometry)."""
+        return int(lib.wspm_picard_shapes(self.plan))
 
     @property
     def live_diagonals(self):

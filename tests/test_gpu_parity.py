@@ -616,3 +616,51 @@ def test_engine_on_a_device_built_pattern_matches_host_built():
                            precond="jacobi", krylov_tol=1e-8, krylov_maxiter=5000, mixed=True)
         out.append(eng.run(-np.ones(len(pts)), 1e-4, 1e-3, fixed_dt=True, max_steps=2)["pressure_head"])
     np.testing.assert_array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("case", ["tri-binary", "tri-jitter", "tet-binary"])
+@pytest.mark.parametrize("mixed", [False, True])
+def test_element_shape_table_gives_bitwise_identical_steps(case, mixed):
+    """The plan's element-shape path (distinct element Jacobians found once; each element-row's geometric factors
+    read from a per-shape table) runs the same Picard steps bit for bit as the assembly that recomputes every
+    element's geometry: a grid with exact binary coordinates has 2 triangle shapes (6 Kuhn tetrahedra); a jittered
+    mesh has one shape per element, too many, and keeps the recomputing kernel."""
+    from wspm_b200.device import DeviceMesh, merge_dirichlet
+    from wspm_b200.engine import PicardEngine
+    rng = np.random.default_rng(7)
+    if case == "tri-binary":
+        pts, el = mesh.structured_triangles(64, 1.0)
+        want = 2
+    elif case == "tri-jitter":
+        pts, el = mesh.structured_triangles(40, 1.0)
+        inner = np.all((pts > 0) & (pts < 1), axis=1)
+        pts = pts.copy()
+        pts[inner] += rng.uniform(-0.2, 0.2, (int(inner.sum()), 2)) / 40
+        want = 0
+    else:
+        pts, el = mesh.kuhn_tetrahedra(8, 1.0)
+        want = 6
+    dim = pts.shape[1]
+    top = np.where(pts[:, dim - 1] == pts[:, dim - 1].max())[0]
+    Ks = 0.0922 * np.exp(rng.standard_normal(len(el)))
+    bc = merge_dirichlet(len(pts), [(top, -0.1)])
+    dm = DeviceMesh(pts, el)
+    runs, shapes, engines = [], [], []
+    for flag in (True, False):
+        eng = PicardEngine(dm, "vg", (3.35, 0.368, 0.102, 2.0, 0.5, 1.0), Ks_elem=Ks, bc_val=bc,
+                           solver="cg" if dim == 2 else "bicgstab", precond="jacobi", krylov_tol=1e-10,
+                           krylov_maxiter=5000, mixed=mixed, inner_tol=1e-5, inner_maxiter=5000,
+                           element_shapes=flag)
+        shapes.append(eng.element_shape_count())
+        runs.append(eng.run(-np.ones(len(pts)), 1e-3, 1.0, fixed_dt=True, max_steps=3))
+        engines.append(eng)
+    assert shapes == [want, 0]
+    np.testing.assert_array_equal(runs[0]["pressure_head"], runs[1]["pressure_head"])
+    assert list(runs[0]["iterations"]) == list(runs[1]["iterations"])
+    assert list(runs[0]["krylov_iterations"]) == list(runs[1]["krylov_iterations"])
+    # one assembly of each plan's current system (wspm_picard_assemble): the same arrays bit for bit
+    for eng in engines:
+        eng.assemble()
+    torch.cuda.synchronize()
+    for name in ("vals", "rhs", "dinv"):
+        assert torch.equal(getattr(engines[0], name), getattr(engines[1], name)), name
