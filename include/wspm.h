@@ -444,7 +444,9 @@ int64_t wspm_picard_dia_live(void *plan);
 int32_t wspm_picard_shapes(void *plan);
 /* One assembly of the plan's system at its current state (theta_m, h_m, K, C
  * and dt as the step left them; Dirichlet rows, 1/diag, the FP32 copy on a
- * mixed plan) with the kernel the step runs, the shape path included.
+ * mixed plan) with the kernel the step runs, the shape path included; Ks
+ * is taken in incidence order as gathered at plan creation or at the start
+ * of the last step.
  * Replaces assemble_global_matrices_sparse_re (src/numerics/
  * assembly_re_v2.py:62-166) for a caller that holds a plan.               */
 int wspm_picard_assemble(void *plan, void *stream);

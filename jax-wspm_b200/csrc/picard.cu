@@ -656,6 +656,12 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     P->live = richards_dia_live_mask(&P->mesh, &P->pat, reinterpret_cast<unsigned long long *>(P->partials));
     // element shapes, found once from the geometry (synchronous)
     if (d.shapes) P->n_shapes = richards_build_shapes(&P->mesh, &P->pat, d.shapes, &P->shape_words, &P->shape_tab);
+    // Ks in incidence order as of creation (every step refreshes it at its start)
+    if (P->Ks_inc && (launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, 0) != WSPM_OK ||
+                      cudaDeviceSynchronize() != cudaSuccess)) {
+        delete P;
+        return WSPM_CUDA_ERROR;
+    }
     int rc = build_picard_graph(P);
     if (rc != WSPM_OK) {
         delete P;
@@ -670,10 +676,6 @@ extern "C" int wspm_picard_assemble(void *plan, void *stream) {
     PicardPlan *P = (PicardPlan *)plan;
     const wspm_picard_desc &d = P->d;
     cudaStream_t st = (cudaStream_t)stream;
-    if (P->Ks_inc) {
-        const int rc = launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, st);
-        if (rc != WSPM_OK) return rc;
-    }
     return launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                            P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
                                            d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, nullptr, P->shape_words,
