@@ -1068,9 +1068,14 @@ __device__ __forceinline__ bool pcg_spmv_dia(int nl, int lo_i, int hi_i, const T
 }
 
 constexpr int kInitBatch = 8;   // rows per thread whose loads the start-up loops issue together
+// Threads per block of the pipelined kernel: for FP32 systems of at most 8 diagonals 32 warps per SM hide more
+// of the SpMV's gather latency than 16 (the compiler fits that instance in 64 registers without spills: 9.7 vs
+// 10.3 us per FP32 iteration at 1024^2); the other instances would spill at 64 registers and keep 512.
+template <typename T, int MW>
+constexpr int pcg_block() { return (sizeof(T) == 4 && MW <= 8) ? 1024 : kRcgBlock; }
 
 template <typename T, int MW, bool XS, bool WS>
-__global__ void __launch_bounds__(kRcgBlock, 1) pcg_resident_kernel(PcgArgs<T> a) {
+__global__ void __launch_bounds__(pcg_block<T, MW>(), 1) pcg_resident_kernel(PcgArgs<T> a) {
     using VT = Vec16<T>;
     using V = typename VT::V;
     constexpr int N = VT::N;
@@ -1376,7 +1381,7 @@ static cudaError_t pcg_launch(int grid, size_t smem, const PcgArgs<T> &a, cudaSt
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(kRcgBlock);
+    cfg.blockDim = dim3(pcg_block<T, MW>());
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
