@@ -243,6 +243,23 @@ def assembly_seconds(eng, reps=20):
     return e0.elapsed_time(e1) * 1e-3 / reps
 
 
+def spmv_seconds(dm, vals, x, flush, reps=10):
+    """Average duration (CUDA events, one per launch) of the stand-alone FP64 SpMV (wspm_spmv_f64) on the step's
+    matrix, L2 flushed before every launch (the matrix and both vectors would otherwise stay in L2)."""
+    import torch
+    from wspm_b200.device import spmv
+    spmv(dm, vals, x)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for a, b in ev:
+        flush()
+        a.record()
+        spmv(dm, vals, x)
+        b.record()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev) * 1e-3 / reps
+
+
 def assembly_public_seconds(eng, dm, reps=20):
     """The same through the plan-free entry point (wspm_assemble_richards), which recomputes every element's
     geometry (Ks gathered by element id, FP32 copy written)."""
@@ -774,6 +791,8 @@ def main():
     # the assembly is the HBM-streaming kernel of the step (SURVEY-style algorithmic bytes, per launch)
     t_asm = assembly_seconds(eng64)
     t_asm_public = assembly_public_seconds(engmx, dm)
+    t_spmv = spmv_seconds(dm, eng64.vals, eng64.x, flush)
+    b_spmv = nd * ld * 8 + 2 * N * 8      # every stored diagonal (the stand-alone SpMV reads all of them) + x + y
     b_asm = E * 12 + N * 16 + 2 * N * 8 + E * 8 + nnz * 8 + N * 8 + N * 8
     ms64 = allreduce_max(r64["ms"], world)
     msmx = allreduce_max(rmx["ms"], world)
@@ -838,7 +857,12 @@ def main():
                                   "element_shapes": eng64.element_shape_count(),
                                   "recomputing_geometry": {"entry": "wspm_assemble_richards (no plan; FP32 copy "
                                                                     "written)", "seconds": t_asm_public,
-                                                           "frac": b_asm / t_asm_public / 1e9 / peak_hbm}}},
+                                                           "frac": b_asm / t_asm_public / 1e9 / peak_hbm}},
+                     "spmv": {"kernel": "spmv_kernel (wspm_spmv_f64, DIA, FP64) on the step's matrix",
+                              "bound": "hbm", "bytes": b_spmv, "seconds": t_spmv,
+                              "achieved": b_spmv / t_spmv / 1e9, "peak": peak_hbm,
+                              "frac": b_spmv / t_spmv / 1e9 / peak_hbm,
+                              "l2_policy": "256 MiB write before every launch, one CUDA-event pair per launch"}},
         "clocks": clk.summary(),
     }
     if parity is not None:
