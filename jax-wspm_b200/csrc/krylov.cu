@@ -47,13 +47,99 @@ __global__ void __launch_bounds__(kBlock) spmv_kernel(Sell A, const T *__restric
     y[i] = sell_row<T, MW>(A, vals, i, [&](int c) { return __ldg(x + c); });
 }
 
-void spmv_f64(const Sell &A, const double *vals, const double *x, double *y, cudaStream_t st) {
+// 16-byte vectors: a thread owns NV consecutive rows (4 in FP32, 2 in FP64) so
+// every matrix diagonal and every per-row vector moves as one 16-byte access.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+    using V = float4;
+    static constexpr int N = 4;
+    __device__ static __forceinline__ void split(const float4 &v, float (&o)[4]) {
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+    __device__ static __forceinline__ float4 join(const float (&o)[4]) { return make_float4(o[0], o[1], o[2], o[3]); }
+};
+template <> struct Vec16<double> {
+    using V = double2;
+    static constexpr int N = 2;
+    __device__ static __forceinline__ void split(const double2 &v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
+    __device__ static __forceinline__ double2 join(const double (&o)[2]) { return make_double2(o[0], o[1]); }
+};
+
+// DIA SpMV: a thread owns 16 bytes of rows (2 in FP64, 4 in FP32); the live diagonals' offsets sit in shared
+// memory, and every value load and gather of the thread's rows is issued before the first product (the generic
+// kernel reads each offset from global memory before the gather that needs it).  Products in diagonal order,
+// like sell_row.
+template <typename T, int MW>
+__global__ void __launch_bounds__(kBlock) spmv_dia_kernel(Sell A, const T *__restrict__ vals, const T *__restrict__ x,
+                                                          T *__restrict__ y) {
+    using VT = Vec16<T>;
+    constexpr int N = VT::N;
+    __shared__ int s_off[MW];
+    __shared__ int64_t s_vo[MW];
+    __shared__ int s_nd;
+    if (threadIdx.x == 0) {
+        int nd = 0;
+        for (int k = 0; k < A.n_diags; ++k) {
+            if (!dia_live(A, k)) continue;
+            s_off[nd] = __ldg(A.diag_off + k);
+            s_vo[nd] = (int64_t)k * A.ld;
+            ++nd;
+        }
+        s_nd = nd;
+    }
+    __syncthreads();
+    const int nd = s_nd;
+    const int n = A.n_rows, last = n - 1;
+    const int i = N * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= n) return;
+    T e[MW][N], xv[MW][N];
+#pragma unroll
+    for (int k = 0; k < MW; ++k) {
+        if (k < nd) {
+            VT::split(__ldg(reinterpret_cast<const typename VT::V *>(vals + s_vo[k] + i)), e[k]);
+#pragma unroll
+            for (int q = 0; q < N; ++q) {
+                int c = i + q + s_off[k];
+                c = c < 0 ? 0 : (c > last ? last : c);
+                xv[k][q] = __ldg(x + c);
+            }
+        }
+    }
+    T w[N];
+#pragma unroll
+    for (int q = 0; q < N; ++q) w[q] = T(0);
+#pragma unroll
+    for (int k = 0; k < MW; ++k)
+        if (k < nd)
+#pragma unroll
+            for (int q = 0; q < N; ++q) w[q] = fma(e[k][q], xv[k][q], w[q]);
+    if (i + N <= n) {
+        *reinterpret_cast<typename VT::V *>(y + i) = VT::join(w);
+    } else {
+        for (int q = 0; q < N && i + q < n; ++q) y[i + q] = w[q];
+    }
+}
+
+template <typename T>
+static void spmv_launch(const Sell &A, const T *vals, const T *x, T *y, cudaStream_t st) {
+    // the DIA form needs 16-byte aligned values and output (ld and every diagonal start are multiples of 32 rows)
+    const bool aligned = ((((uintptr_t)vals) | ((uintptr_t)y)) % 16) == 0;
+    if (A.n_diags > 0 && A.n_diags <= 16 && aligned) {
+        const int threads = (A.n_rows + Vec16<T>::N - 1) / Vec16<T>::N;
+        const int blocks = (threads + kBlock - 1) / kBlock;
+        if (A.n_diags <= 8) spmv_dia_kernel<T, 8><<<blocks, kBlock, 0, st>>>(A, vals, x, y);
+        else spmv_dia_kernel<T, 16><<<blocks, kBlock, 0, st>>>(A, vals, x, y);
+        return;
+    }
     WSPM_WIDTH_DISPATCH(A.max_width,
-                        spmv_kernel<double, MW><<<(A.n_rows + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, vals, x, y));
+                        spmv_kernel<T, MW><<<(A.n_rows + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, vals, x, y));
+}
+
+void spmv_f64(const Sell &A, const double *vals, const double *x, double *y, cudaStream_t st) {
+    spmv_launch<double>(A, vals, x, y, st);
 }
 void spmv_f32(const Sell &A, const float *vals, const float *x, float *y, cudaStream_t st) {
-    WSPM_WIDTH_DISPATCH(A.max_width,
-                        spmv_kernel<float, MW><<<(A.n_rows + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, vals, x, y));
+    spmv_launch<float>(A, vals, x, y, st);
 }
 
 // ---------------------------------------------------------------- CG
@@ -382,23 +468,6 @@ __device__ __forceinline__ void reduce_partials_rows(const T *partials, int nb, 
     for (int j = 0; j < NV; ++j) out[j] = bc[j];
 }
 
-// 16-byte vectors: a thread owns NV consecutive rows (4 in FP32, 2 in FP64) so
-// every matrix diagonal and every per-row vector moves as one 16-byte access.
-template <typename T> struct Vec16;
-template <> struct Vec16<float> {
-    using V = float4;
-    static constexpr int N = 4;
-    __device__ static __forceinline__ void split(const float4 &v, float (&o)[4]) {
-        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
-    }
-    __device__ static __forceinline__ float4 join(const float (&o)[4]) { return make_float4(o[0], o[1], o[2], o[3]); }
-};
-template <> struct Vec16<double> {
-    using V = double2;
-    static constexpr int N = 2;
-    __device__ static __forceinline__ void split(const double2 &v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
-    __device__ static __forceinline__ double2 join(const double (&o)[2]) { return make_double2(o[0], o[1]); }
-};
 
 // Row i of A times z with the values and gathers of a group of diagonals in
 // flight at once, accumulated in diagonal order like sell_row_dot (used for

@@ -139,11 +139,14 @@ def test_assembly_with_dirichlet_rows_and_apply_dirichlet(layout):
     np.testing.assert_allclose(host(D.jacobi_dinv(dm, vals)), host(dinv), rtol=0)
 
 
+@pytest.mark.parametrize("kind", ["tet", "tri"])
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 @pytest.mark.parametrize("layout", ["dia", "sell"])
-def test_spmv(dtype, layout):
+def test_spmv(dtype, layout, kind):
+    """SpMV against SciPy: DIA (the 16-byte-per-thread kernel: 15 diagonals for tetrahedra, 7 for triangles; the
+    triangle mesh has a row count that is not a multiple of the 16-byte group) and SELL."""
     rng = np.random.default_rng(3)
-    pts, el = mesh.kuhn_tetrahedra(7)
+    pts, el = mesh.kuhn_tetrahedra(7) if kind == "tet" else mesh.structured_triangles(30, 1.0)
     D = dev()
     dm = D.DeviceMesh(pts, el, layout=layout)
     data = rng.standard_normal(dm.pattern.nnz)
