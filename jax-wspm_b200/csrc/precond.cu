@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(1024) tri_sweep_kernel(Sell A, const double *_
 // `vals`): the strict lower part holds L (unit diagonal implied), the rest U.  A
 // zero pivot u_kk is taken as 1 (the reference's convention for zero diagonals).
 // Not the reference's `ilu` (which never updates a pivot, see create_ilu0
-// above): this is the factorization SURVEY-style "true ILU(0)" names.
+// above): this is the textbook incomplete LU with zero fill.
 
 // position q of column j in row i, -1 when the row does not hold it
 __device__ __forceinline__ int entry_index(const Sell &A, int i, int j) {
