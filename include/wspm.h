@@ -408,9 +408,12 @@ typedef struct wspm_picard_desc {
                                   bytes of device memory: the plan records the
                                   mesh's distinct element Jacobians (bitwise)
                                   there at creation, and when they are few
-                                  (<= 256 triangle / 64 tetrahedron shapes) its
-                                  assembly reads each element-row's geometric
-                                  factors from a per-shape table instead of
+                                  (<= 256 triangle / 64 tetrahedron shapes, the
+                                  table in shared memory; or, for tetrahedra
+                                  with at most 16 stored entries per row, up to
+                                  16,384 shapes in a global table) its assembly
+                                  reads each element-row's geometric factors
+                                  from the per-shape table instead of
                                   recomputing them (same values bit for bit);
                                   NULL: always recompute                     */
 } wspm_picard_desc;

@@ -69,9 +69,20 @@ struct RichardsAsmArgs {
 // the geometric factors of every element-row from a small table instead of
 // recomputing them.  Entry of a shape: detJ, then gg[li][j] = G[:,li] . G[:,j]
 // (NV x NV, the fma chain of the row kernel), then G[DIM-1][li] (NV values).
+//
+// Two forms of the tagged incidence words.  Mode 1: the words keep their 6-bit
+// row positions, the shape id sits above them (12 bits in 2D, 6 in 3D) and the
+// table (at most 256 triangle / 64 tetrahedron shapes) is copied into shared
+// memory.  Mode 2, for patterns with at most 16 entries per row: the row
+// positions are repacked into 4 bits each, the id takes the 14 (3D) bits above
+// them, and the table (up to 16,384 shapes; 1.7 MB for the 10,368 tetrahedra of
+// a 96^3 grid with coordinates i/96) is read from global memory, where it stays
+// in L2.
 template <int DIM> constexpr int kShapeStride = 1 + (DIM + 1) * (DIM + 1) + (DIM + 1);
-template <int DIM> constexpr int kShapeShift = 2 + 6 * (DIM + 1);   // shape id above the incidence word's fields
-template <int DIM> constexpr int kMaxShapes = DIM == 2 ? 256 : 64;
+template <int DIM, int SHP> constexpr int kPosBits = SHP == 2 ? 4 : 6;
+template <int DIM, int SHP> constexpr int kShapeShift = 2 + kPosBits<DIM, SHP> * (DIM + 1);
+template <int DIM> constexpr int kMaxShapes = DIM == 2 ? 256 : 64;          // mode 1
+constexpr int kMaxShapesGlobal = 16384;                                      // mode 2 (3D: 14 bits)
 
 template <int DIM>
 __device__ __forceinline__ void p1_geometry(const double *__restrict__ coords, const int (&nd)[DIM + 1],
@@ -301,12 +312,15 @@ __global__ void incidence_gather_kernel(int n_slices, const int64_t *__restrict_
 // The element-local row index li selects a column of G by selects: an indexed
 // register array would live in local memory.
 //
-// CLS: the incidence words carry the element's shape id (kShapeShift) and the
-// geometric factors come from the shape table, copied into shared memory once
-// per block; the column stage then holds K only.  Every value and every
-// accumulation order are those of the geometry-computing form.
-template <int DIM, int MW, int KSM, bool STAGE, int TB, int MINB, bool RES, bool CLS>
+// SHP (element shapes; 0: none): the incidence words carry the element's shape
+// id and the geometric factors come from the shape table -- copied into shared
+// memory once per block (1) or read from global memory (2); the column stage
+// then holds K only.  Every value and every accumulation order are those of the
+// geometry-computing form.
+template <int DIM, int MW, int KSM, bool STAGE, int TB, int MINB, bool RES, int SHP>
 __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs a) {
+    constexpr bool CLS = SHP != 0;
+    constexpr int PB = kPosBits<DIM, SHP>, PM = (1 << PB) - 1;   // row-position field of the incidence word
     constexpr int NV = DIM + 1;
     constexpr int CH = STAGE ? 4 : 1;   // incidences whose loads are issued together
     constexpr int CV = CLS ? 1 : NV;    // staged values per column (K; or coordinates and K)
@@ -318,7 +332,7 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
     if (dia)
         for (int k = threadIdx.x; k < a.n_diags; k += TB) s_off[k] = a.diag_off[k];
     double *const s_shape = acc_sm + MW * TB * (STAGE ? 1 + CV : 1);
-    if constexpr (CLS)
+    if constexpr (SHP == 1)
         for (int k = threadIdx.x; k < a.n_shapes * kShapeStride<DIM>; k += TB) s_shape[k] = a.shape_tab[k];
     __syncthreads();
     double res_v[2] = {0.0, 0.0};   // RES: this row's (r.r, b.b)
@@ -420,7 +434,7 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
                 double X[NV][DIM], Kv[NV];
 #pragma unroll
                 for (int j = 0; j < NV; ++j) {
-                    const int kp = (packed >> (2 + 6 * j)) & 63;
+                    const int kp = (packed >> (2 + PB * j)) & PM;
                     if constexpr (STAGE) {
                         if constexpr (!CLS) {
 #pragma unroll
@@ -441,19 +455,29 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
                 for (int j = 0; j < NV; ++j) Kbar = fma(a.s[j], Kv[j], Kbar);
                 if constexpr (KSM != 0) Kbar *= kse[c];
                 if constexpr (CLS) {
-                    const double *sh = s_shape + (packed >> kShapeShift<DIM>) * kShapeStride<DIM>;
-                    const double detJ = sh[0];
+                    const int64_t so = (int64_t)(packed >> kShapeShift<DIM, SHP>) * kShapeStride<DIM>;
+                    double detJ, ggl[NV], glast;
+                    if constexpr (SHP == 1) {
+                        detJ = s_shape[so];
+#pragma unroll
+                        for (int j = 0; j < NV; ++j) ggl[j] = s_shape[so + 1 + li * NV + j];
+                        glast = s_shape[so + 1 + NV * NV + li];
+                    } else {
+                        detJ = __ldg(a.shape_tab + so);
+#pragma unroll
+                        for (int j = 0; j < NV; ++j) ggl[j] = __ldg(a.shape_tab + so + 1 + li * NV + j);
+                        glast = __ldg(a.shape_tab + so + 1 + NV * NV + li);
+                    }
                     const double kd = Kbar * detJ;
                     const double Ml = a.mcoef[li] * detJ;
-                    const double *ggl = sh + 1 + li * NV;
 #pragma unroll
                     for (int j = 0; j < NV; ++j) {
                         double v = kd * ggl[j];
                         if (j == li) v += inv_dt * (Ml * Ci);
-                        const int kpos = (packed >> (2 + 6 * j)) & 63;
+                        const int kpos = (packed >> (2 + PB * j)) & PM;
                         acc[kpos * TB] += v;
                     }
-                    bsum += -kd * sh[1 + NV * NV + li] - inv_dt * (Ml * storage);
+                    bsum += -kd * glast - inv_dt * (Ml * storage);
                 } else {
                     double G[DIM][NV], detJ;
                     p1_geometry_xyz<DIM>(X, G, detJ);
@@ -474,7 +498,7 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
                         for (int d = 0; d < DIM; ++d) gg = fma(gli[d], G[d][j], gg);
                         double v = kd * gg;
                         if (j == li) v += inv_dt * (Ml * Ci);
-                        const int kpos = (packed >> (2 + 6 * j)) & 63;
+                        const int kpos = (packed >> (2 + PB * j)) & PM;
                         acc[kpos * TB] += v;
                     }
                     bsum += -kd * gli[DIM - 1] - inv_dt * (Ml * storage);
@@ -564,24 +588,25 @@ void quadrature_constants(int dim, const double *Q, const double *W, int nq, dou
     }
 }
 
-template <int DIM, int MW, bool STAGE, int TB, int MINB, bool CLS>
+template <int DIM, int MW, bool STAGE, int TB, int MINB, int SHP>
 static void launch_rows(const RichardsAsmArgs &a, int ksm, int n_slices, bool res, cudaStream_t st) {
+    constexpr bool CLS = SHP != 0;
     const int blocks = (n_slices * kSlice + TB - 1) / TB;
     const int cv = CLS ? 1 : DIM + 1;
     const size_t smem = (size_t)MW * TB * sizeof(double) * (STAGE ? 1 + cv : 1) +
-                        (CLS ? (size_t)a.n_shapes * kShapeStride<DIM> * sizeof(double) : 0);
+                        (SHP == 1 ? (size_t)a.n_shapes * kShapeStride<DIM> * sizeof(double) : 0);
     auto run = [&](auto kfn) {
         if (smem > 48 * 1024) cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kfn<<<blocks, TB, smem, st>>>(a);
     };
     if (res) {
-        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, true, CLS>);
-        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, true, CLS>);
-        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, true, CLS>);
+        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, true, SHP>);
+        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, true, SHP>);
+        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, true, SHP>);
     } else {
-        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, false, CLS>);
-        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, false, CLS>);
-        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, false, CLS>);
+        if (ksm == 2) run(richards_rows_kernel<DIM, MW, 2, STAGE, TB, MINB, false, SHP>);
+        else if (ksm == 1) run(richards_rows_kernel<DIM, MW, 1, STAGE, TB, MINB, false, SHP>);
+        else run(richards_rows_kernel<DIM, MW, 0, STAGE, TB, MINB, false, SHP>);
     }
 }
 
@@ -600,7 +625,7 @@ int richards_assembly_blocks(const wspm_mesh *mesh, const wspm_pattern *pat) {
 // slots (state 0 free, 1 being written, 2 ready; keys are the Jacobian's bits).
 // Every wait and probe sequence is bounded; a table that overflows, or a wait that
 // gives up, sets the overflow word and the shape path is not used.
-constexpr int kShapeSlots = 2048;
+constexpr int kShapeSlots = 32768;     // > kMaxShapesGlobal, and slot ids fit the 16-bit element slots
 
 __device__ __forceinline__ unsigned int shape_ld_acquire(const unsigned int *p) {
     unsigned int v;
@@ -706,12 +731,14 @@ __global__ void shape_table_kernel(const unsigned int *state, const unsigned lon
     }
 }
 
-// Incidence words with the element's shape id above the position fields.
-template <int DIM>
+// Incidence words with the element's shape id above the position fields (mode
+// 1: the 6-bit positions kept; mode 2: repacked into 4 bits each).
+template <int DIM, int SHP>
 __global__ void shape_words_kernel(int n_slices, const int64_t *__restrict__ inc_ptr,
                                    const int32_t *__restrict__ inc_width, const int32_t *__restrict__ inc_elem,
                                    const uint32_t *__restrict__ inc_slots, const uint16_t *__restrict__ elem_slot,
                                    const int *__restrict__ slot_shape, uint32_t *words) {
+    constexpr int NV = DIM + 1;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = i >> 5, lane = i & 31;
     if (s >= n_slices) return;
@@ -720,8 +747,14 @@ __global__ void shape_words_kernel(int n_slices, const int64_t *__restrict__ inc
     for (int k = 0; k < w; ++k) {
         const int64_t o = ib + (int64_t)kSlice * k;
         const int e = inc_elem[o];
-        uint32_t word = inc_slots[o];
-        if (e >= 0) word |= (uint32_t)slot_shape[elem_slot[e]] << kShapeShift<DIM>;
+        const uint32_t src = inc_slots[o];
+        uint32_t word = src;
+        if constexpr (SHP == 2) {
+            word = src & 3u;
+#pragma unroll
+            for (int j = 0; j < NV; ++j) word |= ((src >> (2 + 6 * j)) & 15u) << (2 + 4 * j);
+        }
+        if (e >= 0) word |= (uint32_t)slot_shape[elem_slot[e]] << kShapeShift<DIM, SHP>;
         words[o] = word;
     }
 }
@@ -747,7 +780,7 @@ static ShapeBuffer carve_shapes(void *base, const wspm_mesh *mesh, const wspm_pa
     sb.keys = (unsigned long long *)take((int64_t)kShapeSlots * dim * dim * 8);
     sb.slot_shape = (int *)take((int64_t)kShapeSlots * 4);
     sb.meta = (int *)take(64 * 4);
-    sb.table = (double *)take((int64_t)(dim == 2 ? kMaxShapes<2> * kShapeStride<2> : kMaxShapes<3> * kShapeStride<3>) * 8);
+    sb.table = (double *)take((int64_t)(dim == 2 ? kMaxShapes<2> * kShapeStride<2> : kMaxShapesGlobal * kShapeStride<3>) * 8);
     sb.bytes = off;
     return sb;
 }
@@ -759,9 +792,11 @@ int64_t richards_shape_bytes(const wspm_mesh *mesh, const wspm_pattern *pat) {
 
 // Builds the shape words and table in `buf` (synchronous, plan creation).  Returns
 // the number of shapes, or 0 when the mesh has too many (the caller then uses the
-// geometry-computing kernel) or anything failed.
+// geometry-computing kernel) or anything failed; *mode: 1 (table in shared memory)
+// or 2 (global table, 4-bit row positions: 3D patterns of at most 16 entries per row).
 int richards_build_shapes(const wspm_mesh *mesh, const wspm_pattern *pat, void *buf, const uint32_t **words,
-                          const double **table) {
+                          const double **table, int *mode) {
+    *mode = 0;
     if (!mesh || !pat || !buf || mesh->n_elems <= 0 || pat->n_slices <= 0 || !pat->inc_slots || !pat->inc_elem)
         return 0;
     if (mesh->dim != 2 && mesh->dim != 3) return 0;
@@ -776,21 +811,28 @@ int richards_build_shapes(const wspm_mesh *mesh, const wspm_pattern *pat, void *
         shape_table_kernel<2><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table, kMaxShapes<2>);
     } else {
         shape_insert_kernel<3><<<blocks, 256>>>(*mesh, sb.state, sb.keys, sb.elem_slot, sb.meta);
-        shape_table_kernel<3><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table, kMaxShapes<3>);
+        shape_table_kernel<3><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table,
+                                          pat->max_width <= 16 ? kMaxShapesGlobal : kMaxShapes<3>);
     }
     int meta[2] = {0, 1};
     if (cudaGetLastError() != cudaSuccess || cudaMemcpy(meta, sb.meta, sizeof(meta), cudaMemcpyDeviceToHost) != cudaSuccess)
         return 0;
     if (meta[1] != 0 || meta[0] <= 0) return 0;
+    const int md = meta[0] <= (mesh->dim == 2 ? kMaxShapes<2> : kMaxShapes<3>) ? 1 : 2;
+    if (md == 2 && (mesh->dim != 3 || pat->max_width > 16 || meta[0] > kMaxShapesGlobal)) return 0;
     if (mesh->dim == 2)
-        shape_words_kernel<2><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
-                                            pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
+        shape_words_kernel<2, 1><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
+                                               pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
+    else if (md == 1)
+        shape_words_kernel<3, 1><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
+                                               pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
     else
-        shape_words_kernel<3><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
-                                            pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
+        shape_words_kernel<3, 2><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
+                                               pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return 0;
     *words = sb.words;
     *table = sb.table;
+    *mode = md;
     return meta[0];
 }
 
@@ -800,7 +842,7 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
                                          const double *Ks_inc, const double s[4], const double mc[4], double dt,
                                          const double *dt_dev, const double *bc_val, double *vals, float *vals32,
                                          double *rhs, double *dinv, const RefineStart *res, const uint32_t *shape_words,
-                                         const double *shape_tab, int n_shapes, cudaStream_t st) {
+                                         const double *shape_tab, int n_shapes, int shape_mode, cudaStream_t st) {
     RichardsAsmArgs a;
     const bool fused = res != nullptr;
     if (fused) a.res = *res;
@@ -825,7 +867,8 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     const int ns = pat->n_slices;
     const int mw = pat->max_width;
     // the shape path where the plan found few element shapes (its words carry the shape ids)
-    const bool cls = shape_words && shape_tab && n_shapes > 0 && mw <= 16;
+    const int shp = (shape_words && shape_tab && n_shapes > 0 && mw <= 16) ? shape_mode : 0;
+    const bool cls = shp != 0;
     if (cls) {
         a.inc_slots = shape_words;
         a.shape_tab = shape_tab;
@@ -834,25 +877,28 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     // launch shapes measured on the 1024^2 triangle and 96^3 Kuhn-tetrahedron grids (B200)
     if (mesh->dim == 2) {
         if (mw <= 8) {
-            if (cls) launch_rows<2, 8, true, 256, 5, true>(a, ksm, ns, fused, st);
-            else launch_rows<2, 8, true, 256, 3, false>(a, ksm, ns, fused, st);
+            if (shp == 1) launch_rows<2, 8, true, 256, 5, 1>(a, ksm, ns, fused, st);
+            else launch_rows<2, 8, true, 256, 3, 0>(a, ksm, ns, fused, st);
         } else if (mw <= 16) {
-            if (cls) launch_rows<2, 16, true, 128, 2, true>(a, ksm, ns, fused, st);
-            else launch_rows<2, 16, true, 128, 1, false>(a, ksm, ns, fused, st);
-        } else if (mw <= 32) launch_rows<2, 32, true, 64, 1, false>(a, ksm, ns, fused, st);
-        else launch_rows<2, 64, true, 32, 1, false>(a, ksm, ns, fused, st);
+            if (shp == 1) launch_rows<2, 16, true, 128, 2, 1>(a, ksm, ns, fused, st);
+            else launch_rows<2, 16, true, 128, 1, 0>(a, ksm, ns, fused, st);
+        } else if (mw <= 32) launch_rows<2, 32, true, 64, 1, 0>(a, ksm, ns, fused, st);
+        else launch_rows<2, 64, true, 32, 1, 0>(a, ksm, ns, fused, st);
     } else {
         if (pat->n_diags > 0 && mw <= 16) {
-            if (cls) launch_rows<3, 16, false, 128, 8, true>(a, ksm, ns, fused, st);
-            else launch_rows<3, 16, false, 128, 8, false>(a, ksm, ns, fused, st);
+            if (shp == 1) launch_rows<3, 16, false, 128, 8, 1>(a, ksm, ns, fused, st);
+            else if (shp == 2) launch_rows<3, 16, false, 128, 8, 2>(a, ksm, ns, fused, st);
+            else launch_rows<3, 16, false, 128, 8, 0>(a, ksm, ns, fused, st);
         } else if (mw <= 8) {
-            if (cls) launch_rows<3, 8, true, 128, 2, true>(a, ksm, ns, fused, st);
-            else launch_rows<3, 8, true, 128, 1, false>(a, ksm, ns, fused, st);
+            if (shp == 1) launch_rows<3, 8, true, 128, 2, 1>(a, ksm, ns, fused, st);
+            else if (shp == 2) launch_rows<3, 8, true, 128, 2, 2>(a, ksm, ns, fused, st);
+            else launch_rows<3, 8, true, 128, 1, 0>(a, ksm, ns, fused, st);
         } else if (mw <= 16) {
-            if (cls) launch_rows<3, 16, true, 128, 2, true>(a, ksm, ns, fused, st);
-            else launch_rows<3, 16, true, 128, 1, false>(a, ksm, ns, fused, st);
-        } else if (mw <= 32) launch_rows<3, 32, true, 64, 1, false>(a, ksm, ns, fused, st);
-        else launch_rows<3, 64, true, 32, 1, false>(a, ksm, ns, fused, st);
+            if (shp == 1) launch_rows<3, 16, true, 128, 2, 1>(a, ksm, ns, fused, st);
+            else if (shp == 2) launch_rows<3, 16, true, 128, 2, 2>(a, ksm, ns, fused, st);
+            else launch_rows<3, 16, true, 128, 1, 0>(a, ksm, ns, fused, st);
+        } else if (mw <= 32) launch_rows<3, 32, true, 64, 1, 0>(a, ksm, ns, fused, st);
+        else launch_rows<3, 64, true, 32, 1, 0>(a, ksm, ns, fused, st);
     }
     if (fused) refine_start_kernel<<<1, 1024, 0, st>>>(*res, richards_assembly_blocks(mesh, pat));
     return cudaGetLastError() == cudaSuccess ? WSPM_OK : WSPM_CUDA_ERROR;
@@ -864,7 +910,7 @@ int launch_richards_assembly(const wspm_mesh *mesh, const wspm_pattern *pat, con
                              const double *bc_val, double *vals, float *vals32, double *rhs, double *dinv,
                              cudaStream_t st) {
     return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, nullptr, s, mc, dt,
-                                         nullptr, bc_val, vals, vals32, rhs, dinv, nullptr, nullptr, nullptr, 0, st);
+                                         nullptr, bc_val, vals, vals32, rhs, dinv, nullptr, nullptr, nullptr, 0, 0, st);
 }
 
 int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *pat, const double *theta_m,
@@ -873,10 +919,10 @@ int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *p
                                     const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
                                     float *vals32, double *rhs, double *dinv, const RefineStart *res,
                                     const uint32_t *shape_words, const double *shape_tab, int n_shapes,
-                                    cudaStream_t st) {
+                                    int shape_mode, cudaStream_t st) {
     return launch_richards_assembly_impl(mesh, pat, theta_m, theta_n, h_m, K, C, Ks_elem, Ks_inc, s, mc, 1.0,
                                          dt_dev, bc_val, vals, vals32, rhs, dinv, res, shape_words, shape_tab,
-                                         n_shapes, st);
+                                         n_shapes, shape_mode, st);
 }
 
 int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st) {

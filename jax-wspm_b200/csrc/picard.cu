@@ -34,11 +34,11 @@ int launch_richards_assembly_dev_dt(const wspm_mesh *mesh, const wspm_pattern *p
                                     const double mc[4], const double *dt_dev, const double *bc_val, double *vals,
                                     float *vals32, double *rhs, double *dinv, const RefineStart *res,
                                     const uint32_t *shape_words, const double *shape_tab, int n_shapes,
-                                    cudaStream_t st);
+                                    int shape_mode, cudaStream_t st);
 int richards_assembly_blocks(const wspm_mesh *mesh, const wspm_pattern *pat);
 int64_t richards_shape_bytes(const wspm_mesh *mesh, const wspm_pattern *pat);
 int richards_build_shapes(const wspm_mesh *mesh, const wspm_pattern *pat, void *buf, const uint32_t **words,
-                          const double **table);
+                          const double **table, int *mode);
 unsigned long long richards_dia_live_mask(const wspm_mesh *mesh, const wspm_pattern *pat, unsigned long long *word);
 int launch_incidence_gather(const wspm_pattern *pat, const double *elem, double *out, cudaStream_t st);
 
@@ -322,6 +322,7 @@ struct PicardPlan {
     const uint32_t *shape_words = nullptr;
     const double *shape_tab = nullptr;
     int n_shapes = 0;
+    int shape_mode = 0;   // 1: table in shared memory, 2: global table (4-bit row positions in the words)
 };
 
 // The plan's matrix descriptor: the pattern with its structural-zero diagonals marked.
@@ -398,7 +399,8 @@ static int build_picard_graph(PicardPlan *P) {
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                         P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
                                         d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr,
-                                        P->shape_words, P->shape_tab, P->n_shapes, bs);
+                                        P->shape_words, P->shape_tab, P->n_shapes,
+                                        P->shape_mode, bs);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           bs);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
@@ -505,7 +507,8 @@ static int picard_step_host(PicardPlan *P, cudaStream_t st) {
         launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                         P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
                                         d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, fused ? &rs : nullptr,
-                                        P->shape_words, P->shape_tab, P->n_shapes, st);
+                                        P->shape_words, P->shape_tab, P->n_shapes,
+                                        P->shape_mode, st);
         launch_edge_terms(&P->pat, &P->neumann, WSPM_EDGE_NEUMANN, d.neumann_flux, 0.0, d.K, nullptr, d.vals, d.rhs,
                           st);
         launch_edge_terms(&P->pat, &P->drainage, WSPM_EDGE_DRAINAGE_WATER, 0.0, 0.0, d.K, nullptr, d.vals, d.rhs,
@@ -655,7 +658,9 @@ extern "C" int wspm_picard_create(const wspm_picard_desc *desc, void **plan_out)
     // partial-sum slot of the workspace serves as the scratch word)
     P->live = richards_dia_live_mask(&P->mesh, &P->pat, reinterpret_cast<unsigned long long *>(P->partials));
     // element shapes, found once from the geometry (synchronous)
-    if (d.shapes) P->n_shapes = richards_build_shapes(&P->mesh, &P->pat, d.shapes, &P->shape_words, &P->shape_tab);
+    if (d.shapes)
+        P->n_shapes = richards_build_shapes(&P->mesh, &P->pat, d.shapes, &P->shape_words, &P->shape_tab,
+                                            &P->shape_mode);
     // Ks in incidence order as of creation (every step refreshes it at its start)
     if (P->Ks_inc && (launch_incidence_gather(&P->pat, d.Ks_elem, P->Ks_inc, 0) != WSPM_OK ||
                       cudaDeviceSynchronize() != cudaSuccess)) {
@@ -679,7 +684,7 @@ extern "C" int wspm_picard_assemble(void *plan, void *stream) {
     return launch_richards_assembly_dev_dt(&P->mesh, &P->pat, d.theta_m, d.theta_n, d.h_m, d.K, d.C, d.Ks_elem,
                                            P->Ks_inc, P->s, P->mc, d.dt_dev, d.bc_val, d.vals,
                                            d.mixed ? d.vals32 : nullptr, d.rhs, d.dinv, nullptr, P->shape_words,
-                                           P->shape_tab, P->n_shapes, st);
+                                           P->shape_tab, P->n_shapes, P->shape_mode, st);
 }
 
 extern "C" int32_t wspm_picard_shapes(void *plan) {

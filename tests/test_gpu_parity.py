@@ -621,13 +621,14 @@ def test_engine_on_a_device_built_pattern_matches_host_built():
     np.testing.assert_array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("case", ["tri-binary", "tri-jitter", "tet-binary"])
+@pytest.mark.parametrize("case", ["tri-binary", "tri-jitter", "tet-binary", "tet-decimal"])
 @pytest.mark.parametrize("mixed", [False, True])
 def test_element_shape_table_gives_bitwise_identical_steps(case, mixed):
     """The plan's element-shape path (distinct element Jacobians found once; each element-row's geometric factors
     read from a per-shape table) runs the same Picard steps bit for bit as the assembly that recomputes every
     element's geometry: a grid with exact binary coordinates has 2 triangle shapes (6 Kuhn tetrahedra); a jittered
-    mesh has one shape per element, too many, and keeps the recomputing kernel."""
+    mesh has one shape per element, too many, and keeps the recomputing kernel; a Kuhn grid with coordinates i/21
+    has 3,072 (more than the shared-memory table holds) and takes the global table with 4-bit row positions."""
     from wspm_b200.device import DeviceMesh, merge_dirichlet
     from wspm_b200.engine import PicardEngine
     rng = np.random.default_rng(7)
@@ -640,9 +641,12 @@ def test_element_shape_table_gives_bitwise_identical_steps(case, mixed):
         pts = pts.copy()
         pts[inner] += rng.uniform(-0.2, 0.2, (int(inner.sum()), 2)) / 40
         want = 0
-    else:
+    elif case == "tet-binary":
         pts, el = mesh.kuhn_tetrahedra(8, 1.0)
         want = 6
+    else:   # coordinates i/21: 3,072 distinct Jacobians, the global table with 4-bit row positions
+        pts, el = mesh.kuhn_tetrahedra(21, 1.0)
+        want = 3072
     dim = pts.shape[1]
     top = np.where(pts[:, dim - 1] == pts[:, dim - 1].max())[0]
     Ks = 0.0922 * np.exp(rng.standard_normal(len(el)))
