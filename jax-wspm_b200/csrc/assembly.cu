@@ -887,7 +887,7 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     } else {
         if (pat->n_diags > 0 && mw <= 16) {
             if (shp == 1) launch_rows<3, 16, false, 128, 8, 1>(a, ksm, ns, fused, st);
-            else if (shp == 2) launch_rows<3, 16, false, 128, 8, 2>(a, ksm, ns, fused, st);
+            else if (shp == 2) launch_rows<3, 16, false, 128, 12, 2>(a, ksm, ns, fused, st);
             else launch_rows<3, 16, false, 128, 8, 0>(a, ksm, ns, fused, st);
         } else if (mw <= 8) {
             if (shp == 1) launch_rows<3, 8, true, 128, 2, 1>(a, ksm, ns, fused, st);
