@@ -408,10 +408,12 @@ typedef struct wspm_picard_desc {
                                   bytes of device memory: the plan records the
                                   mesh's distinct element Jacobians (bitwise)
                                   there at creation, and when they are few
-                                  (<= 256 triangle / 64 tetrahedron shapes, the
-                                  table in shared memory; or, for tetrahedra
-                                  with at most 16 stored entries per row, up to
-                                  16,384 shapes in a global table) its assembly
+                                  (up to 64 shapes, the table in shared
+                                  memory; for patterns with at most 16 stored
+                                  entries per row, up to 16,384 shapes and at
+                                  least 8 elements per shape, a global table;
+                                  wider rows: up to 256 triangle shapes in
+                                  shared memory) its assembly
                                   reads each element-row's geometric factors
                                   from the per-shape table instead of
                                   recomputing them (same values bit for bit);

@@ -74,15 +74,17 @@ struct RichardsAsmArgs {
 // row positions, the shape id sits above them (12 bits in 2D, 6 in 3D) and the
 // table (at most 256 triangle / 64 tetrahedron shapes) is copied into shared
 // memory.  Mode 2, for patterns with at most 16 entries per row: the row
-// positions are repacked into 4 bits each, the id takes the 14 (3D) bits above
-// them, and the table (up to 16,384 shapes; 1.7 MB for the 10,368 tetrahedra of
-// a 96^3 grid with coordinates i/96) is read from global memory, where it stays
-// in L2.
+// positions are repacked into 4 bits each, the id takes the 18 (2D) or 14 (3D)
+// bits above them, and the table (up to 16,384 shapes; 1.7 MB for the 10,368
+// tetrahedra of a 96^3 grid with coordinates i/96) is read from global memory,
+// where it stays in L2.
 template <int DIM> constexpr int kShapeStride = 1 + (DIM + 1) * (DIM + 1) + (DIM + 1);
 template <int DIM, int SHP> constexpr int kPosBits = SHP == 2 ? 4 : 6;
 template <int DIM, int SHP> constexpr int kShapeShift = 2 + kPosBits<DIM, SHP> * (DIM + 1);
 template <int DIM> constexpr int kMaxShapes = DIM == 2 ? 256 : 64;          // mode 1
-constexpr int kMaxShapesGlobal = 16384;                                      // mode 2 (3D: 14 bits)
+constexpr int kMaxShapesGlobal = 16384;                                      // mode 2 (2D: 18 bits, 3D: 14)
+constexpr int kShapeReuse = 8;                                               // mode 2: elements per shape, at least
+constexpr int kShapesShared = 64;                                            // mode 1 preferred up to this many
 
 template <int DIM>
 __device__ __forceinline__ void p1_geometry(const double *__restrict__ coords, const int (&nd)[DIM + 1],
@@ -780,7 +782,7 @@ static ShapeBuffer carve_shapes(void *base, const wspm_mesh *mesh, const wspm_pa
     sb.keys = (unsigned long long *)take((int64_t)kShapeSlots * dim * dim * 8);
     sb.slot_shape = (int *)take((int64_t)kShapeSlots * 4);
     sb.meta = (int *)take(64 * 4);
-    sb.table = (double *)take((int64_t)(dim == 2 ? kMaxShapes<2> * kShapeStride<2> : kMaxShapesGlobal * kShapeStride<3>) * 8);
+    sb.table = (double *)take((int64_t)kMaxShapesGlobal * (dim == 2 ? kShapeStride<2> : kShapeStride<3>) * 8);
     sb.bytes = off;
     return sb;
 }
@@ -808,7 +810,8 @@ int richards_build_shapes(const wspm_mesh *mesh, const wspm_pattern *pat, void *
     const int nsw = (pat->n_slices * kSlice + 255) / 256;
     if (mesh->dim == 2) {
         shape_insert_kernel<2><<<blocks, 256>>>(*mesh, sb.state, sb.keys, sb.elem_slot, sb.meta);
-        shape_table_kernel<2><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table, kMaxShapes<2>);
+        shape_table_kernel<2><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table,
+                                          pat->max_width <= 16 ? kMaxShapesGlobal : kMaxShapes<2>);
     } else {
         shape_insert_kernel<3><<<blocks, 256>>>(*mesh, sb.state, sb.keys, sb.elem_slot, sb.meta);
         shape_table_kernel<3><<<1, 256>>>(sb.state, sb.keys, sb.slot_shape, sb.meta, sb.table,
@@ -818,10 +821,23 @@ int richards_build_shapes(const wspm_mesh *mesh, const wspm_pattern *pat, void *
     if (cudaGetLastError() != cudaSuccess || cudaMemcpy(meta, sb.meta, sizeof(meta), cudaMemcpyDeviceToHost) != cudaSuccess)
         return 0;
     if (meta[1] != 0 || meta[0] <= 0) return 0;
-    const int md = meta[0] <= (mesh->dim == 2 ? kMaxShapes<2> : kMaxShapes<3>) ? 1 : 2;
-    if (md == 2 && (mesh->dim != 3 || pat->max_width > 16 || meta[0] > kMaxShapesGlobal)) return 0;
-    if (mesh->dim == 2)
+    // The global table replaces a recomputation of cheap geometry with reads from L2: it is taken only when each
+    // shape serves at least kShapeReuse elements on average (a structured grid), never for a mesh whose elements
+    // are all distinct.  Every block copies the shared-memory table whole, so beyond kShapesShared shapes the
+    // global table is the faster of the two (2D assembly at 1000^2, 162 shapes: 63.7 against 69.8 us; at 24
+    // shapes the shared table wins, 59.8 against 63.7 us).
+    const bool global_ok = pat->max_width <= 16 && meta[0] <= kMaxShapesGlobal &&
+                           (int64_t)meta[0] * kShapeReuse <= (int64_t)mesh->n_elems;
+    int md;
+    if (global_ok && meta[0] > kShapesShared) md = 2;
+    else if (meta[0] <= (mesh->dim == 2 ? kMaxShapes<2> : kMaxShapes<3>)) md = 1;
+    else if (global_ok) md = 2;
+    else return 0;
+    if (mesh->dim == 2 && md == 1)
         shape_words_kernel<2, 1><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
+                                               pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
+    else if (mesh->dim == 2)
+        shape_words_kernel<2, 2><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
                                                pat->inc_slots, sb.elem_slot, sb.slot_shape, sb.words);
     else if (md == 1)
         shape_words_kernel<3, 1><<<nsw, 256>>>(pat->n_slices, pat->inc_ptr, pat->inc_width, pat->inc_elem,
@@ -878,9 +894,11 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     if (mesh->dim == 2) {
         if (mw <= 8) {
             if (shp == 1) launch_rows<2, 8, true, 256, 5, 1>(a, ksm, ns, fused, st);
+            else if (shp == 2) launch_rows<2, 8, true, 256, 4, 2>(a, ksm, ns, fused, st);
             else launch_rows<2, 8, true, 256, 3, 0>(a, ksm, ns, fused, st);
         } else if (mw <= 16) {
             if (shp == 1) launch_rows<2, 16, true, 128, 2, 1>(a, ksm, ns, fused, st);
+            else if (shp == 2) launch_rows<2, 16, true, 128, 2, 2>(a, ksm, ns, fused, st);
             else launch_rows<2, 16, true, 128, 1, 0>(a, ksm, ns, fused, st);
         } else if (mw <= 32) launch_rows<2, 32, true, 64, 1, 0>(a, ksm, ns, fused, st);
         else launch_rows<2, 64, true, 32, 1, 0>(a, ksm, ns, fused, st);

@@ -621,20 +621,24 @@ def test_engine_on_a_device_built_pattern_matches_host_built():
     np.testing.assert_array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("case", ["tri-binary", "tri-jitter", "tet-binary", "tet-decimal"])
+@pytest.mark.parametrize("case", ["tri-binary", "tri-decimal", "tri-jitter", "tet-binary", "tet-decimal"])
 @pytest.mark.parametrize("mixed", [False, True])
 def test_element_shape_table_gives_bitwise_identical_steps(case, mixed):
     """The plan's element-shape path (distinct element Jacobians found once; each element-row's geometric factors
     read from a per-shape table) runs the same Picard steps bit for bit as the assembly that recomputes every
     element's geometry: a grid with exact binary coordinates has 2 triangle shapes (6 Kuhn tetrahedra); a jittered
-    mesh has one shape per element, too many, and keeps the recomputing kernel; a Kuhn grid with coordinates i/21
-    has 3,072 (more than the shared-memory table holds) and takes the global table with 4-bit row positions."""
+    mesh has one shape per element, too many, and keeps the recomputing kernel; a triangle grid with coordinates
+    i/300 has 800 shapes and a Kuhn grid with coordinates i/21 3,072 (more than the shared-memory table holds): both
+    take the global table with 4-bit row positions."""
     from wspm_b200.device import DeviceMesh, merge_dirichlet
     from wspm_b200.engine import PicardEngine
     rng = np.random.default_rng(7)
     if case == "tri-binary":
         pts, el = mesh.structured_triangles(64, 1.0)
         want = 2
+    elif case == "tri-decimal":   # coordinates i/300: 800 shapes, the global table with 4-bit row positions
+        pts, el = mesh.structured_triangles(300, 1.0)
+        want = 800
     elif case == "tri-jitter":
         pts, el = mesh.structured_triangles(40, 1.0)
         inner = np.all((pts > 0) & (pts < 1), axis=1)
