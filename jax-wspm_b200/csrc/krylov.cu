@@ -498,12 +498,21 @@ __device__ __forceinline__ T dia_row_z(const T *__restrict__ vals, const int64_t
 // Rows i .. i+N-1 (i a multiple of N) of a DIA matrix times z: one 16-byte load
 // per diagonal, issued G diagonals at a time before their first use, then the
 // gathers diagonal by diagonal.  Each row accumulates in diagonal order.
+//
+// FP32: the four values z[i+o .. i+o+3] of a diagonal come from one or two
+// aligned 16-byte loads (the window's misalignment (i+o) mod 4 is the same for
+// every thread, so the selection below is a uniform branch).  With the lanes of
+// a warp 16 bytes apart, a scalar gather moves 512 bytes through L1 for 128
+// used; the windows move each byte once.  Groups whose window leaves [0, n)
+// (the first and last rows) and unaligned z take the scalar gathers with the
+// clamped columns.  Same products in the same order either way.
 template <typename T, int MW>
 __device__ __forceinline__ void dia_group_z(const T *__restrict__ vals, const int64_t *s_vo, int i, int last, int nd,
                                             const int *s_off, const T *z, T (&w)[Vec16<T>::N]) {
     using VT = Vec16<T>;
     constexpr int N = VT::N;
-    constexpr int G = MW < 4 ? MW : 4;
+    constexpr int G = MW < 4 ? MW : (N == 4 ? 2 : 4);
+    const bool zal = (reinterpret_cast<uintptr_t>(z) & 15) == 0;
 #pragma unroll
     for (int q = 0; q < N; ++q) w[q] = T(0);
 #pragma unroll
@@ -519,6 +528,35 @@ __device__ __forceinline__ void dia_group_z(const T *__restrict__ vals, const in
                 T e[N];
                 VT::split(vv[g], e);
                 const int o = s_off[k0 + g];
+                if constexpr (N == 4) {
+                    const int c0 = i + o;
+                    const int mis = c0 & 3;
+                    const int base = c0 - mis;
+                    if (zal && base >= 0 && base + (mis ? 8 : 4) <= last + 1) {
+                        const float4 lo = *reinterpret_cast<const float4 *>(z + base);
+                        float4 hi = lo;
+                        if (mis) hi = *reinterpret_cast<const float4 *>(z + base + 4);
+                        switch (mis) {
+                        case 0:
+                            w[0] = fma(e[0], lo.x, w[0]); w[1] = fma(e[1], lo.y, w[1]);
+                            w[2] = fma(e[2], lo.z, w[2]); w[3] = fma(e[3], lo.w, w[3]);
+                            break;
+                        case 1:
+                            w[0] = fma(e[0], lo.y, w[0]); w[1] = fma(e[1], lo.z, w[1]);
+                            w[2] = fma(e[2], lo.w, w[2]); w[3] = fma(e[3], hi.x, w[3]);
+                            break;
+                        case 2:
+                            w[0] = fma(e[0], lo.z, w[0]); w[1] = fma(e[1], lo.w, w[1]);
+                            w[2] = fma(e[2], hi.x, w[2]); w[3] = fma(e[3], hi.y, w[3]);
+                            break;
+                        default:
+                            w[0] = fma(e[0], lo.w, w[0]); w[1] = fma(e[1], hi.x, w[1]);
+                            w[2] = fma(e[2], hi.y, w[2]); w[3] = fma(e[3], hi.z, w[3]);
+                            break;
+                        }
+                        continue;
+                    }
+                }
 #pragma unroll
                 for (int q = 0; q < N; ++q) {
                     int c = i + q + o;
