@@ -305,6 +305,10 @@ __global__ void incidence_gather_kernel(int n_slices, const int64_t *__restrict_
 // element at column i + off[position] (L1-resident: the row's columns are the
 // neighbouring rows' columns too).  2D takes the stage; 3D (15 columns x 4
 // values would hold occupancy to two blocks per SM) takes the direct reads.
+// Either way the incidence words (and Ks) of 4 incidences are loaded together
+// before the first of them is used: with one incidence at a time the 3D rows
+// (24 tetrahedra per vertex) were a chain of dependent round trips (96^3 Kuhn
+// grid, global shape table: 217 -> 178 us; binary 64^3 grid: 75 -> 45 us).
 //
 // KSM selects the per-element conductivity factor: 0 none, 1 gathered by
 // element id, 2 read in incidence order (Ks_inc, built once per time step by
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(TB, MINB) richards_rows_kernel(RichardsAsmArgs
     constexpr bool CLS = SHP != 0;
     constexpr int PB = kPosBits<DIM, SHP>, PM = (1 << PB) - 1;   // row-position field of the incidence word
     constexpr int NV = DIM + 1;
-    constexpr int CH = STAGE ? 4 : 1;   // incidences whose loads are issued together
+    constexpr int CH = 4;               // incidences whose loads are issued together
     constexpr int CV = CLS ? 1 : NV;    // staged values per column (K; or coordinates and K)
     extern __shared__ double acc_sm[];  // [MW][TB] accumulators, [MW][CV][TB] column data (STAGE), shapes (CLS)
     __shared__ int s_off[MW];
@@ -905,7 +909,7 @@ static int launch_richards_assembly_impl(const wspm_mesh *mesh, const wspm_patte
     } else {
         if (pat->n_diags > 0 && mw <= 16) {
             if (shp == 1) launch_rows<3, 16, false, 128, 8, 1>(a, ksm, ns, fused, st);
-            else if (shp == 2) launch_rows<3, 16, false, 128, 12, 2>(a, ksm, ns, fused, st);
+            else if (shp == 2) launch_rows<3, 16, false, 128, 10, 2>(a, ksm, ns, fused, st);
             else launch_rows<3, 16, false, 128, 8, 0>(a, ksm, ns, fused, st);
         } else if (mw <= 8) {
             if (shp == 1) launch_rows<3, 8, true, 128, 2, 1>(a, ksm, ns, fused, st);
