@@ -699,17 +699,31 @@ __global__ void shape_table_kernel(const unsigned int *state, const unsigned lon
                                    int *meta, double *table, int max_shapes) {
     constexpr int NV = DIM + 1, NK = DIM * DIM;
     __shared__ int s_count;
+    __shared__ int s_first[1024];
+    // ids in ascending slot order: every thread counts the filled slots of its contiguous range, an exclusive
+    // prefix over the threads (in thread order) gives each range its first id
+    const int T = blockDim.x;
+    const int per = (kShapeSlots + T - 1) / T;
+    const int lo = min(kShapeSlots, (int)threadIdx.x * per), hi = min(kShapeSlots, lo + per);
+    int mine = 0;
+    for (int sl = lo; sl < hi; ++sl) mine += state[sl] == 2u ? 1 : 0;
+    s_first[threadIdx.x] = mine;
+    __syncthreads();
     if (threadIdx.x == 0) {
         int c = 0;
-        for (int sl = 0; sl < kShapeSlots; ++sl) {
-            if (state[sl] == 2u) slot_shape[sl] = c++;
-            else slot_shape[sl] = -1;
+        for (int t = 0; t < T; ++t) {
+            const int m = s_first[t];
+            s_first[t] = c;
+            c += m;
         }
         meta[0] = c;
         if (c > max_shapes) meta[1] = 1;
         s_count = c;
     }
     __syncthreads();
+    int next = s_first[threadIdx.x];
+    for (int sl = lo; sl < hi; ++sl) slot_shape[sl] = state[sl] == 2u ? next++ : -1;
+    __syncthreads();   // every slot's id written before the loop below reads other threads' slots
     if (s_count > max_shapes) return;
     for (int sl = threadIdx.x; sl < kShapeSlots; sl += blockDim.x) {
         const int id = slot_shape[sl];
